@@ -1,0 +1,72 @@
+// Shared device-side definitions for the gs-native B200 kernels (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "gsn_types.h"
+
+namespace gsn {
+
+constexpr int kTile = GSN_TILE_SIZE;           // 16x16 pixel tiles (renderer.cu:11)
+constexpr int kTilePixels = kTile * kTile;
+constexpr int kParams = GSN_PARAM_COUNT;       // 58 rows per Gaussian
+constexpr int kShStride = GSN_SH_COEFFS;       // 16 coefficients per colour channel
+constexpr float kLowPass = 0.3f;               // screen-space dilation (renderer.cu:12)
+constexpr float kFovClamp = 1.3f;              // Jacobian clamp (renderer.cu:13)
+constexpr float kNearFloor = 1e-6f;            // renderer.cu:14
+constexpr float kAlphaMax = 0.99f;             // renderer.cu:315
+constexpr float kAlphaMin = 1.0f / 255.0f;     // renderer.cu:316
+constexpr float kTransmittanceMin = 1e-4f;     // renderer.cu:320
+
+// Real spherical-harmonics normalisation constants, degrees 0-3 (standard values;
+// same table as renderer.cu:17-30).
+constexpr float kSh0 = 0.28209479177387814f;
+constexpr float kSh1 = 0.4886025119029199f;
+constexpr float kSh2a = 1.0925484305920792f;
+constexpr float kSh2b = 0.31539156525252005f;
+constexpr float kSh2c = 0.5462742152960396f;
+constexpr float kSh3a = 0.5900435899266435f;
+constexpr float kSh3b = 2.890611442640554f;
+constexpr float kSh3c = 0.4570457994644658f;
+constexpr float kSh3d = 0.3731763325901154f;
+constexpr float kSh3e = 1.445305721320277f;
+
+__host__ __device__ inline int ceil_div(int64_t a, int64_t b) { return static_cast<int>((a + b - 1) / b); }
+
+// Status helper: map the last launch error to a gsn status.
+inline int launch_status() {
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) return GSN_OK;
+    return e == cudaErrorMemoryAllocation ? GSN_ERR_OUT_OF_MEMORY : GSN_ERR_CUDA;
+}
+
+// Rodrigues rotation of an axis-angle vector. The expression order is the one
+// the reference uses in renderer.cu:35-66 and solver.cu:185-221, which the
+// bit-exact parity of tile keys depends on.
+__device__ __forceinline__ void axis_angle_to_matrix(float rx, float ry, float rz, float R[9]) {
+    float angle = sqrtf(rx * rx + ry * ry + rz * rz);
+    if (angle < 1e-8f) {
+        R[0] = 1.0f; R[1] = 0.0f; R[2] = 0.0f;
+        R[3] = 0.0f; R[4] = 1.0f; R[5] = 0.0f;
+        R[6] = 0.0f; R[7] = 0.0f; R[8] = 1.0f;
+        return;
+    }
+    float x = rx / angle;
+    float y = ry / angle;
+    float z = rz / angle;
+    float c = cosf(angle);
+    float s = sinf(angle);
+    float t = 1.0f - c;
+    R[0] = c + t * x * x;
+    R[1] = t * x * y - s * z;
+    R[2] = t * x * z + s * y;
+    R[3] = t * x * y + s * z;
+    R[4] = c + t * y * y;
+    R[5] = t * y * z - s * x;
+    R[6] = t * x * z - s * y;
+    R[7] = t * y * z + s * x;
+    R[8] = c + t * z * z;
+}
+
+}  // namespace gsn

@@ -1,0 +1,159 @@
+// (a) Projection / preprocess: axis-angle -> rotation -> 3D covariance -> 2D conic,
+// degree-3 SH colour and per-Gaussian tile-overlap counting.
+//
+// One thread per Gaussian over the 58 x N SoA parameter block, so every parameter
+// row is read with fully coalesced 128-byte transactions. The arithmetic of the
+// screen-space quantities (depth, u, v, radius and therefore the tile rectangle)
+// follows the reference's expression order exactly (renderer.cu:108-221): tile
+// keys, record counts and per-tile ranges must be bit-identical to the
+// reference's own kernels.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace gsn {
+
+namespace {
+
+// Evaluate the real SH basis of degree <= D at unit direction (x, y, z)
+// (renderer.cu:68-106: same basis order and sign convention).
+template <int D>
+__device__ __forceinline__ void sh_basis(float x, float y, float z, float b[16]) {
+    b[0] = kSh0;
+    if (D < 1) return;
+    b[1] = -kSh1 * y;
+    b[2] = kSh1 * z;
+    b[3] = -kSh1 * x;
+    if (D < 2) return;
+    float xx = x * x, yy = y * y, zz = z * z;
+    float xy = x * y, yz = y * z, xz = x * z;
+    b[4] = kSh2a * xy;
+    b[5] = -kSh2a * yz;
+    b[6] = kSh2b * (2.0f * zz - xx - yy);
+    b[7] = -kSh2a * xz;
+    b[8] = kSh2c * (xx - yy);
+    if (D < 3) return;
+    b[9] = -kSh3a * y * (3.0f * xx - yy);
+    b[10] = kSh3b * xy * z;
+    b[11] = -kSh3c * y * (4.0f * zz - xx - yy);
+    b[12] = kSh3d * z * (2.0f * zz - 3.0f * xx - 3.0f * yy);
+    b[13] = -kSh3c * x * (4.0f * zz - xx - yy);
+    b[14] = kSh3e * z * (xx - yy);
+    b[15] = -kSh3a * x * (xx - 3.0f * yy);
+}
+
+template <int D>
+__global__ void __launch_bounds__(256) project_kernel(const float* __restrict__ params,
+                                                      gsn_camera cam, int n,
+                                                      ProjectOutputs out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t N = n;
+    out.tile_counts[i] = 0;
+    out.depth_keys[i] = 0xFFFFFFFFu;
+    if (out.radii) out.radii[i] = 0.0f;
+
+    const float gx = __ldg(params + 0 * N + i);
+    const float gy = __ldg(params + 1 * N + i);
+    const float gz = __ldg(params + 2 * N + i);
+    const float* R = cam.R_c_w;
+    const float* t = cam.t_c_w;
+    float px = R[0] * gx + R[1] * gy + R[2] * gz + t[0];
+    float py = R[3] * gx + R[4] * gy + R[5] * gz + t[1];
+    float z = R[6] * gx + R[7] * gy + R[8] * gz + t[2];
+    float near = fmaxf(cam.near_depth, kNearFloor);
+    if (z <= near || z > fmaxf(cam.far_depth, near)) return;
+
+    float Rg[9];
+    axis_angle_to_matrix(__ldg(params + 6 * N + i), __ldg(params + 7 * N + i),
+                         __ldg(params + 8 * N + i), Rg);
+    float s[3] = {expf(__ldg(params + 3 * N + i)), expf(__ldg(params + 4 * N + i)),
+                  expf(__ldg(params + 5 * N + i))};
+    // M = R_c_w * R_g * S, cov = M M^T.
+    float M[9];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            M[r * 3 + c] = (R[r * 3] * Rg[c] + R[r * 3 + 1] * Rg[3 + c] + R[r * 3 + 2] * Rg[6 + c]) * s[c];
+    float V[9];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            V[r * 3 + c] = M[r * 3] * M[c * 3] + M[r * 3 + 1] * M[c * 3 + 1] + M[r * 3 + 2] * M[c * 3 + 2];
+
+    // Clamped perspective Jacobian.
+    float lim_x = kFovClamp * 0.5f * cam.width / cam.fx;
+    float lim_y = kFovClamp * 0.5f * cam.height / cam.fy;
+    float cxz = fminf(fmaxf(px / z, -lim_x), lim_x) * z;
+    float cyz = fminf(fmaxf(py / z, -lim_y), lim_y) * z;
+    float J[6] = {cam.fx / z, 0.0f, -cam.fx * cxz / (z * z), 0.0f, cam.fy / z, -cam.fy * cyz / (z * z)};
+    float JV[6];
+#pragma unroll
+    for (int r = 0; r < 2; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            JV[r * 3 + c] = J[r * 3] * V[c] + J[r * 3 + 1] * V[3 + c] + J[r * 3 + 2] * V[6 + c];
+    float a = JV[0] * J[0] + JV[1] * J[1] + JV[2] * J[2] + kLowPass;
+    float b = JV[0] * J[3] + JV[1] * J[4] + JV[2] * J[5];
+    float c = JV[3] * J[3] + JV[4] * J[4] + JV[5] * J[5] + kLowPass;
+    float det = a * c - b * b;
+    if (!(det > 0.0f)) return;
+    float mid = 0.5f * (a + c);
+    float radius = ceilf(3.0f * sqrtf(mid + sqrtf(fmaxf(0.1f, mid * mid - det))));
+    float u = cam.fx * px / z + cam.cx;
+    float v = cam.fy * py / z + cam.cy;
+    if (!isfinite(radius) || !isfinite(u) || !isfinite(v)) return;
+    int4 rect;
+    rect.x = static_cast<int>(fminf(cam.tile_count_x, fmaxf(0.0f, (u - radius) / kTile)));
+    rect.y = static_cast<int>(fminf(cam.tile_count_y, fmaxf(0.0f, (v - radius) / kTile)));
+    rect.z = static_cast<int>(fminf(cam.tile_count_x, fmaxf(0.0f, (u + radius + kTile - 1) / kTile)));
+    rect.w = static_cast<int>(fminf(cam.tile_count_y, fmaxf(0.0f, (v + radius + kTile - 1) / kTile)));
+    if (rect.x >= rect.z || rect.y >= rect.w) return;
+
+    out.depths[i] = z;
+    out.depth_keys[i] = __float_as_uint(z);
+    out.rects[i] = rect;
+    out.tile_counts[i] = (rect.z - rect.x) * (rect.w - rect.y);
+    if (out.radii) out.radii[i] = radius;
+    float det_inv = 1.0f / det;
+    float opacity = 1.0f / (1.0f + expf(-__ldg(params + 9 * N + i)));
+    out.means[i] = make_float2(u, v);
+    out.conic_opacity[i] = make_float4(c * det_inv, -b * det_inv, a * det_inv, opacity);
+
+    // View direction from the camera centre, C = -R^T t.
+    float dx = gx + R[0] * t[0] + R[3] * t[1] + R[6] * t[2];
+    float dy = gy + R[1] * t[0] + R[4] * t[1] + R[7] * t[2];
+    float dz = gz + R[2] * t[0] + R[5] * t[1] + R[8] * t[2];
+    float inv_len = rsqrtf(dx * dx + dy * dy + dz * dz);
+    float basis[16];
+    sh_basis<D>(dx * inv_len, dy * inv_len, dz * inv_len, basis);
+    constexpr int K = (D + 1) * (D + 1);
+    float rgb[3];
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch) {
+        const float* sh = params + (GSN_SH_INDEX + ch * kShStride) * N + i;
+        float value = 0.0f;
+#pragma unroll
+        for (int k = 0; k < K; ++k) value += basis[k] * __ldg(sh + k * N);
+        rgb[ch] = fmaxf(value + 0.5f, 0.0f);
+    }
+    out.colors[i] = make_float3(rgb[0], rgb[1], rgb[2]);
+}
+
+}  // namespace
+
+int launch_project(const float* params, int n, const gsn_camera& cam, int sh_degree,
+                   const ProjectOutputs& out, cudaStream_t stream) {
+    if (n <= 0) return GSN_OK;
+    dim3 grid(ceil_div(n, 256));
+    switch (sh_degree < 0 ? 0 : (sh_degree > 3 ? 3 : sh_degree)) {
+        case 0: project_kernel<0><<<grid, 256, 0, stream>>>(params, cam, n, out); break;
+        case 1: project_kernel<1><<<grid, 256, 0, stream>>>(params, cam, n, out); break;
+        case 2: project_kernel<2><<<grid, 256, 0, stream>>>(params, cam, n, out); break;
+        default: project_kernel<3><<<grid, 256, 0, stream>>>(params, cam, n, out); break;
+    }
+    return launch_status();
+}
+
+}  // namespace gsn

@@ -1,0 +1,409 @@
+// (b) Tile|depth ordering: stable LSD radix sort, exclusive scan, depth-ordered
+// record emission and per-tile ranges.
+//
+// The reference sorts one (tile << 32 | depth bits) 64-bit key per record with
+// a stable radix sort over 32 + ceil(log2 T) bits (renderer.cu:223-271, 541-563).
+// Here the same order - tile ascending, then depth bits ascending, then Gaussian
+// id ascending - is produced with far less traffic:
+//   1. a stable 32-bit radix sort of the N per-Gaussian depth keys (ids as values),
+//   2. records emitted in that depth order (exclusive scan of tile counts),
+//   3. a stable radix sort of the R records on the ceil(log2 T) tile bits only.
+// Stability of step 3 keeps depth (then id) order inside every tile, so the
+// resulting per-tile lists equal the reference's bit for bit.
+//
+// Every kernel reads its element count from device memory when one is given, so
+// the whole chain runs without a host round trip and can be captured in a graph.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace gsn {
+
+namespace {
+
+constexpr int kSortThreads = 256;
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kSortItems = 16;                      // per thread
+constexpr int kSortChunk = kSortThreads * kSortItems;  // 4096 keys per block
+constexpr int kBins = 256;
+
+// Device-resident counts are clamped to the host-side capacity the grid was sized
+// for, so an overflowing count can never drive an access past the buffers.
+__device__ __forceinline__ int load_count(const int* dev, int host) { return dev ? min(*dev, host) : host; }
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Per-block digit histogram of one 8-bit digit.
+__global__ void __launch_bounds__(kSortThreads) radix_upsweep(const uint32_t* __restrict__ keys,
+                                                              const int* n_dev, int n_host, int bit,
+                                                              uint32_t* __restrict__ block_hist,
+                                                              size_t hist_stride,
+                                                              uint32_t* __restrict__ digit_total) {
+    __shared__ uint32_t hist[kSortWarps][kBins];
+    const int n = load_count(n_dev, n_host);
+    const int64_t start = static_cast<int64_t>(blockIdx.x) * kSortChunk;
+    if (start >= n) return;
+    const int64_t end = min(static_cast<int64_t>(n), start + kSortChunk);
+    const int warp = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < kSortWarps * kBins; i += kSortThreads) (&hist[0][0])[i] = 0;
+    __syncthreads();
+#pragma unroll 4
+    for (int k = 0; k < kSortItems; ++k) {
+        int64_t idx = start + k * kSortThreads + threadIdx.x;
+        if (idx < end) atomicAdd(&hist[warp][(__ldg(keys + idx) >> bit) & 0xFF], 1u);
+    }
+    __syncthreads();
+    const int d = threadIdx.x;
+    uint32_t total = 0;
+#pragma unroll
+    for (int w = 0; w < kSortWarps; ++w) total += hist[w][d];
+    block_hist[d * hist_stride + blockIdx.x] = total;
+    if (total) atomicAdd(digit_total + d, total);
+}
+
+// One block per digit: exclusive scan of that digit's per-block counts, offset by
+// the number of keys with a smaller digit.
+__global__ void __launch_bounds__(kSortThreads) radix_scan(const int* n_dev, int n_host,
+                                                           uint32_t* __restrict__ block_hist,
+                                                           size_t hist_stride,
+                                                           const uint32_t* __restrict__ digit_total) {
+    __shared__ uint32_t warp_sums[kSortWarps];
+    __shared__ uint32_t carry;
+    const int n = load_count(n_dev, n_host);
+    const int blocks = ceil_div(n, kSortChunk);
+    const int d = blockIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // base = sum of totals of smaller digits
+    uint32_t v = threadIdx.x < d ? digit_total[threadIdx.x] : 0u;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) warp_sums[warp] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t s = 0;
+        for (int w = 0; w < kSortWarps; ++w) s += warp_sums[w];
+        carry = s;
+    }
+    __syncthreads();
+    uint32_t* row = block_hist + d * hist_stride;
+    for (int base = 0; base < blocks; base += kSortThreads) {
+        int i = base + threadIdx.x;
+        uint32_t x = i < blocks ? row[i] : 0u;
+        // inclusive warp scan
+        uint32_t inc = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += y;
+        }
+        __syncthreads();
+        if (lane == 31) warp_sums[warp] = inc;
+        __syncthreads();
+        uint32_t warp_prefix = 0, chunk_total = 0;
+#pragma unroll
+        for (int w = 0; w < kSortWarps; ++w) {
+            uint32_t s = warp_sums[w];
+            if (w < warp) warp_prefix += s;
+            chunk_total += s;
+        }
+        uint32_t c = carry;
+        if (i < blocks) row[i] = c + warp_prefix + inc - x;
+        __syncthreads();
+        if (threadIdx.x == 0) carry = c + chunk_total;
+    }
+}
+
+// Stable scatter. Warp w owns the w-th 512-key slice of the block's chunk and
+// walks it in 32-key steps; __match_any_sync ranks equal digits inside a step and
+// warp-private counters carry the rank across steps, which keeps the original
+// order among equal digits.
+template <bool kIdentityValues>
+__global__ void __launch_bounds__(kSortThreads) radix_downsweep(
+    const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ values_in,
+    uint32_t* __restrict__ keys_out, uint32_t* __restrict__ values_out, const int* n_dev, int n_host,
+    int bit, const uint32_t* __restrict__ block_hist, size_t hist_stride) {
+    __shared__ uint32_t counts[kSortWarps][kBins];
+    __shared__ uint32_t global_base[kBins];
+    const int n = load_count(n_dev, n_host);
+    const int64_t start = static_cast<int64_t>(blockIdx.x) * kSortChunk;
+    if (start >= n) return;
+    const int64_t end = min(static_cast<int64_t>(n), start + kSortChunk);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < kSortWarps * kBins; i += kSortThreads) (&counts[0][0])[i] = 0;
+    global_base[threadIdx.x] = block_hist[threadIdx.x * hist_stride + blockIdx.x];
+    __syncthreads();
+
+    const uint32_t lt = lanemask_lt();
+    const int64_t slice = start + static_cast<int64_t>(warp) * (kSortItems * 32);
+    uint32_t key[kSortItems], val[kSortItems], rank[kSortItems];
+#pragma unroll
+    for (int s = 0; s < kSortItems; ++s) {
+        int64_t idx = slice + s * 32 + lane;
+        bool valid = idx < end;
+        key[s] = valid ? keys_in[idx] : 0u;
+        if (kIdentityValues) val[s] = static_cast<uint32_t>(idx);
+        else val[s] = valid ? values_in[idx] : 0u;
+        uint32_t digit = valid ? ((key[s] >> bit) & 0xFF) : 0x100u;
+        uint32_t peers = __match_any_sync(0xffffffffu, digit);
+        uint32_t before = 0;
+        if (valid) before = counts[warp][digit];
+        __syncwarp();
+        rank[s] = before + __popc(peers & lt);
+        if (valid && (peers & lt) == 0) counts[warp][digit] = before + __popc(peers);
+        __syncwarp();
+        key[s] = valid ? key[s] : 0xFFFFFFFFu;
+        if (!valid) rank[s] = 0xFFFFFFFFu;
+    }
+    __syncthreads();
+    {   // exclusive prefix over warps, one thread per digit
+        const int d = threadIdx.x;
+        uint32_t run = 0;
+#pragma unroll
+        for (int w = 0; w < kSortWarps; ++w) {
+            uint32_t c = counts[w][d];
+            counts[w][d] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int s = 0; s < kSortItems; ++s) {
+        if (rank[s] == 0xFFFFFFFFu) continue;
+        uint32_t digit = (key[s] >> bit) & 0xFF;
+        uint32_t pos = global_base[digit] + counts[warp][digit] + rank[s];
+        keys_out[pos] = key[s];
+        values_out[pos] = val[s];
+    }
+}
+
+// ---------------------------------------------------------------- scan
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanChunk = kScanThreads * kScanItems;
+
+__device__ __forceinline__ int block_exclusive_scan(int x, int* warp_sums, int* total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int inc = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+    }
+    if (lane == 31) warp_sums[warp] = inc;
+    __syncthreads();
+    int prefix = 0, sum = 0;
+#pragma unroll
+    for (int w = 0; w < kScanThreads / 32; ++w) {
+        int s = warp_sums[w];
+        if (w < warp) prefix += s;
+        sum += s;
+    }
+    __syncthreads();
+    *total = sum;
+    return prefix + inc - x;
+}
+
+__global__ void __launch_bounds__(kScanThreads) scan_reduce(const int* __restrict__ in,
+                                                            const uint32_t* __restrict__ gather, int n,
+                                                            int* __restrict__ block_sums) {
+    __shared__ int warp_sums[kScanThreads / 32];
+    const int64_t start = static_cast<int64_t>(blockIdx.x) * kScanChunk;
+    int s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        int64_t i = start + k * kScanThreads + threadIdx.x;
+        if (i < n) s += gather ? in[gather[i]] : in[i];
+    }
+    int total;
+    block_exclusive_scan(s, warp_sums, &total);
+    if (threadIdx.x == 0) block_sums[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kScanThreads) scan_block_sums(int* __restrict__ block_sums, int blocks,
+                                                                int* __restrict__ total_out) {
+    __shared__ int warp_sums[kScanThreads / 32];
+    int carry = 0;
+    for (int base = 0; base < blocks; base += kScanThreads) {
+        int i = base + threadIdx.x;
+        int x = i < blocks ? block_sums[i] : 0;
+        int total;
+        int ex = block_exclusive_scan(x, warp_sums, &total);
+        if (i < blocks) block_sums[i] = carry + ex;
+        carry += total;
+    }
+    if (threadIdx.x == 0) *total_out = carry;
+}
+
+__global__ void __launch_bounds__(kScanThreads) scan_downsweep(const int* in, const uint32_t* __restrict__ gather,
+                                                               int n, const int* __restrict__ block_sums,
+                                                               int* out) {
+    __shared__ int warp_sums[kScanThreads / 32];
+    __shared__ int tile[kScanChunk];
+    const int64_t start = static_cast<int64_t>(blockIdx.x) * kScanChunk;
+    // striped coalesced load -> blocked per-thread sequences via shared memory
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        int j = k * kScanThreads + threadIdx.x;
+        int64_t i = start + j;
+        tile[j] = i < n ? (gather ? in[gather[i]] : in[i]) : 0;
+    }
+    __syncthreads();
+    int v[kScanItems];
+    int s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        v[k] = tile[threadIdx.x * kScanItems + k];
+        s += v[k];
+    }
+    int total;
+    int run = block_exclusive_scan(s, warp_sums, &total) + block_sums[blockIdx.x];
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        tile[threadIdx.x * kScanItems + k] = run;
+        run += v[k];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        int j = k * kScanThreads + threadIdx.x;
+        int64_t i = start + j;
+        if (i < n) out[i] = tile[j];
+    }
+}
+
+// ---------------------------------------------------------------- records
+// Four lanes per Gaussian walk its tile rectangle row-major; the records of one
+// Gaussian are contiguous and in the same order as the reference writes them.
+__global__ void __launch_bounds__(256) emit_records(const uint32_t* __restrict__ sorted_ids,
+                                                    const int* __restrict__ record_start,
+                                                    const int4* __restrict__ rects, int n, int tile_count_x,
+                                                    uint32_t* __restrict__ tile_keys,
+                                                    uint32_t* __restrict__ record_ids, int64_t capacity,
+                                                    int* overflow) {
+    const int64_t gidx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int64_t p = gidx >> 2;
+    const int sub = static_cast<int>(gidx & 3);
+    if (p >= n) return;
+    const int begin = record_start[p];
+    const int count = record_start[p + 1] - begin;
+    if (count <= 0) return;
+    if (begin + static_cast<int64_t>(count) > capacity) {
+        if (sub == 0) atomicExch(overflow, 1);
+        return;
+    }
+    const uint32_t id = sorted_ids[p];
+    const int4 r = rects[id];
+    const int width = r.z - r.x;
+    for (int k = sub; k < count; k += 4) {
+        int ty = r.y + k / width;
+        int tx = r.x + k % width;
+        tile_keys[begin + k] = static_cast<uint32_t>(ty * tile_count_x + tx);
+        record_ids[begin + k] = id;
+    }
+}
+
+__global__ void __launch_bounds__(256) tile_ranges(const uint32_t* __restrict__ tiles, const int* n_dev,
+                                                   int max_records, int tile_count, int64_t* __restrict__ offsets) {
+    const int n = min(*n_dev, max_records);
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+    const int64_t first = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (n <= 0) {
+        for (int64_t i = first; i <= tile_count; i += stride) offsets[i] = 0;
+        return;
+    }
+    for (int64_t r = first; r < n; r += stride) {
+        int t = static_cast<int>(tiles[r]);
+        int prev = r == 0 ? -1 : static_cast<int>(tiles[r - 1]);
+        for (int e = prev + 1; e <= t; ++e) offsets[e] = r;
+        if (r == n - 1)
+            for (int e = t + 1; e <= tile_count; ++e) offsets[e] = n;
+    }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- host side
+size_t radix_sort_scratch_bytes(int max_count) {
+    size_t blocks = static_cast<size_t>(ceil_div(max_count > 0 ? max_count : 1, kSortChunk));
+    return (static_cast<size_t>(kBins) * blocks + kBins * 4) * sizeof(uint32_t) + 256;
+}
+
+RadixSortScratch radix_sort_scratch(void* base, int max_count) {
+    RadixSortScratch s;
+    s.max_blocks = static_cast<size_t>(ceil_div(max_count > 0 ? max_count : 1, kSortChunk));
+    s.digit_total = static_cast<uint32_t*>(base);
+    s.block_hist = s.digit_total + kBins * 4;
+    return s;
+}
+
+int launch_radix_sort(uint32_t* keys, uint32_t* values, uint32_t* keys_alt, uint32_t* values_alt,
+                      bool identity_values, int max_count, const int* count_device, int begin_bit,
+                      int end_bit, const RadixSortScratch& scratch, bool* result_in_alt,
+                      cudaStream_t stream) {
+    *result_in_alt = false;
+    if (max_count <= 0 || end_bit <= begin_bit) return GSN_OK;
+    const int passes = (end_bit - begin_bit + 7) / 8;
+    if (passes > 4 || !keys || !keys_alt || !values || !values_alt) return GSN_ERR_INVALID_ARGUMENT;
+    if (cudaMemsetAsync(scratch.digit_total, 0, sizeof(uint32_t) * kBins * passes, stream) != cudaSuccess)
+        return GSN_ERR_CUDA;
+    const int blocks = ceil_div(max_count, kSortChunk);
+    uint32_t *kin = keys, *vin = values, *kout = keys_alt, *vout = values_alt;
+    for (int p = 0; p < passes; ++p) {
+        int bit = begin_bit + 8 * p;
+        uint32_t* dt = scratch.digit_total + kBins * p;
+        radix_upsweep<<<blocks, kSortThreads, 0, stream>>>(kin, count_device, max_count, bit,
+                                                           scratch.block_hist, scratch.max_blocks, dt);
+        radix_scan<<<kBins, kSortThreads, 0, stream>>>(count_device, max_count, scratch.block_hist,
+                                                       scratch.max_blocks, dt);
+        if (identity_values && p == 0)
+            radix_downsweep<true><<<blocks, kSortThreads, 0, stream>>>(
+                kin, nullptr, kout, vout, count_device, max_count, bit, scratch.block_hist, scratch.max_blocks);
+        else
+            radix_downsweep<false><<<blocks, kSortThreads, 0, stream>>>(
+                kin, vin, kout, vout, count_device, max_count, bit, scratch.block_hist, scratch.max_blocks);
+        uint32_t* tk = kin; kin = kout; kout = tk;
+        uint32_t* tv = vin; vin = vout; vout = tv;
+    }
+    *result_in_alt = (passes % 2) == 1;
+    return launch_status();
+}
+
+size_t scan_scratch_bytes(int n) {
+    return static_cast<size_t>(ceil_div(n > 0 ? n : 1, kScanChunk) + 1) * sizeof(int);
+}
+
+int launch_exclusive_scan(const int* in, const uint32_t* gather, int* out, int n, void* scratch,
+                          cudaStream_t stream) {
+    if (n < 0) return GSN_ERR_INVALID_ARGUMENT;
+    int* block_sums = static_cast<int*>(scratch);
+    int blocks = ceil_div(n > 0 ? n : 1, kScanChunk);
+    if (n > 0) scan_reduce<<<blocks, kScanThreads, 0, stream>>>(in, gather, n, block_sums);
+    else cudaMemsetAsync(block_sums, 0, sizeof(int), stream);
+    scan_block_sums<<<1, kScanThreads, 0, stream>>>(block_sums, n > 0 ? blocks : 0, out + n);
+    if (n > 0) scan_downsweep<<<blocks, kScanThreads, 0, stream>>>(in, gather, n, block_sums, out);
+    return launch_status();
+}
+
+int launch_emit_records(const uint32_t* sorted_ids, const int* record_start, const int4* rects, int n,
+                        int tile_count_x, uint32_t* tile_keys, uint32_t* record_ids, int64_t capacity,
+                        int* overflow, cudaStream_t stream) {
+    if (n <= 0) return GSN_OK;
+    emit_records<<<ceil_div(4ll * n, 256), 256, 0, stream>>>(sorted_ids, record_start, rects, n, tile_count_x,
+                                                             tile_keys, record_ids, capacity, overflow);
+    return launch_status();
+}
+
+int launch_tile_ranges(const uint32_t* sorted_tiles, const int* record_count_device, int max_records,
+                       int tile_count, int64_t* offsets, cudaStream_t stream) {
+    int64_t work = max_records > tile_count + 1 ? max_records : tile_count + 1;
+    int blocks = ceil_div(work, 256);
+    if (blocks > 148 * 32) blocks = 148 * 32;
+    tile_ranges<<<blocks, 256, 0, stream>>>(sorted_tiles, record_count_device, max_records, tile_count,
+                                           offsets);
+    return launch_status();
+}
+
+}  // namespace gsn

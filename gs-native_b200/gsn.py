@@ -1,0 +1,148 @@
+"""ctypes binding of libgsn_b200.so, the gs-native B200 C ABI (include/gsn.h).
+
+Python here is only the FFI plumbing that the tests and the benchmark use to
+drive the C ABI; device memory is passed as raw CUDA addresses (for example
+``torch.Tensor.data_ptr()``). Loading fails loudly when the compiled library is
+missing: there is no Python or CPU fallback for any stage.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgsn_b200.so")
+
+PARAM_COUNT = 58
+POSITION_INDEX, LOG_SCALE_INDEX, ROTATION_INDEX, OPACITY_INDEX, SH_INDEX = 0, 3, 6, 9, 10
+TILE = 16
+
+c_float_p = ctypes.POINTER(ctypes.c_float)
+
+
+class Camera(ctypes.Structure):
+    """Byte-compatible with gsn_camera / gs_native::CameraParams."""
+
+    _fields_ = [
+        ("fx", ctypes.c_float), ("fy", ctypes.c_float), ("cx", ctypes.c_float), ("cy", ctypes.c_float),
+        ("R_c_w", ctypes.c_float * 9), ("t_c_w", ctypes.c_float * 3),
+        ("near_depth", ctypes.c_float), ("far_depth", ctypes.c_float),
+        ("width", ctypes.c_int), ("height", ctypes.c_int),
+        ("pixel_offset", ctypes.c_int64),
+        ("tile_count_x", ctypes.c_int), ("tile_count_y", ctypes.c_int),
+        ("tile_offset", ctypes.c_int),
+    ]
+
+    @property
+    def tiles(self):
+        return self.tile_count_x * self.tile_count_y
+
+    @property
+    def pixels(self):
+        return self.width * self.height
+
+
+class RendererBuffers(ctypes.Structure):
+    _fields_ = [
+        ("means", ctypes.c_void_p), ("conic_opacity", ctypes.c_void_p), ("colors", ctypes.c_void_p),
+        ("depths", ctypes.c_void_p), ("rects", ctypes.c_void_p), ("tile_counts", ctypes.c_void_p),
+        ("radii", ctypes.c_void_p), ("tile_gaussian_ids", ctypes.c_void_p), ("tile_offsets", ctypes.c_void_p),
+        ("contributors", ctypes.c_void_p), ("record_count", ctypes.c_void_p), ("overflow", ctypes.c_void_p),
+        ("record_count_host", ctypes.c_int64), ("gaussian_capacity", ctypes.c_int),
+        ("tile_capacity", ctypes.c_int),
+    ]
+
+
+_lib = None
+
+
+class GsnError(RuntimeError):
+    pass
+
+
+def _check(status, what):
+    if status != 0:
+        raise GsnError(f"{what} failed with gsn status {status}")
+
+
+def lib():
+    """Loads libgsn_b200.so once; raises when it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise GsnError(f"{LIB_PATH} is missing: build it with `make -C {HERE}` (the CUDA path has no fallback)")
+    L = ctypes.CDLL(LIB_PATH)
+    vp, i32, i64, f32 = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_float
+    P = ctypes.POINTER
+    sig = {
+        "gsn_version": ([], ctypes.c_char_p),
+        "gsn_memcpy": ([vp, vp, ctypes.c_size_t], i32),
+        "gsn_stream_synchronize": ([vp], i32),
+        "gsn_renderer_create": ([P(vp)], i32),
+        "gsn_renderer_destroy": ([vp], i32),
+        "gsn_renderer_set_stream": ([vp, vp], i32),
+        "gsn_renderer_render": ([vp, vp, i32, P(Camera), c_float_p, vp, i32], i32),
+        "gsn_renderer_get_buffers": ([vp, P(RendererBuffers)], i32),
+        "gsn_renderer_record_offsets": ([vp, P(vp)], i32),
+        "gsn_renderer_set_record_capacity": ([vp, i64], i32),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = L
+    return L
+
+
+def declare(name, args, res=ctypes.c_int):
+    fn = getattr(lib(), name)
+    fn.argtypes = args
+    fn.restype = res
+    return fn
+
+
+def floats3(values):
+    return (ctypes.c_float * 3)(*[float(v) for v in values])
+
+
+class Renderer:
+    """Handle over gs_native::Renderer (reference renderer.h:10-89)."""
+
+    def __init__(self):
+        h = ctypes.c_void_p()
+        _check(lib().gsn_renderer_create(ctypes.byref(h)), "gsn_renderer_create")
+        self.handle = h
+
+    def close(self):
+        if self.handle:
+            lib().gsn_renderer_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream):
+        _check(lib().gsn_renderer_set_stream(self.handle, ctypes.c_void_p(stream)), "set_stream")
+
+    def render(self, params_ptr, count, camera, background, image_ptr, sh_degree):
+        return lib().gsn_renderer_render(self.handle, ctypes.c_void_p(params_ptr), int(count), ctypes.byref(camera),
+                                         floats3(background), ctypes.c_void_p(image_ptr), int(sh_degree))
+
+    def buffers(self):
+        b = RendererBuffers()
+        _check(lib().gsn_renderer_get_buffers(self.handle, ctypes.byref(b)), "get_buffers")
+        return b
+
+    def record_offsets(self):
+        p = ctypes.c_void_p()
+        _check(lib().gsn_renderer_record_offsets(self.handle, ctypes.byref(p)), "record_offsets")
+        return p.value
+
+    def set_record_capacity(self, records):
+        return lib().gsn_renderer_set_record_capacity(self.handle, int(records))
+
+
+def memcpy(dst, src, nbytes):
+    _check(lib().gsn_memcpy(ctypes.c_void_p(dst), ctypes.c_void_p(src), ctypes.c_size_t(nbytes)), "gsn_memcpy")

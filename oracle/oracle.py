@@ -1,0 +1,256 @@
+"""ctypes bindings of the CPU oracle (liboracle.so) and of the reference's own
+CUDA kernels compiled into _ref/libgsref.so.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by the smoke check and by the
+benchmark's CPU-baseline leg, never by the product.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_PATH = os.path.join(HERE, "liboracle.so")
+REF_PATH = os.path.join(HERE, "_ref", "libgsref.so")
+
+_vp, _i32, _i64, _f32, _f64, _u64 = (ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_float,
+                                     ctypes.c_double, ctypes.c_uint64)
+
+
+class Proj(ctypes.Structure):
+    _fields_ = [("visible", ctypes.c_int), ("rect", ctypes.c_int * 4), ("depth", _f64), ("u", _f64), ("v", _f64),
+                ("cov", _f64 * 3), ("conic", _f64 * 3), ("opacity", _f64), ("radius", _f64),
+                ("rgb", _f64 * 3), ("rgb_raw", _f64 * 3)]
+
+
+PROJ_DTYPE = np.dtype([("visible", np.int32), ("rect", np.int32, 4), ("depth", np.float64), ("u", np.float64),
+                       ("v", np.float64), ("cov", np.float64, 3), ("conic", np.float64, 3),
+                       ("opacity", np.float64), ("radius", np.float64), ("rgb", np.float64, 3),
+                       ("rgb_raw", np.float64, 3)], align=True)
+assert PROJ_DTYPE.itemsize == ctypes.sizeof(Proj)
+
+
+class LR(ctypes.Structure):
+    _fields_ = [("position", _f64), ("scale", _f64), ("rotation", _f64), ("opacity", _f64), ("sh_dc", _f64),
+                ("sh_rest", _f64)]
+
+
+REFERENCE_LR = dict(position=1e-4, scale=0.005, rotation=0.001, opacity=0.025, sh_dc=0.0025, sh_rest=0.0025 / 20)
+
+_orc = None
+_ref = None
+
+
+def ptr(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None else ctypes.c_void_p(0)
+
+
+def oracle():
+    global _orc
+    if _orc is None:
+        if not os.path.exists(ORACLE_PATH):
+            raise RuntimeError(f"{ORACLE_PATH} missing: run `make -C {HERE}`")
+        L = ctypes.CDLL(ORACLE_PATH)
+        from gsn import Camera  # noqa: F401 (same struct layout)
+        cp = ctypes.c_void_p
+        sigs = {
+            "orc_project": [cp, _i32, cp, _i32, cp],
+            "orc_sort_records": [cp, cp, cp, _i32, _i32, _i32, cp, cp],
+            "orc_tile_lists": [cp, _i32, cp, ctypes.POINTER(cp), ctypes.POINTER(cp)],
+            "orc_free": [cp],
+            "orc_render": [cp, cp, cp, cp, cp, cp, cp, cp, _i32, _i32],
+            "orc_loss": [cp, cp, _i32, _i32],
+            "orc_loss_gradient": [cp, cp, _i32, _i32, cp, _i32, _i32],
+            "orc_backward": [cp, _i32, cp, cp, cp, cp, cp, cp, cp, _i32, _i32],
+            "orc_projection_statistics": [cp, _i32, cp, cp, cp, cp, cp],
+            "orc_map_gradients": [cp, _i32, cp, _i32, cp, cp],
+            "orc_adam": [cp, cp, cp, cp, _i32, cp, _u64],
+            "orc_density_counts": [cp, _i32, cp, cp, cp, _f32, _f32, _f32, _f32, _i32, _f32, cp],
+            "orc_density_apply": [cp, _i32, cp, cp, cp, cp, cp],
+            "orc_knn3": [cp, _i32, cp, cp],
+            "orc_set_threads": [_i32],
+        }
+        res = {"orc_sort_records": _i64, "orc_loss": _f64, "orc_density_apply": _i32, "orc_set_threads": _i32}
+        for name, args in sigs.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res.get(name, None)
+        _orc = L
+    return _orc
+
+
+def ref_available():
+    return os.path.exists(REF_PATH)
+
+
+def reference():
+    """The reference's own CUDA kernels/classes (GPU only)."""
+    global _ref
+    if _ref is None:
+        if not ref_available():
+            raise RuntimeError(f"{REF_PATH} missing: run `make -C {HERE} ref` where the reference tree exists")
+        L = ctypes.CDLL(REF_PATH)
+        for name in dir(L):
+            pass
+        _ref = L
+    return _ref
+
+
+def ref_fn(name, args, res=ctypes.c_int):
+    fn = getattr(reference(), name)
+    fn.argtypes = args
+    fn.restype = res
+    return fn
+
+
+# ------------------------------------------------------------------ oracle API
+def cam_ref(cam):
+    return ctypes.byref(cam)
+
+
+def project(params, cam, sh_degree):
+    params = np.ascontiguousarray(params, dtype=np.float32)
+    n = params.shape[1]
+    out = np.zeros(n, dtype=PROJ_DTYPE)
+    oracle().orc_project(ptr(params), n, cam_ref(cam), sh_degree, ptr(out))
+    return out
+
+
+def sort_records(depth_bits, rects, counts, cam):
+    n = len(counts)
+    bits = np.ascontiguousarray(depth_bits, dtype=np.uint32)
+    rects = np.ascontiguousarray(rects, dtype=np.int32)
+    counts = np.ascontiguousarray(counts, dtype=np.int32)
+    total = int(np.sum(counts, dtype=np.int64))
+    ids = np.zeros(max(total, 1), dtype=np.int32)
+    offsets = np.zeros(cam.tile_count_x * cam.tile_count_y + 1, dtype=np.int64)
+    r = oracle().orc_sort_records(ptr(bits), ptr(rects), ptr(counts), n, cam.tile_count_x, cam.tile_count_y,
+                                  ptr(ids), ptr(offsets))
+    return ids[:r], offsets
+
+
+def tile_lists(proj, cam):
+    off = ctypes.c_void_p()
+    ids = ctypes.c_void_p()
+    oracle().orc_tile_lists(ptr(proj), len(proj), cam_ref(cam), ctypes.byref(off), ctypes.byref(ids))
+    tiles = cam.tile_count_x * cam.tile_count_y
+    offsets = np.ctypeslib.as_array(ctypes.cast(off, ctypes.POINTER(ctypes.c_int64)), shape=(tiles + 1,)).copy()
+    total = int(offsets[-1])
+    if total > 0:
+        idv = np.ctypeslib.as_array(ctypes.cast(ids, ctypes.POINTER(ctypes.c_int32)), shape=(total,)).copy()
+    else:
+        idv = np.zeros(0, dtype=np.int32)
+    oracle().orc_free(off)
+    oracle().orc_free(ids)
+    return offsets, idv
+
+
+def render(proj, cam, offsets, ids, background, tile_range=(0, 0)):
+    P = cam.width * cam.height
+    image = np.zeros(P * 3, dtype=np.float64)
+    final_t = np.zeros(P, dtype=np.float64)
+    contributors = np.zeros(P, dtype=np.int32)
+    bg = np.asarray(background, dtype=np.float64)
+    ids = np.ascontiguousarray(ids, dtype=np.int32) if len(ids) else np.zeros(1, dtype=np.int32)
+    offsets = np.ascontiguousarray(offsets, dtype=np.int64)
+    oracle().orc_render(ptr(proj), cam_ref(cam), ptr(offsets), ptr(ids), ptr(bg), ptr(image), ptr(final_t),
+                        ptr(contributors), tile_range[0], tile_range[1])
+    return image.reshape(cam.height, cam.width, 3), final_t.reshape(cam.height, cam.width), \
+        contributors.reshape(cam.height, cam.width)
+
+
+def render_params(params, cam, background, sh_degree):
+    proj = project(params, cam, sh_degree)
+    offsets, ids = tile_lists(proj, cam)
+    return render(proj, cam, offsets, ids, background)[0]
+
+
+def loss(image, target):
+    image = np.ascontiguousarray(image, dtype=np.float64)
+    target = np.ascontiguousarray(target, dtype=np.uint8)
+    h, w = target.shape[:2]
+    return oracle().orc_loss(ptr(image), ptr(target), w, h)
+
+
+def loss_gradient(image, target, rows=(0, 0)):
+    image = np.ascontiguousarray(image, dtype=np.float64)
+    target = np.ascontiguousarray(target, dtype=np.uint8)
+    h, w = target.shape[:2]
+    g = np.zeros((h, w, 3), dtype=np.float64)
+    oracle().orc_loss_gradient(ptr(image), ptr(target), w, h, ptr(g), rows[0], rows[1])
+    return g
+
+
+def backward(proj, cam, offsets, ids, image, image_gradient, tile_range=(0, 0)):
+    n = len(proj)
+    g9 = np.zeros((9, n), dtype=np.float64)
+    a2 = np.zeros((2, n), dtype=np.float64)
+    ids = np.ascontiguousarray(ids, dtype=np.int32) if len(ids) else np.zeros(1, dtype=np.int32)
+    offsets = np.ascontiguousarray(offsets, dtype=np.int64)
+    image = np.ascontiguousarray(image, dtype=np.float64)
+    image_gradient = np.ascontiguousarray(image_gradient, dtype=np.float64)
+    oracle().orc_backward(ptr(proj), n, cam_ref(cam), ptr(offsets), ptr(ids), ptr(image), ptr(image_gradient),
+                          ptr(g9), ptr(a2), tile_range[0], tile_range[1])
+    return g9, a2
+
+
+def projection_statistics(proj, cam, g9, a2):
+    n = len(proj)
+    stats = np.zeros((2, n), dtype=np.float64)
+    abs_stats = np.zeros(n, dtype=np.float64)
+    oracle().orc_projection_statistics(ptr(proj), n, cam_ref(cam), ptr(g9), ptr(a2), ptr(stats), ptr(abs_stats))
+    return stats, abs_stats
+
+
+def map_gradients(params, cam, sh_degree, g9):
+    params = np.ascontiguousarray(params, dtype=np.float32)
+    n = params.shape[1]
+    g58 = np.zeros((58, n), dtype=np.float64)
+    g9 = np.ascontiguousarray(g9, dtype=np.float64)
+    oracle().orc_map_gradients(ptr(params), n, cam_ref(cam), sh_degree, ptr(g9), ptr(g58))
+    return g58
+
+
+def adam(params, m, v, g58, lr, step):
+    lrs = LR(**lr)
+    oracle().orc_adam(ptr(params), ptr(m), ptr(v), ptr(g58), params.shape[1], ctypes.byref(lrs), step)
+
+
+def density_counts(params, grad_sums, abs_sums, obs, grad_thr, split_thr, min_opacity, max_world, prune_large,
+                   abs_thr):
+    params = np.ascontiguousarray(params, dtype=np.float32)
+    n = params.shape[1]
+    out = np.zeros((n, 4), dtype=np.int32)
+    grad_sums = np.ascontiguousarray(grad_sums, dtype=np.float32)
+    abs_sums = np.ascontiguousarray(abs_sums, dtype=np.float32)
+    obs = np.ascontiguousarray(obs, dtype=np.uint32)
+    oracle().orc_density_counts(ptr(params), n, ptr(grad_sums), ptr(abs_sums), ptr(obs), grad_thr, split_thr,
+                                min_opacity, max_world, int(prune_large), abs_thr, ptr(out))
+    return out
+
+
+def density_apply(params, counts4, samples):
+    params = np.ascontiguousarray(params, dtype=np.float32)
+    n = params.shape[1]
+    total = int(counts4[:, 0].sum() + counts4[:, 1].sum() + 2 * counts4[:, 3].sum())
+    out = np.zeros((58, max(total, 1)), dtype=np.float32)
+    parents = np.zeros(max(total, 1), dtype=np.int32)
+    hist = np.zeros(max(total, 1), dtype=np.int32)
+    counts4 = np.ascontiguousarray(counts4, dtype=np.int32)
+    samples = np.ascontiguousarray(samples, dtype=np.float32)
+    m = oracle().orc_density_apply(ptr(params), n, ptr(counts4), ptr(samples), ptr(out), ptr(parents), ptr(hist))
+    return out[:, :m], parents[:m], hist[:m]
+
+
+def knn3(points):
+    points = np.ascontiguousarray(points, dtype=np.float32)
+    n = points.shape[0]
+    d = np.zeros(n, dtype=np.float64)
+    nb = np.zeros((n, 3), dtype=np.int32)
+    if n:
+        oracle().orc_knn3(ptr(points), n, ptr(d), ptr(nb))
+    return d, nb
+
+
+def set_threads(k):
+    return oracle().orc_set_threads(int(k))
