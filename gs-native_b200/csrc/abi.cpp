@@ -6,14 +6,30 @@
 #include <new>
 
 #include "core/render/renderer.h"
+#include "core/solver/solver.h"
 
 struct gsn_renderer {
     gs_native::Renderer impl;
 };
 
+struct gsn_solver {
+    gs_native::Solver impl;
+};
+
 namespace {
 
 inline cudaStream_t AsStream(void* s) { return static_cast<cudaStream_t>(s); }
+
+inline const gs_native::CameraParams& AsCamera(const gsn_camera* c) {
+    return *reinterpret_cast<const gs_native::CameraParams*>(c);
+}
+
+inline gs_native::GaussianBuffers View(const float* params, int count) {
+    gs_native::GaussianBuffers g;
+    g.gaussians_ = const_cast<float*>(params);
+    g.gaussian_count_ = count;
+    return g;
+}
 
 }  // namespace
 
@@ -88,6 +104,115 @@ int gsn_renderer_record_offsets(gsn_renderer* r, const int** out) {
 int gsn_renderer_set_record_capacity(gsn_renderer* r, int64_t records) {
     if (!r) return GSN_ERR_INVALID_ARGUMENT;
     return r->impl.SetRecordCapacity(records) ? GSN_OK : GSN_ERR_INVALID_ARGUMENT;
+}
+
+int gsn_solver_create(gsn_solver** out) {
+    if (!out) return GSN_ERR_INVALID_ARGUMENT;
+    *out = new (std::nothrow) gsn_solver();
+    return *out ? GSN_OK : GSN_ERR_OUT_OF_MEMORY;
+}
+
+int gsn_solver_destroy(gsn_solver* s) {
+    delete s;
+    return GSN_OK;
+}
+
+int gsn_solver_set_stream(gsn_solver* s, void* stream) {
+    if (!s) return GSN_ERR_INVALID_ARGUMENT;
+    s->impl.SetStream(AsStream(stream));
+    return GSN_OK;
+}
+
+int gsn_solver_iterate(gsn_solver* s, const gsn_camera* camera, gsn_renderer* renderer, const float* image,
+                       const uint8_t* target, float* params, int count, float position_lr, int sh_degree) {
+    if (!s || !camera || !renderer) return GSN_ERR_INVALID_ARGUMENT;
+    gs_native::GaussianBuffers g = View(params, count);
+    return s->impl.Iterate(AsCamera(camera), renderer->impl, image, target, g, position_lr, sh_degree)
+               ? GSN_OK
+               : GSN_ERR_INVALID_ARGUMENT;
+}
+
+int gsn_solver_reset_opacity_history(gsn_solver* s) {
+    if (!s) return GSN_ERR_INVALID_ARGUMENT;
+    return s->impl.ResetOpacityHistory() ? GSN_OK : GSN_ERR_CUDA;
+}
+
+int gsn_solver_remap(gsn_solver* s, const int* parent_ids, int count) {
+    if (!s) return GSN_ERR_INVALID_ARGUMENT;
+    return s->impl.RemapGaussians(parent_ids, count) ? GSN_OK : GSN_ERR_INVALID_ARGUMENT;
+}
+
+int gsn_solver_statistics(gsn_solver* s, const float** stats, const float** absolute_stats) {
+    if (!s || !stats || !absolute_stats) return GSN_ERR_INVALID_ARGUMENT;
+    *stats = s->impl.GetProjectionStatistics();
+    *absolute_stats = s->impl.GetAbsoluteProjectionStatistics();
+    return GSN_OK;
+}
+
+int gsn_solver_set_learning_rates(gsn_solver* s, float scale, float rotation, float opacity, float sh_dc,
+                                  float sh_rest) {
+    if (!s) return GSN_ERR_INVALID_ARGUMENT;
+    gs_native::LearningRates lr;
+    lr.scale = scale;
+    lr.rotation = rotation;
+    lr.opacity = opacity;
+    lr.sh_dc = sh_dc;
+    lr.sh_rest = sh_rest;
+    s->impl.SetLearningRates(lr);
+    return GSN_OK;
+}
+
+int gsn_solver_set_compute_loss(gsn_solver* s, int enabled) {
+    if (!s) return GSN_ERR_INVALID_ARGUMENT;
+    s->impl.SetComputeLoss(enabled != 0);
+    return GSN_OK;
+}
+
+int gsn_solver_loss(gsn_solver* s, double* out) {
+    if (!s || !out || !s->impl.GetLossDevice()) return GSN_ERR_INVALID_ARGUMENT;
+    return cudaMemcpy(out, s->impl.GetLossDevice(), 4 * sizeof(double), cudaMemcpyDeviceToHost) == cudaSuccess
+               ? GSN_OK
+               : GSN_ERR_CUDA;
+}
+
+int gsn_solver_loss_device(gsn_solver* s, const double** out) {
+    if (!s || !out) return GSN_ERR_INVALID_ARGUMENT;
+    *out = s->impl.GetLossDevice();
+    return *out ? GSN_OK : GSN_ERR_INVALID_ARGUMENT;
+}
+
+int gsn_solver_image_gradients(gsn_solver* s, const gsn_camera* camera, const float* image, const uint8_t* target,
+                               const float** out) {
+    if (!s || !camera || !out) return GSN_ERR_INVALID_ARGUMENT;
+    if (!s->impl.ComputeImageGradients(AsCamera(camera), image, target)) return GSN_ERR_INVALID_ARGUMENT;
+    *out = s->impl.GetImageGradients();
+    return GSN_OK;
+}
+
+int gsn_solver_screen_gradients(gsn_solver* s, const gsn_camera* camera, gsn_renderer* renderer,
+                                const float* image, const float* params, int count, const float** out) {
+    if (!s || !camera || !renderer || !out) return GSN_ERR_INVALID_ARGUMENT;
+    if (!s->impl.ComputeScreenGradients(AsCamera(camera), renderer->impl, View(params, count), image))
+        return GSN_ERR_INVALID_ARGUMENT;
+    *out = s->impl.GetScreenGradients();
+    return GSN_OK;
+}
+
+int gsn_solver_map_gradients(gsn_solver* s, const gsn_camera* camera, gsn_renderer* renderer, float* params,
+                             int count, int sh_degree, float* grads_out) {
+    if (!s || !camera || !renderer || !grads_out) return GSN_ERR_INVALID_ARGUMENT;
+    gs_native::GaussianBuffers g = View(params, count);
+    return s->impl.UpdateGaussians(AsCamera(camera), renderer->impl, g, 0.0f, sh_degree, false, grads_out)
+               ? GSN_OK
+               : GSN_ERR_INVALID_ARGUMENT;
+}
+
+int gsn_solver_moments(gsn_solver* s, float** first, float** second, uint64_t* iteration) {
+    if (!s || !first || !second || !iteration) return GSN_ERR_INVALID_ARGUMENT;
+    *first = s->impl.GetFirstMoments();
+    *second = s->impl.GetSecondMoments();
+    *iteration = s->impl.GetIteration();
+    return GSN_OK;
 }
 
 }  // extern "C"

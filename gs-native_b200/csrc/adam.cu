@@ -1,0 +1,353 @@
+// (f) Per-Gaussian update: view-space statistics, chain rule from the
+// screen-space gradients to the 58 parameters, and Adam - fused into one pass
+// over the SoA parameter block.
+//
+// The reference runs these as four launches around a 58 x N gradient buffer
+// that is zeroed, written in place and read back (solver.cu:468-689, 862-923).
+// Here one thread owns one Gaussian: it reads its 12 screen-space values, keeps
+// the 58 parameter gradients in registers (the SH ones are formed on the fly as
+// dL/dcolour * basis) and streams p, m, v once. That removes the 58 x N gradient
+// round trip (3 x 232 B per Gaussian) from the largest HBM consumer of the step.
+//
+// The chain-rule arithmetic mirrors MapGaussianGradientsKernel (solver.cu:492-623)
+// expression for expression, so for identical screen-space input the mapped
+// gradients are bit-identical to the reference's; Adam follows
+// UpdateGaussiansKernel (solver.cu:651-689).
+#include "common.cuh"
+#include "kernels.h"
+
+namespace gsn {
+
+namespace {
+
+struct Chain {
+    float g[10];      // position 0-2, log-scale 3-5, axis-angle 6-8, opacity 9
+    float basis[16];  // SH basis at the view direction
+    float grgb[3];    // dL/dcolour, zero where the unclamped colour is negative
+};
+
+template <int D>
+__device__ __forceinline__ void sh_with_derivatives(const float* __restrict__ p, int64_t N, int i, const gsn_camera& cam,
+                                                    float* basis, float* color, float* dcol) {
+    constexpr int s = (D + 1) * (D + 1);
+    float dir[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        dir[a] = p[a * N + i];
+#pragma unroll
+        for (int b = 0; b < 3; ++b) dir[a] += cam.R_c_w[b * 3 + a] * cam.t_c_w[b];
+    }
+    float il = rsqrtf(dir[0] * dir[0] + dir[1] * dir[1] + dir[2] * dir[2]);
+    float x = dir[0] * il, y = dir[1] * il, z = dir[2] * il;
+    float der[s * 3];
+#pragma unroll
+    for (int k = 0; k < s * 3; ++k) der[k] = 0.0f;
+    basis[0] = kSh0;
+    if (D >= 1) {
+        basis[1] = -kSh1 * y;
+        basis[2] = kSh1 * z;
+        basis[3] = -kSh1 * x;
+        der[4] = -kSh1;
+        der[8] = kSh1;
+        der[9] = -kSh1;
+    }
+    if (D >= 2) {
+        constexpr float c = kSh2a, d = kSh2b, e = kSh2c;
+        basis[4] = c * x * y;
+        basis[5] = -c * y * z;
+        basis[6] = d * (2 * z * z - x * x - y * y);
+        basis[7] = -c * x * z;
+        basis[8] = e * (x * x - y * y);
+        der[12] = c * y;
+        der[13] = c * x;
+        der[16] = -c * z;
+        der[17] = -c * y;
+        der[18] = -2 * d * x;
+        der[19] = -2 * d * y;
+        der[20] = 4 * d * z;
+        der[21] = -c * z;
+        der[23] = -c * x;
+        der[24] = 2 * e * x;
+        der[25] = -2 * e * y;
+    }
+    if (D >= 3) {
+        constexpr float a = -kSh3a, b = kSh3b, c = -kSh3c, d = kSh3d, e = kSh3e;
+        basis[9] = a * y * (3 * x * x - y * y);
+        basis[10] = b * x * y * z;
+        basis[11] = c * y * (4 * z * z - x * x - y * y);
+        basis[12] = d * z * (2 * z * z - 3 * x * x - 3 * y * y);
+        basis[13] = c * x * (4 * z * z - x * x - y * y);
+        basis[14] = e * z * (x * x - y * y);
+        basis[15] = a * x * (x * x - 3 * y * y);
+        der[27] = 6 * a * x * y;
+        der[28] = 3 * a * (x * x - y * y);
+        der[30] = b * y * z;
+        der[31] = b * x * z;
+        der[32] = b * x * y;
+        der[33] = -2 * c * x * y;
+        der[34] = c * (4 * z * z - x * x - 3 * y * y);
+        der[35] = 8 * c * y * z;
+        der[36] = -6 * d * x * z;
+        der[37] = -6 * d * y * z;
+        der[38] = d * (6 * z * z - 3 * x * x - 3 * y * y);
+        der[39] = c * (4 * z * z - 3 * x * x - y * y);
+        der[40] = -2 * c * x * y;
+        der[41] = 8 * c * x * z;
+        der[42] = 2 * e * x * z;
+        der[43] = -2 * e * y * z;
+        der[44] = e * (x * x - y * y);
+        der[45] = 3 * a * (x * x - y * y);
+        der[46] = -6 * a * x * y;
+    }
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch) {
+        float value = 0.0f;
+        float dv[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll
+        for (int j = 0; j < s; ++j) {
+            float coef = p[(GSN_SH_INDEX + ch * kShStride + j) * N + i];
+            value += coef * basis[j];
+#pragma unroll
+            for (int a2 = 0; a2 < 3; ++a2) dv[a2] += coef * der[j * 3 + a2];
+        }
+        color[ch] = value + 0.5f;
+        float radial = dv[0] * x + dv[1] * y + dv[2] * z;
+        dcol[ch * 3] = (dv[0] - radial * x) * il;
+        dcol[ch * 3 + 1] = (dv[1] - radial * y) * il;
+        dcol[ch * 3 + 2] = (dv[2] - radial * z) * il;
+    }
+}
+
+// Chain rule of solver.cu:512-622 for one Gaussian with screen gradients in[0..8].
+template <int D>
+__device__ __forceinline__ void chain_rule(const float* __restrict__ p, int64_t N, int i, const gsn_camera& cam,
+                                           const float in[9], Chain& out) {
+    float rot[9], crot[9], cov[9], pos[3], s2[3];
+    axis_angle_to_matrix(p[(GSN_ROTATION_INDEX + 0) * N + i], p[(GSN_ROTATION_INDEX + 1) * N + i],
+                         p[(GSN_ROTATION_INDEX + 2) * N + i], rot);
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        pos[r] = cam.t_c_w[r];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            pos[r] += cam.R_c_w[r * 3 + c] * p[static_cast<int64_t>(c) * N + i];
+            crot[r * 3 + c] = cam.R_c_w[r * 3] * rot[c] + cam.R_c_w[r * 3 + 1] * rot[3 + c] +
+                              cam.R_c_w[r * 3 + 2] * rot[6 + c];
+        }
+        float sc = expf(p[static_cast<int64_t>(GSN_LOG_SCALE_INDEX + r) * N + i]);
+        s2[r] = sc * sc;
+    }
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            cov[r * 3 + c] = 0;
+#pragma unroll
+            for (int j = 0; j < 3; ++j) cov[r * 3 + c] += crot[r * 3 + j] * s2[j] * crot[c * 3 + j];
+        }
+    float iz = 1.0f / pos[2];
+    float nx = pos[0] * iz, ny = pos[1] * iz;
+    float lx = 1.3f * 0.5f * cam.width / cam.fx;
+    float ly = 1.3f * 0.5f * cam.height / cam.fy;
+    float jx = fminf(fmaxf(nx, -lx), lx);
+    float jy = fminf(fmaxf(ny, -ly), ly);
+    float P[6] = {cam.fx * iz, 0, -cam.fx * jx * iz, 0, cam.fy * iz, -cam.fy * jy * iz};
+    float PV[6] = {}, LP[6] = {};
+#pragma unroll
+    for (int r = 0; r < 2; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                PV[r * 3 + c] += P[r * 3 + j] * cov[j * 3 + c];
+                LP[r * 3 + c] += P[r * 3 + j] * crot[j * 3 + c];
+            }
+    float color[3], dcol[9];
+    sh_with_derivatives<D>(p, N, i, cam, out.basis, color, dcol);
+    float right[3];
+#pragma unroll
+    for (int axis = 0; axis < 3; ++axis) {
+        float dx = cam.R_c_w[axis], dy = cam.R_c_w[3 + axis], dz = cam.R_c_w[6 + axis];
+        float du = (dx - nx * dz) * iz;
+        float dv = (dy - ny * dz) * iz;
+        float djx = nx >= -lx && nx <= lx ? du : 0;
+        float djy = ny >= -ly && ny <= ly ? dv : 0;
+        float delta[6] = {-cam.fx * dz * iz * iz, 0, -cam.fx * (djx - jx * dz * iz) * iz,
+                          0, -cam.fy * dz * iz * iz, -cam.fy * (djy - jy * dz * iz) * iz};
+        float daa = 0, dab = 0, ddd = 0;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            daa += 2 * delta[j] * PV[j];
+            dab += delta[j] * PV[3 + j] + delta[3 + j] * PV[j];
+            ddd += 2 * delta[3 + j] * PV[3 + j];
+        }
+        float cg = in[0] * cam.fx * du + in[1] * cam.fy * dv + in[2] * daa + in[3] * dab + in[4] * ddd;
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            if (color[c] >= 0) cg += in[6 + c] * dcol[c * 3 + axis];
+        out.g[axis] = cg;
+        float la = LP[axis], lb = LP[3 + axis];
+        out.g[3 + axis] = 2 * s2[axis] * (in[2] * la * la + in[3] * la * lb + in[4] * lb * lb);
+        int j = (axis + 1) % 3, k = (axis + 2) % 3;
+        float diff = s2[j] - s2[k];
+        right[axis] = diff * (2 * in[2] * LP[j] * LP[k] + in[3] * (LP[j] * LP[3 + k] + LP[k] * LP[3 + j]) +
+                              2 * in[4] * LP[3 + j] * LP[3 + k]);
+    }
+    float w[3];
+    float th2 = 0;
+#pragma unroll
+    for (int axis = 0; axis < 3; ++axis) {
+        w[axis] = p[static_cast<int64_t>(GSN_ROTATION_INDEX + axis) * N + i];
+        th2 += w[axis] * w[axis];
+    }
+    float ca = 0.5f, cb = 1.0f / 6.0f;
+    if (th2 > 1e-4f) {
+        float th = sqrtf(th2);
+        float hs = sinf(0.5f * th) / (0.5f * th);
+        ca = 0.5f * hs * hs;
+        cb = (th - sinf(th)) / (th2 * th);
+    } else {
+        ca -= th2 / 24.0f;
+        cb -= th2 / 120.0f;
+    }
+    float cr[3];
+#pragma unroll
+    for (int axis = 0; axis < 3; ++axis) {
+        int j = (axis + 1) % 3, k = (axis + 2) % 3;
+        cr[axis] = w[j] * right[k] - w[k] * right[j];
+    }
+#pragma unroll
+    for (int axis = 0; axis < 3; ++axis) {
+        int j = (axis + 1) % 3, k = (axis + 2) % 3;
+        out.g[6 + axis] = right[axis] + ca * cr[axis] + cb * (w[j] * cr[k] - w[k] * cr[j]);
+    }
+    out.g[9] = in[5];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) out.grgb[c] = color[c] >= 0 ? in[6 + c] : 0.0f;
+}
+
+__device__ __forceinline__ float row_lr(const GaussianUpdateArgs& a, int row) {
+    if (row < GSN_LOG_SCALE_INDEX) return a.lr[0];
+    if (row < GSN_ROTATION_INDEX) return a.lr[1];
+    if (row < GSN_OPACITY_INDEX) return a.lr[2];
+    if (row < GSN_SH_INDEX) return a.lr[3];
+    return (row - GSN_SH_INDEX) % kShStride == 0 ? a.lr[4] : a.lr[5];
+}
+
+__device__ __forceinline__ void adam_row(const GaussianUpdateArgs& a, int row, int64_t idx, float g) {
+    float first = 0.9f * a.m[idx] + 0.1f * g;
+    float second = 0.999f * a.v[idx] + 0.001f * g * g;
+    a.m[idx] = first;
+    a.v[idx] = second;
+    a.params[idx] -= row_lr(a, row) * (first * a.c1) / (sqrtf(second * a.c2) + 1e-15f);
+}
+
+template <int D>
+__global__ void __launch_bounds__(256) gaussian_update_kernel(GaussianUpdateArgs a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const int64_t N = a.n;
+    const float4* sg = reinterpret_cast<const float4*>(a.screen + static_cast<int64_t>(i) * 12);
+    float4 s0 = sg[0], s1 = sg[1], s2 = sg[2];
+    float in[9] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y, s1.z, s1.w, s2.x};
+    float adu = s2.y, adv = s2.z;
+    const bool visible = a.tile_counts[i] > 0;
+
+    // view-space statistics (solver.cu:468-490) and round accumulation
+    // (density_controller.cu:280-295)
+    float x = in[0] * (0.5f * a.cam.width);
+    float y = in[1] * (0.5f * a.cam.height);
+    float ax = adu * (0.5f * a.cam.width);
+    float ay = adv * (0.5f * a.cam.height);
+    float signed_len = sqrtf(x * x + y * y);
+    float abs_len = sqrtf(ax * ax + ay * ay);
+    if (a.stats) {
+        a.stats[i] = signed_len;
+        a.stats[N + i] = visible ? 1.0f : 0.0f;
+    }
+    if (a.abs_stats) {
+        a.abs_stats[i] = abs_len;
+        a.abs_stats[N + i] = adv;
+    }
+    if (a.grad_sums) {
+        a.grad_sums[i] += signed_len;
+        a.abs_sums[i] += abs_len;
+        a.obs_counts[i] += visible ? 1u : 0u;
+    }
+
+    bool active = false;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) active = active || in[k] != 0.0f;
+    Chain ch;
+    if (active) {
+        chain_rule<D>(a.params, N, i, a.cam, in, ch);
+    } else {
+#pragma unroll
+        for (int k = 0; k < 10; ++k) ch.g[k] = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 16; ++k) ch.basis[k] = 0.0f;
+        ch.grgb[0] = ch.grgb[1] = ch.grgb[2] = 0.0f;
+    }
+    constexpr int K = (D + 1) * (D + 1);
+    if (a.grads_out) {
+#pragma unroll
+        for (int r = 0; r < 10; ++r) a.grads_out[r * N + i] = ch.g[r];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int k = 0; k < kShStride; ++k)
+                a.grads_out[(GSN_SH_INDEX + c * kShStride + k) * N + i] = k < K ? ch.grgb[c] * ch.basis[k] : 0.0f;
+    }
+    if (!a.m) return;
+#pragma unroll
+    for (int r = 0; r < 10; ++r) adam_row(a, r, r * N + i, ch.g[r]);
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int k = 0; k < kShStride; ++k) {
+            int row = GSN_SH_INDEX + c * kShStride + k;
+            adam_row(a, row, row * N + i, k < K ? ch.grgb[c] * ch.basis[k] : 0.0f);
+        }
+}
+
+__global__ void remap_moments_kernel(const int* __restrict__ parents, const float* __restrict__ prev_m,
+                                     const float* __restrict__ prev_v, float* __restrict__ m, float* __restrict__ v,
+                                     int prev_count, int count) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const int row = blockIdx.y;
+    const int parent = parents ? parents[i] : -1;
+    const int64_t dst = static_cast<int64_t>(row) * count + i;
+    if (parent >= 0 && parent < prev_count) {
+        const int64_t src = static_cast<int64_t>(row) * prev_count + parent;
+        m[dst] = prev_m[src];
+        v[dst] = prev_v[src];
+    } else {
+        m[dst] = 0.0f;
+        v[dst] = 0.0f;
+    }
+}
+
+}  // namespace
+
+int launch_gaussian_update(const GaussianUpdateArgs& a, int sh_degree, cudaStream_t stream) {
+    if (a.n <= 0) return GSN_OK;
+    dim3 grid(ceil_div(a.n, 256));
+    switch (sh_degree < 0 ? 0 : (sh_degree > 3 ? 3 : sh_degree)) {
+        case 0: gaussian_update_kernel<0><<<grid, 256, 0, stream>>>(a); break;
+        case 1: gaussian_update_kernel<1><<<grid, 256, 0, stream>>>(a); break;
+        case 2: gaussian_update_kernel<2><<<grid, 256, 0, stream>>>(a); break;
+        default: gaussian_update_kernel<3><<<grid, 256, 0, stream>>>(a); break;
+    }
+    return launch_status();
+}
+
+int launch_remap_moments(const int* parents, const float* prev_m, const float* prev_v, float* m, float* v,
+                         int prev_count, int count, cudaStream_t stream) {
+    if (count <= 0) return GSN_OK;
+    dim3 grid(ceil_div(count, 256), kParams);
+    remap_moments_kernel<<<grid, 256, 0, stream>>>(parents, prev_m, prev_v, m, v, prev_count, count);
+    return launch_status();
+}
+
+}  // namespace gsn

@@ -78,4 +78,53 @@ struct RasterForwardArgs {
 };
 int launch_raster_forward(const RasterForwardArgs& a, cudaStream_t stream);
 
+// ---------------------------------------------------------------- loss
+// dL/dimage of 0.8 * L1 + 0.2 * (1 - SSIM) for an fp32 HWC image against a u8
+// HWC target. `sums` (optional, 3 doubles, zeroed by the launcher) receives
+// sum|I - T|, sum SSIM and sum (I - T)^2 in FP64.
+int launch_loss_gradient(const float* image, const uint8_t* target, float* grad, int width, int height,
+                         double* sums, cudaStream_t stream);
+// out[0..3] = loss, mean L1, mean SSIM, PSNR (dB) from the sums above.
+int launch_finalize_loss(const double* sums, int width, int height, double* out, cudaStream_t stream);
+
+// ---------------------------------------------------------------- backward
+struct RasterBackwardArgs {
+    const uint32_t* tile_ids;
+    const int64_t* tile_offsets;
+    const float2* means;
+    const float4* conic_opacity;
+    const float3* colors;
+    const float* image;        // final colours of the forward pass
+    const float* image_grad;   // dL/dimage
+    const int* contributors;   // per-pixel record bound from the forward pass (optional)
+    gsn_camera cam;
+    float* grad_out;           // [N][12] screen-space accumulators, zeroed by the caller
+};
+int launch_raster_backward(const RasterBackwardArgs& a, cudaStream_t stream);
+
+// ---------------------------------------------------------------- update
+struct GaussianUpdateArgs {
+    float* params;            // 58 x n SoA, updated in place by Adam
+    float* m;                 // Adam first moments (null: no Adam step)
+    float* v;                 // Adam second moments
+    const float* screen;      // [n][12] from the backward pass
+    const int* tile_counts;   // [n] visibility of the frame
+    gsn_camera cam;
+    int n;
+    float lr[6];              // position, log-scale, rotation, opacity, SH DC, SH rest
+    float c1, c2;             // Adam bias corrections 1/(1-b1^t), 1/(1-b2^t)
+    float* stats;             // optional 2 x n: view-space gradient norm, visible
+    float* abs_stats;         // optional 2 x n: norm of the absolute sums, sum|dv|
+    float* grad_sums;         // optional density accumulators (all three or none)
+    float* abs_sums;
+    unsigned int* obs_counts;
+    float* grads_out;         // optional 58 x n mapped parameter gradients
+};
+int launch_gaussian_update(const GaussianUpdateArgs& a, int sh_degree, cudaStream_t stream);
+
+// Adam history gather after densification: row r of the new moments takes the
+// parent's entry, or zero for parent -1 / out of range.
+int launch_remap_moments(const int* parents, const float* prev_m, const float* prev_v, float* m, float* v,
+                         int prev_count, int count, cudaStream_t stream);
+
 }  // namespace gsn

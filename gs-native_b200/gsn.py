@@ -84,6 +84,21 @@ def lib():
         "gsn_renderer_get_buffers": ([vp, P(RendererBuffers)], i32),
         "gsn_renderer_record_offsets": ([vp, P(vp)], i32),
         "gsn_renderer_set_record_capacity": ([vp, i64], i32),
+        "gsn_solver_create": ([P(vp)], i32),
+        "gsn_solver_destroy": ([vp], i32),
+        "gsn_solver_set_stream": ([vp, vp], i32),
+        "gsn_solver_iterate": ([vp, P(Camera), vp, vp, vp, vp, i32, f32, i32], i32),
+        "gsn_solver_reset_opacity_history": ([vp], i32),
+        "gsn_solver_remap": ([vp, vp, i32], i32),
+        "gsn_solver_statistics": ([vp, P(vp), P(vp)], i32),
+        "gsn_solver_set_learning_rates": ([vp, f32, f32, f32, f32, f32], i32),
+        "gsn_solver_set_compute_loss": ([vp, i32], i32),
+        "gsn_solver_loss": ([vp, P(ctypes.c_double)], i32),
+        "gsn_solver_loss_device": ([vp, P(vp)], i32),
+        "gsn_solver_image_gradients": ([vp, P(Camera), vp, vp, P(vp)], i32),
+        "gsn_solver_screen_gradients": ([vp, P(Camera), vp, vp, vp, i32, P(vp)], i32),
+        "gsn_solver_map_gradients": ([vp, P(Camera), vp, vp, i32, i32, vp], i32),
+        "gsn_solver_moments": ([vp, P(vp), P(vp), P(ctypes.c_uint64)], i32),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -146,3 +161,81 @@ class Renderer:
 
 def memcpy(dst, src, nbytes):
     _check(lib().gsn_memcpy(ctypes.c_void_p(dst), ctypes.c_void_p(src), ctypes.c_size_t(nbytes)), "gsn_memcpy")
+
+
+class Solver:
+    """Handle over gs_native::Solver (reference solver.h:11-68)."""
+
+    def __init__(self):
+        h = ctypes.c_void_p()
+        _check(lib().gsn_solver_create(ctypes.byref(h)), "gsn_solver_create")
+        self.handle = h
+
+    def close(self):
+        if self.handle:
+            lib().gsn_solver_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream):
+        _check(lib().gsn_solver_set_stream(self.handle, ctypes.c_void_p(stream)), "set_stream")
+
+    def iterate(self, camera, renderer, image_ptr, target_ptr, params_ptr, count, position_lr, sh_degree):
+        return lib().gsn_solver_iterate(self.handle, ctypes.byref(camera), renderer.handle, ctypes.c_void_p(image_ptr),
+                                        ctypes.c_void_p(target_ptr), ctypes.c_void_p(params_ptr), int(count),
+                                        float(position_lr), int(sh_degree))
+
+    def reset_opacity_history(self):
+        return lib().gsn_solver_reset_opacity_history(self.handle)
+
+    def remap(self, parents_ptr, count):
+        return lib().gsn_solver_remap(self.handle, ctypes.c_void_p(parents_ptr), int(count))
+
+    def statistics(self):
+        a, b = ctypes.c_void_p(), ctypes.c_void_p()
+        _check(lib().gsn_solver_statistics(self.handle, ctypes.byref(a), ctypes.byref(b)), "statistics")
+        return a.value, b.value
+
+    def set_learning_rates(self, scale, rotation, opacity, sh_dc, sh_rest):
+        _check(lib().gsn_solver_set_learning_rates(self.handle, scale, rotation, opacity, sh_dc, sh_rest), "lr")
+
+    def set_compute_loss(self, enabled=True):
+        _check(lib().gsn_solver_set_compute_loss(self.handle, int(bool(enabled))), "set_compute_loss")
+
+    def loss(self):
+        out = (ctypes.c_double * 4)()
+        _check(lib().gsn_solver_loss(self.handle, out), "loss")
+        return list(out)
+
+    def loss_device(self):
+        p = ctypes.c_void_p()
+        _check(lib().gsn_solver_loss_device(self.handle, ctypes.byref(p)), "loss_device")
+        return p.value
+
+    def image_gradients(self, camera, image_ptr, target_ptr):
+        p = ctypes.c_void_p()
+        _check(lib().gsn_solver_image_gradients(self.handle, ctypes.byref(camera), ctypes.c_void_p(image_ptr),
+                                                ctypes.c_void_p(target_ptr), ctypes.byref(p)), "image_gradients")
+        return p.value
+
+    def screen_gradients(self, camera, renderer, image_ptr, params_ptr, count):
+        p = ctypes.c_void_p()
+        _check(lib().gsn_solver_screen_gradients(self.handle, ctypes.byref(camera), renderer.handle,
+                                                 ctypes.c_void_p(image_ptr), ctypes.c_void_p(params_ptr), int(count),
+                                                 ctypes.byref(p)), "screen_gradients")
+        return p.value
+
+    def map_gradients(self, camera, renderer, params_ptr, count, sh_degree, grads_ptr):
+        _check(lib().gsn_solver_map_gradients(self.handle, ctypes.byref(camera), renderer.handle,
+                                              ctypes.c_void_p(params_ptr), int(count), int(sh_degree),
+                                              ctypes.c_void_p(grads_ptr)), "map_gradients")
+
+    def moments(self):
+        a, b, it = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_uint64()
+        _check(lib().gsn_solver_moments(self.handle, ctypes.byref(a), ctypes.byref(b), ctypes.byref(it)), "moments")
+        return a.value, b.value, it.value

@@ -81,6 +81,61 @@ int gsn_renderer_record_offsets(gsn_renderer* r, const int** out);
 /* Fixed record capacity (0 = grow on demand, the reference behaviour). */
 int gsn_renderer_set_record_capacity(gsn_renderer* r, int64_t records);
 
+
+/* ------------------------------------------------------------------ solver
+ * Replaces gs_native::Solver (reference src/core/solver/solver.h:11-68).
+ * A solver is paired with the renderer whose last frame it differentiates.
+ */
+typedef struct gsn_solver gsn_solver;
+
+int gsn_solver_create(gsn_solver** out);
+int gsn_solver_destroy(gsn_solver* s);
+int gsn_solver_set_stream(gsn_solver* s, void* stream);
+
+/* Solver::Iterate (solver.h:19-26; solver.cu:702-720): loss gradient of `image`
+ * (device fp32 HWC, the renderer's output) against `target` (device u8 HWC),
+ * backward through the renderer's frame, chain rule and one Adam step on the
+ * 58 x count device block `params`. */
+int gsn_solver_iterate(gsn_solver* s, const gsn_camera* camera, gsn_renderer* renderer, const float* image,
+                       const uint8_t* target, float* params, int count, float position_lr, int sh_degree);
+
+/* Solver::ResetOpacityHistory (solver.cu:722-733). */
+int gsn_solver_reset_opacity_history(gsn_solver* s);
+
+/* Solver::RemapGaussians (solver.cu:761-835): parent_ids (device, may be NULL)
+ * maps every new Gaussian to the old index whose Adam history it inherits
+ * (-1 = fresh history). */
+int gsn_solver_remap(gsn_solver* s, const int* parent_ids, int count);
+
+/* GetProjectionStatistics / GetAbsoluteProjectionStatistics (solver.h:35-41):
+ * device float[2 * count] each. */
+int gsn_solver_statistics(gsn_solver* s, const float** stats, const float** absolute_stats);
+
+/* Learning rates of the non-position groups (reference defaults: scale 0.005,
+ * rotation 0.001, opacity 0.025, SH DC 0.0025, SH rest 0.0025 / 20). */
+int gsn_solver_set_learning_rates(gsn_solver* s, float scale, float rotation, float opacity, float sh_dc,
+                                  float sh_rest);
+
+/* Enables the FP64 loss reduction; gsn_solver_loss then copies
+ * [loss, mean L1, mean SSIM, PSNR dB] of the last iterate to `out` (host). */
+int gsn_solver_set_compute_loss(gsn_solver* s, int enabled);
+int gsn_solver_loss(gsn_solver* s, double* out);
+int gsn_solver_loss_device(gsn_solver* s, const double** out);
+
+/* Stage entry points of Iterate for parity tests and partial pipelines:
+ * dL/dimage into the solver's buffer (device float[pixels * 3] via *out);
+ * screen-space gradients ([count][12] floats via *out); mapped parameter
+ * gradients (58 x count) into `grads_out` without an Adam step. */
+int gsn_solver_image_gradients(gsn_solver* s, const gsn_camera* camera, const float* image, const uint8_t* target,
+                               const float** out);
+int gsn_solver_screen_gradients(gsn_solver* s, const gsn_camera* camera, gsn_renderer* renderer,
+                                const float* image, const float* params, int count, const float** out);
+int gsn_solver_map_gradients(gsn_solver* s, const gsn_camera* camera, gsn_renderer* renderer, float* params,
+                             int count, int sh_degree, float* grads_out);
+
+/* Adam state (device, 58 x count each) and the step counter. */
+int gsn_solver_moments(gsn_solver* s, float** first, float** second, uint64_t* iteration);
+
 #ifdef __cplusplus
 }
 #endif
