@@ -1,0 +1,393 @@
+"""Benchmark of the 3DGS training hot path on B200.
+
+One step = one training iteration of the plain FP32 form on the 1.2M-Gaussian
+cap of the 1600x1064 ring-camera training scene: project + depth/tile ordering +
+per-tile blend + fused L1/SSIM gradient + backward + chain rule + Adam, through
+the library's C ABI (gs_native Renderer + Solver). This is the steady-state
+iteration of the training schedule (iterations 15k-30k: SH degree 3, no
+densification), with the model at the Gaussian cap.
+
+Scene (seeded, synthetic): the hidden target model is 1.5M Gaussians (seed 7,
+means N(0, 3^2)); 200 cameras on a ring of radius 8 at elevation +/-15 deg,
+1600x1064, fx = fy = 1400, every tenth held out; targets are rendered from the
+hidden model and quantised to u8. The model being optimised is a 1.2M-Gaussian
+draw of the same distribution (seed 8).
+
+Printed JSON line: `value` is iterations/s with targets resident in HBM,
+`e2e` the same through host buffers (pinned H2D target upload and a D2H loss
+read every step), plus per-stage device times, the roofline of the dominant
+kernel, SM clocks sampled during the timed region and the FP64 CPU oracle
+timed on the host cores (`cpu_baseline`). `--impl reference` times only the CPU
+implementation of the path (the oracle restatement of the reference's code).
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [os.path.join(ROOT, "gs-native_b200")]
+
+METRIC = "iters/sec @1.2M Gaussians 1600×1064: chosen form vs plain FP32, ΔPSNR≤0.1 dB"
+UNIT = "iters/sec"
+SH_DEGREE = 3
+TARGET_GAUSSIANS = 1_500_000
+MODEL_GAUSSIANS = 1_200_000
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=200)
+    p.add_argument("--warmup", type=int, default=10)
+    p.add_argument("--impl", default="gsn", choices=["gsn", "reference"])
+    p.add_argument("--gaussians", type=int, default=MODEL_GAUSSIANS)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--profile-only", action="store_true", help="one profiled pass, no JSON (for ncu captures)")
+    return p.parse_args()
+
+
+def position_lr(iteration, extent):
+    f = min(1.0, iteration / 30000.0)
+    return extent * math.exp(math.log(1.6e-4) * (1 - f) + math.log(1.6e-6) * f)
+
+
+def scene(n_model):
+    import scenes
+    target = scenes.random_gaussians(TARGET_GAUSSIANS, 7, mean_sigma=3.0)
+    model = scenes.random_gaussians(n_model, 8, mean_sigma=3.0)
+    train, _ = scenes.training_scene_cameras()
+    centers = []
+    for c in train:
+        R = np.array(list(c.R_c_w), dtype=np.float64).reshape(3, 3)
+        t = np.array(list(c.t_c_w), dtype=np.float64)
+        centers.append(-R.T @ t)
+    centers = np.array(centers)
+    extent = 1.1 * np.linalg.norm(centers - centers.mean(0), axis=1).max()
+    return target, model, train, float(extent)
+
+
+class ClockSampler:
+    """nvidia-smi SM clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.rows = []
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100",
+                 "-i", str(device_index)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 8:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        if not self.rows:
+            return None
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if r[4 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def algorithmic_bytes(n, records, tiles, pixels, s=16, tile_passes=2, visible=None):
+    """Compulsory HBM bytes per launch of each stage (formulas in DESIGN.md)."""
+    vis = n if visible is None else visible
+    return {
+        "project": n * (4 * (10 + 3 * s) + 68),
+        "depth_sort": 4 * n * 20,
+        "record_scan": n * 20,
+        "emit_records": records * 8 + vis * 24,
+        "tile_sort": tile_passes * records * 20,
+        "tile_ranges": records * 4 + (tiles + 1) * 8,
+        "raster_forward": records * 40 + pixels * 16,
+        "loss_gradient": pixels * 3 * 9,
+        "raster_backward": records * 40 + pixels * 28 + vis * 48,
+        "gaussian_update": n * (58 * 4 * 6 + 48 + 4 + 16),
+    }
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def cpu_baseline(model, cam, target_u8, extent, steps=1, threads=None):
+    """FP64 oracle (the CPU restatement of the reference's path) on a bounded
+    sample: per-Gaussian stages on all Gaussians, per-tile stages on one band of
+    tile rows, scaled to a full step by the band fraction."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    cores = threads or len(os.sched_getaffinity(0))
+    oracle.set_threads(cores)
+    n = model.shape[1]
+    tiles_x, tiles_y = cam.tile_count_x, cam.tile_count_y
+    band_row = tiles_y // 2
+    t0, t1 = band_row * tiles_x, (band_row + 1) * tiles_x
+    rows = (band_row * 16, min(cam.height, (band_row + 1) * 16))
+    frac = (t1 - t0) / (tiles_x * tiles_y)
+    params64 = model.astype(np.float64)
+    m = np.zeros_like(params64)
+    v = np.zeros_like(params64)
+    lr = dict(oracle.REFERENCE_LR)
+    lr["position"] = position_lr(15000, extent)
+    per_step = []
+    for step in range(steps):
+        p32 = params64.astype(np.float32)
+        a = time.perf_counter()
+        proj = oracle.project(p32, cam, SH_DEGREE)
+        offsets, ids = oracle.tile_lists(proj, cam)
+        b = time.perf_counter()
+        image, _, _ = oracle.render(proj, cam, offsets, ids, [0, 0, 0], (t0, t1))
+        gI = oracle.loss_gradient(image, target_u8, rows)
+        g9, a2 = oracle.backward(proj, cam, offsets, ids, image, gI, (t0, t1))
+        c = time.perf_counter()
+        g58 = oracle.map_gradients(p32, cam, SH_DEGREE, g9)
+        oracle.adam(params64, m, v, g58, lr, step + 1)
+        d = time.perf_counter()
+        per_step.append((b - a) + (c - b) / frac + (d - c))
+        sampled = d - a
+    sec = float(np.median(per_step))
+    return {"value": 1.0 / sec, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": (f"FP64 oracle step on {n} Gaussians: projection, tile lists, chain rule and Adam on all "
+                       f"Gaussians; blend, loss gradient and backward on tile row {band_row} "
+                       f"({t1 - t0} of {tiles_x * tiles_y} tiles), scaled by {1 / frac:.1f}; "
+                       f"{steps} step(s), {sampled:.1f} s sampled CPU time per step"),
+            "seconds_per_step": sec}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import scenes
+    target_model, model, train, extent = scene(args.gaussians)
+    cam = train[0]
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    img = oracle.render_params(target_model, cam, [0, 0, 0], SH_DEGREE)
+    target = np.clip(np.rint(img * 255), 0, 255).astype(np.uint8)
+    steps = max(1, args.steps)
+    warm = max(0, args.warmup)
+    res = cpu_baseline(model, cam, target, extent, steps=min(steps + warm, 3))
+    value = res["value"]
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": steps, "warmup": warm, "ms_per_step": 1000.0 / value, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "plain training step, 1.2M Gaussians, 1600x1064, SH degree 3, ring view 0",
+                   "gaussians": args.gaussians, "width": 1600, "height": 1064},
+        "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def run_gsn(args):
+    import torch
+    import gsn
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    gsn.lib()
+    target_model, model, train, extent = scene(args.gaussians)
+    n = model.shape[1]
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+
+    renderer = gsn.Renderer()
+    solver = gsn.Solver()
+    renderer.set_stream(sp)
+    solver.set_stream(sp)
+    # hidden-model targets, resident in HBM and in pinned host memory
+    tm = torch.from_numpy(target_model).cuda()
+    img = torch.empty((1064, 1600, 3), device="cuda")
+    targets = torch.empty((len(train), 1064, 1600, 3), dtype=torch.uint8, device="cuda")
+    for k, cam in enumerate(train):
+        assert renderer.render(tm.data_ptr(), tm.shape[1], cam, [0, 0, 0], img.data_ptr(), SH_DEGREE) == 0
+        targets[k] = (img * 255.0).round().clamp(0, 255).to(torch.uint8)
+    del tm
+    host_targets = targets.cpu().pin_memory()
+    staging = torch.empty((1064, 1600, 3), dtype=torch.uint8, device="cuda")
+    params = torch.from_numpy(model).cuda()
+    lr = position_lr(15000, extent)
+    loss_host = torch.zeros(4, dtype=torch.float64).pin_memory()
+
+    def step(k, e2e=False):
+        cam = train[k % len(train)]
+        if e2e:
+            staging.copy_(host_targets[k % len(train)], non_blocking=True)
+            tgt = staging
+        else:
+            tgt = targets[k % len(train)]
+        assert renderer.render(params.data_ptr(), n, cam, [0, 0, 0], img.data_ptr(), SH_DEGREE) == 0
+        assert solver.iterate(cam, renderer, img.data_ptr(), tgt.data_ptr(), params.data_ptr(), n, lr,
+                              SH_DEGREE) == 0
+        if e2e:
+            gsn.memcpy_async(loss_host.data_ptr(), solver.loss_device(), 32, sp)
+            stream.synchronize()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def timed(k0, steps, e2e=False):
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        launches0 = gsn.launch_count()
+        e0.record(stream)
+        for k in range(steps):
+            step(k0 + k, e2e)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        launches = gsn.launch_count() - launches0
+        barrier()
+        ms = e0.elapsed_time(e1)
+        if dist is not None:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, launches
+
+    for k in range(args.warmup):
+        step(k)
+    torch.cuda.synchronize()
+    if args.profile_only:
+        step(args.warmup)
+        torch.cuda.synchronize()
+        return
+
+    visible = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+    smi_index = visible.split(",")[local] if visible else str(local)
+    sampler = ClockSampler(smi_index) if rank == 0 else None
+    ms, launches = timed(args.warmup, args.steps)
+    clocks = sampler.stop() if sampler else None
+    value = world * args.steps / (ms / 1000.0)
+
+    # per-stage device time (profiled pass of the same steps)
+    gsn.profile_enable(True)
+    for k in range(args.steps):
+        step(args.warmup + k)
+    stages = gsn.profile_collect()
+    gsn.profile_enable(False)
+    stages = {k: v / args.steps for k, v in stages.items() if v > 0}
+
+    # end-to-end through host buffers
+    solver.set_compute_loss(True)
+    for k in range(2):
+        step(k, True)
+    ms_e2e, _ = timed(args.warmup, args.steps, e2e=True)
+    value_e2e = world * args.steps / (ms_e2e / 1000.0)
+    psnr = float(loss_host[3])
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    b = renderer.buffers()
+    records = int(b.record_count_host)
+    cam = train[0]
+    tiles = cam.tile_count_x * cam.tile_count_y
+    pixels = cam.width * cam.height
+    tile_bits = max(1, (tiles - 1).bit_length())
+    counts = torch.empty(n, dtype=torch.int32, device="cuda")
+    gsn.memcpy(counts.data_ptr(), b.tile_counts, 4 * n)
+    vis = int((counts > 0).sum().item())
+    alg = algorithmic_bytes(n, records, tiles, pixels, tile_passes=(tile_bits + 7) // 8, visible=vis)
+    peak, peak_kind = load_peaks()
+    stage_table = {}
+    for name, t in stages.items():
+        entry = {"ms": round(t, 4)}
+        if name in alg:
+            gbs = alg[name] / (t / 1000.0) / 1e9
+            entry.update(bytes=int(alg[name]), gbs=round(gbs, 1), hbm_frac=round(gbs / peak, 4))
+        stage_table[name] = entry
+    kernel_stages = {k: v for k, v in stages.items() if k in alg}
+    dominant = max(kernel_stages, key=kernel_stages.get)
+    hbm_stages = {k: v for k, v in kernel_stages.items() if k in ("gaussian_update", "project", "depth_sort",
+                                                                     "tile_sort", "emit_records", "loss_gradient")}
+    top_hbm = max(hbm_stages, key=hbm_stages.get)
+    achieved = alg[top_hbm] / (stages[top_hbm] / 1000.0) / 1e9
+    roofline = {"bound": "hbm", "kernel": top_hbm, "achieved": round(achieved, 1), "peak": peak,
+                "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured" else
+                "fallback 6650 GB/s",
+                "dominant_kernel": dominant,
+                "dominant_note": ("the per-tile blend kernels are bound by the FP32/MUFU issue rate and the "
+                                  "atomics of the backward, not by HBM; their HBM fractions are in `stages`")}
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        tgt0 = targets[0].cpu().numpy()
+        res = cpu_baseline(model, train[0], tgt0, extent, steps=1)
+        cpu = {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    out = {
+        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": ("plain FP32 training step (render, L1+SSIM gradient, backward, Adam) at the "
+                                "1.2M-Gaussian cap, 1600x1064, SH degree 3, one ring view per step"),
+                   "form": "plain_fp32", "gaussians": n, "width": 1600, "height": 1064,
+                   "records_per_step": records, "visible_gaussians": vis, "parallelism": f"replicas{world}",
+                   "l2": "inputs larger than L2 (params + Adam moments 835 MB, a new 5 MB target per step)"},
+        "gpu_launches": int(launches),
+        "e2e": {"value": round(value_e2e, 3), "unit": UNIT, "h2d_bytes_per_step": 1600 * 1064 * 3,
+                "d2h_bytes_per_step": 32, "psnr_db_last_step": round(psnr, 3)},
+        "roofline": roofline,
+        "stages": stage_table,
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(out), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gsn(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -7,6 +7,7 @@
 
 #include "core/render/renderer.h"
 #include "core/solver/solver.h"
+#include "profile.h"
 
 struct gsn_renderer {
     gs_native::Renderer impl;
@@ -43,9 +44,32 @@ int gsn_memcpy(void* dst, const void* src, size_t bytes) {
     return cudaMemcpy(dst, src, bytes, cudaMemcpyDefault) == cudaSuccess ? GSN_OK : GSN_ERR_CUDA;
 }
 
+int gsn_memcpy_async(void* dst, const void* src, size_t bytes, void* stream) {
+    if (bytes == 0) return GSN_OK;
+    if (!dst || !src) return GSN_ERR_INVALID_ARGUMENT;
+    return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, AsStream(stream)) == cudaSuccess ? GSN_OK
+                                                                                               : GSN_ERR_CUDA;
+}
+
 int gsn_stream_synchronize(void* stream) {
     return cudaStreamSynchronize(AsStream(stream)) == cudaSuccess ? GSN_OK : GSN_ERR_CUDA;
 }
+
+uint64_t gsn_kernel_launch_count(void) { return gsn::launch_count(); }
+
+int gsn_profile_enable(int enabled) {
+    gsn::profile_enable(enabled != 0);
+    return GSN_OK;
+}
+
+int gsn_profile_collect(double* ms, int count) {
+    if (!ms || count < 0) return GSN_ERR_INVALID_ARGUMENT;
+    return gsn::profile_collect(ms, count) == 0 ? GSN_OK : GSN_ERR_CUDA;
+}
+
+const char* gsn_stage_name(int stage) { return gsn::stage_name(stage); }
+
+int gsn_stage_count(void) { return gsn::kStageCount; }
 
 int gsn_renderer_create(gsn_renderer** out) {
     if (!out) return GSN_ERR_INVALID_ARGUMENT;

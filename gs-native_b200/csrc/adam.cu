@@ -339,7 +339,7 @@ int launch_gaussian_update(const GaussianUpdateArgs& a, int sh_degree, cudaStrea
         case 2: gaussian_update_kernel<2><<<grid, 256, 0, stream>>>(a); break;
         default: gaussian_update_kernel<3><<<grid, 256, 0, stream>>>(a); break;
     }
-    return launch_status();
+    return launched(1);
 }
 
 int launch_remap_moments(const int* parents, const float* prev_m, const float* prev_v, float* m, float* v,
@@ -347,7 +347,7 @@ int launch_remap_moments(const int* parents, const float* prev_m, const float* p
     if (count <= 0) return GSN_OK;
     dim3 grid(ceil_div(count, 256), kParams);
     remap_moments_kernel<<<grid, 256, 0, stream>>>(parents, prev_m, prev_v, m, v, prev_count, count);
-    return launch_status();
+    return launched(1);
 }
 
 }  // namespace gsn

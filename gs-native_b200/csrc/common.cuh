@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include "gsn_types.h"
+#include "profile.h"
 
 namespace gsn {
 
@@ -39,6 +40,12 @@ inline int launch_status() {
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) return GSN_OK;
     return e == cudaErrorMemoryAllocation ? GSN_ERR_OUT_OF_MEMORY : GSN_ERR_CUDA;
+}
+
+// Counts `kernels` launches of this library, then returns the launch status.
+inline int launched(int kernels) {
+    note_launch(kernels);
+    return launch_status();
 }
 
 // Rodrigues rotation of an axis-angle vector. The expression order is the one

@@ -228,12 +228,12 @@ int launch_loss_gradient(const float* image, const uint8_t* target, float* grad,
     if (sums && cudaMemsetAsync(sums, 0, 3 * sizeof(double), stream) != cudaSuccess) return GSN_ERR_CUDA;
     dim3 grid(ceil_div(width, kTw), ceil_div(height, kTh), 3);
     loss_gradient_kernel<<<grid, kThreads, 0, stream>>>(image, target, grad, width, height, sums);
-    return launch_status();
+    return launched(1);
 }
 
 int launch_finalize_loss(const double* sums, int width, int height, double* out, cudaStream_t stream) {
     finalize_loss_kernel<<<1, 1, 0, stream>>>(sums, width, height, out);
-    return launch_status();
+    return launched(1);
 }
 
 }  // namespace gsn

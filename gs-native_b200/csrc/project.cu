@@ -153,7 +153,7 @@ int launch_project(const float* params, int n, const gsn_camera& cam, int sh_deg
         case 2: project_kernel<2><<<grid, 256, 0, stream>>>(params, cam, n, out); break;
         default: project_kernel<3><<<grid, 256, 0, stream>>>(params, cam, n, out); break;
     }
-    return launch_status();
+    return launched(1);
 }
 
 }  // namespace gsn

@@ -180,7 +180,7 @@ int launch_raster_backward(const RasterBackwardArgs& a, cudaStream_t stream) {
     int64_t tiles = static_cast<int64_t>(a.cam.tile_count_x) * a.cam.tile_count_y;
     if (tiles <= 0) return GSN_OK;
     raster_backward_kernel<<<static_cast<unsigned>(tiles), kTilePixels, 0, stream>>>(a);
-    return launch_status();
+    return launched(1);
 }
 
 }  // namespace gsn

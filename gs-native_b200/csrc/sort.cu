@@ -368,7 +368,7 @@ int launch_radix_sort(uint32_t* keys, uint32_t* values, uint32_t* keys_alt, uint
         uint32_t* tv = vin; vin = vout; vout = tv;
     }
     *result_in_alt = (passes % 2) == 1;
-    return launch_status();
+    return launched(3 * passes);
 }
 
 size_t scan_scratch_bytes(int n) {
@@ -384,7 +384,7 @@ int launch_exclusive_scan(const int* in, const uint32_t* gather, int* out, int n
     else cudaMemsetAsync(block_sums, 0, sizeof(int), stream);
     scan_block_sums<<<1, kScanThreads, 0, stream>>>(block_sums, n > 0 ? blocks : 0, out + n);
     if (n > 0) scan_downsweep<<<blocks, kScanThreads, 0, stream>>>(in, gather, n, block_sums, out);
-    return launch_status();
+    return launched(n > 0 ? 3 : 1);
 }
 
 int launch_emit_records(const uint32_t* sorted_ids, const int* record_start, const int4* rects, int n,
@@ -393,7 +393,7 @@ int launch_emit_records(const uint32_t* sorted_ids, const int* record_start, con
     if (n <= 0) return GSN_OK;
     emit_records<<<ceil_div(4ll * n, 256), 256, 0, stream>>>(sorted_ids, record_start, rects, n, tile_count_x,
                                                              tile_keys, record_ids, capacity, overflow);
-    return launch_status();
+    return launched(1);
 }
 
 int launch_tile_ranges(const uint32_t* sorted_tiles, const int* record_count_device, int max_records,
@@ -403,7 +403,7 @@ int launch_tile_ranges(const uint32_t* sorted_tiles, const int* record_count_dev
     if (blocks > 148 * 32) blocks = 148 * 32;
     tile_ranges<<<blocks, 256, 0, stream>>>(sorted_tiles, record_count_device, max_records, tile_count,
                                            offsets);
-    return launch_status();
+    return launched(1);
 }
 
 }  // namespace gsn

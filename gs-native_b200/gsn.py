@@ -76,7 +76,13 @@ def lib():
     sig = {
         "gsn_version": ([], ctypes.c_char_p),
         "gsn_memcpy": ([vp, vp, ctypes.c_size_t], i32),
+        "gsn_memcpy_async": ([vp, vp, ctypes.c_size_t, vp], i32),
         "gsn_stream_synchronize": ([vp], i32),
+        "gsn_kernel_launch_count": ([], ctypes.c_uint64),
+        "gsn_profile_enable": ([i32], i32),
+        "gsn_profile_collect": ([P(ctypes.c_double), i32], i32),
+        "gsn_stage_name": ([i32], ctypes.c_char_p),
+        "gsn_stage_count": ([], i32),
         "gsn_renderer_create": ([P(vp)], i32),
         "gsn_renderer_destroy": ([vp], i32),
         "gsn_renderer_set_stream": ([vp, vp], i32),
@@ -157,6 +163,27 @@ class Renderer:
 
     def set_record_capacity(self, records):
         return lib().gsn_renderer_set_record_capacity(self.handle, int(records))
+
+
+def launch_count():
+    return int(lib().gsn_kernel_launch_count())
+
+
+def profile_enable(on=True):
+    _check(lib().gsn_profile_enable(int(bool(on))), "profile_enable")
+
+
+def profile_collect():
+    """{stage name: device ms} since the previous collect."""
+    n = lib().gsn_stage_count()
+    ms = (ctypes.c_double * n)()
+    _check(lib().gsn_profile_collect(ms, n), "profile_collect")
+    return {lib().gsn_stage_name(k).decode(): ms[k] for k in range(n)}
+
+
+def memcpy_async(dst, src, nbytes, stream):
+    _check(lib().gsn_memcpy_async(ctypes.c_void_p(dst), ctypes.c_void_p(src), ctypes.c_size_t(nbytes),
+                                  ctypes.c_void_p(stream)), "gsn_memcpy_async")
 
 
 def memcpy(dst, src, nbytes):

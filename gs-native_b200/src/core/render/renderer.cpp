@@ -6,6 +6,7 @@
 #include <climits>
 
 #include "kernels.h"
+#include "profile.h"
 
 namespace gs_native {
 
@@ -112,7 +113,9 @@ bool Renderer::Render(const GaussianBuffers& gaussians, const CameraParams& came
     if (count > 0) {
         gsn::ProjectOutputs po{means_.get(), conic_opacities_.get(), colors_.get(), depths_.get(),
                                rects_.get(), tile_counts_.get(), depth_keys_[0].get(), radii_.get()};
+        gsn::stage_mark(s, gsn::kStageProject);
         if (gsn::launch_project(gaussians.gaussians_, count, cam, sh_degree, po, s) != GSN_OK) return false;
+        gsn::stage_mark(s, gsn::kStageDepthSort);
         gsn::RadixSortScratch scratch = gsn::radix_sort_scratch(sort_scratch_.get(), sort_max);
         bool in_alt = false;
         if (gsn::launch_radix_sort(depth_keys_[0].get(), depth_ids_[0].get(), depth_keys_[1].get(),
@@ -120,6 +123,7 @@ bool Renderer::Render(const GaussianBuffers& gaussians, const CameraParams& came
                                    s) != GSN_OK)
             return false;
         const uint32_t* by_depth = depth_ids_[in_alt ? 1 : 0].get();
+        gsn::stage_mark(s, gsn::kStageRecordScan);
         if (gsn::launch_exclusive_scan(tile_counts_.get(), by_depth, record_start_.get(), count,
                                        scan_scratch_.get(), s) != GSN_OK)
             return false;
@@ -141,6 +145,7 @@ bool Renderer::Render(const GaussianBuffers& gaussians, const CameraParams& came
             }
             last_records_ = records;
         }
+        gsn::stage_mark(s, gsn::kStageEmitRecords);
         if (gsn::launch_emit_records(by_depth, record_start_.get(), rects_.get(), count, camera.tile_count_x_,
                                      tile_keys_[0].get(), record_ids_[0].get(), record_capacity_, overflow,
                                      s) != GSN_OK)
@@ -148,6 +153,7 @@ bool Renderer::Render(const GaussianBuffers& gaussians, const CameraParams& came
         const int max_records = fixed_capacity_ ? static_cast<int>(record_capacity_) : static_cast<int>(records);
         scratch = gsn::radix_sort_scratch(sort_scratch_.get(), static_cast<int>(sort_scratch_count_));
         in_alt = false;
+        gsn::stage_mark(s, gsn::kStageTileSort);
         if (max_records > 0 &&
             gsn::launch_radix_sort(tile_keys_[0].get(), record_ids_[0].get(), tile_keys_[1].get(),
                                    record_ids_[1].get(), false, max_records,
@@ -155,6 +161,7 @@ bool Renderer::Render(const GaussianBuffers& gaussians, const CameraParams& came
                                    &in_alt, s) != GSN_OK)
             return false;
         sorted_ids_ = record_ids_[in_alt ? 1 : 0].get();
+        gsn::stage_mark(s, gsn::kStageTileRanges);
         if (gsn::launch_tile_ranges(tile_keys_[in_alt ? 1 : 0].get(), record_count, std::max(max_records, 1),
                                     tile_count, tile_offsets_.get(), s) != GSN_OK)
             return false;
@@ -176,7 +183,10 @@ bool Renderer::Render(const GaussianBuffers& gaussians, const CameraParams& came
     ra.image = image;
     ra.final_transmittance = nullptr;
     ra.contributors = contributors_.get();
-    return gsn::launch_raster_forward(ra, s) == GSN_OK;
+    gsn::stage_mark(s, gsn::kStageRasterForward);
+    const bool ok = gsn::launch_raster_forward(ra, s) == GSN_OK;
+    gsn::stage_mark(s, gsn::kStageOther);
+    return ok;
 }
 
 const int* Renderer::GetRecordOffsets() const {

@@ -6,6 +6,7 @@
 #include <cmath>
 
 #include "kernels.h"
+#include "profile.h"
 
 namespace gs_native {
 
@@ -64,6 +65,7 @@ bool Solver::ComputeImageGradients(const CameraParams& camera, const float* imag
         if (!loss_.Reserve(8)) return false;
         sums = loss_.get();
     }
+    gsn::stage_mark(stream_, gsn::kStageLossGradient);
     if (gsn::launch_loss_gradient(image, target, image_gradients_.get(), camera.width_, camera.height_, sums,
                                   stream_) != GSN_OK)
         return false;
@@ -87,6 +89,7 @@ bool Solver::ComputeScreenGradients(const CameraParams& camera, const Renderer& 
     if (count != gaussian_count_) {
         if (iteration_ != 0 || !RemapGaussians(nullptr, count)) return false;
     }
+    gsn::stage_mark(stream_, gsn::kStageRasterBackward);
     if (cudaMemsetAsync(screen_.get(), 0, static_cast<size_t>(count) * 12 * sizeof(float), stream_) != cudaSuccess)
         return false;
     gsn::RasterBackwardArgs a;
@@ -135,7 +138,9 @@ bool Solver::UpdateGaussians(const CameraParams& camera, const Renderer& rendere
         a.obs_counts = acc_count_;
     }
     a.grads_out = grads_out;
+    gsn::stage_mark(stream_, gsn::kStageGaussianUpdate);
     if (gsn::launch_gaussian_update(a, std::clamp(sh_degree, 0, 3), stream_) != GSN_OK) return false;
+    gsn::stage_mark(stream_, gsn::kStageOther);
     if (adam) iteration_ = iteration;
     return true;
 }

@@ -34,8 +34,24 @@ const char* gsn_version(void);
  * callers without their own CUDA bindings. */
 int gsn_memcpy(void* dst, const void* src, size_t bytes);
 
+/* Asynchronous byte copy on `stream` (cudaMemcpyDefault); host memory should
+ * be pinned for the copy to overlap. */
+int gsn_memcpy_async(void* dst, const void* src, size_t bytes, void* stream);
+
 /* Blocks until all work on `stream` is done. */
 int gsn_stream_synchronize(void* stream);
+
+/* Number of this library's kernel launches since load (process-wide). */
+uint64_t gsn_kernel_launch_count(void);
+
+/* Stage profiler: when enabled, stage boundaries record CUDA events on the
+ * stream of the stage; gsn_profile_collect synchronises and writes the device
+ * milliseconds per stage since the last collect into ms[0..count) (stage
+ * names via gsn_stage_name). */
+int gsn_profile_enable(int enabled);
+int gsn_profile_collect(double* ms, int count);
+const char* gsn_stage_name(int stage);
+int gsn_stage_count(void);
 
 /* ------------------------------------------------------------------ renderer
  * Replaces gs_native::Renderer (reference src/core/render/renderer.h:10-89).
