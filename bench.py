@@ -49,7 +49,9 @@ def parse():
     p.add_argument("--impl", default="gsn", choices=["gsn", "reference"])
     p.add_argument("--gaussians", type=int, default=MODEL_GAUSSIANS)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--profile-only", action="store_true", help="one profiled pass, no JSON (for ncu captures)")
+    p.add_argument("--profile-only", action="store_true",
+                   help="warm-up steps plus one step on 3 views, no JSON (for ncu captures)")
+    p.add_argument("--views", type=int, default=0, help="number of training views used (0 = all 180)")
     return p.parse_args()
 
 
@@ -228,6 +230,9 @@ def run_gsn(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     gsn.lib()
     target_model, model, train, extent = scene(args.gaussians)
+    views = 3 if args.profile_only else args.views
+    if views:
+        train = train[:views]
     n = model.shape[1]
     stream = torch.cuda.current_stream()
     sp = stream.cuda_stream

@@ -226,24 +226,41 @@ __device__ __forceinline__ void chain_rule(const float* __restrict__ p, int64_t 
     for (int c = 0; c < 3; ++c) out.grgb[c] = color[c] >= 0 ? in[6 + c] : 0.0f;
 }
 
-__device__ __forceinline__ float row_lr(const GaussianUpdateArgs& a, int row) {
-    if (row < GSN_LOG_SCALE_INDEX) return a.lr[0];
-    if (row < GSN_ROTATION_INDEX) return a.lr[1];
-    if (row < GSN_OPACITY_INDEX) return a.lr[2];
-    if (row < GSN_SH_INDEX) return a.lr[3];
-    return (row - GSN_SH_INDEX) % kShStride == 0 ? a.lr[4] : a.lr[5];
-}
-
-__device__ __forceinline__ void adam_row(const GaussianUpdateArgs& a, int row, int64_t idx, float g) {
-    float first = 0.9f * a.m[idx] + 0.1f * g;
-    float second = 0.999f * a.v[idx] + 0.001f * g * g;
-    a.m[idx] = first;
-    a.v[idx] = second;
-    a.params[idx] -= row_lr(a, row) * (first * a.c1) / (sqrtf(second * a.c2) + 1e-15f);
+// Adam (UpdateGaussiansKernel arithmetic) on CNT consecutive rows starting at
+// row0. All loads of the group are issued before any store, so the three
+// streams of every row are in flight together; the parameter block and the
+// two moment arrays never alias.
+template <int CNT>
+__device__ __forceinline__ void adam_rows(float* __restrict__ P, float* __restrict__ M, float* __restrict__ V,
+                                          int64_t N, int i, int row0, const float* g, const float* lr, float c1,
+                                          float c2) {
+    float p[CNT], m[CNT], v[CNT];
+#pragma unroll
+    for (int r = 0; r < CNT; ++r) {
+        const int64_t idx = static_cast<int64_t>(row0 + r) * N + i;
+        p[r] = P[idx];
+        m[r] = M[idx];
+        v[r] = V[idx];
+    }
+#pragma unroll
+    for (int r = 0; r < CNT; ++r) {
+        float first = 0.9f * m[r] + 0.1f * g[r];
+        float second = 0.999f * v[r] + 0.001f * g[r] * g[r];
+        m[r] = first;
+        v[r] = second;
+        p[r] -= lr[r] * (first * c1) / (sqrtf(second * c2) + 1e-15f);
+    }
+#pragma unroll
+    for (int r = 0; r < CNT; ++r) {
+        const int64_t idx = static_cast<int64_t>(row0 + r) * N + i;
+        P[idx] = p[r];
+        M[idx] = m[r];
+        V[idx] = v[r];
+    }
 }
 
 template <int D>
-__global__ void __launch_bounds__(256) gaussian_update_kernel(GaussianUpdateArgs a) {
+__global__ void __launch_bounds__(256, 2) gaussian_update_kernel(GaussianUpdateArgs a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n) return;
     const int64_t N = a.n;
@@ -299,15 +316,25 @@ __global__ void __launch_bounds__(256) gaussian_update_kernel(GaussianUpdateArgs
                 a.grads_out[(GSN_SH_INDEX + c * kShStride + k) * N + i] = k < K ? ch.grgb[c] * ch.basis[k] : 0.0f;
     }
     if (!a.m) return;
+    float* __restrict__ P = a.params;
+    float* __restrict__ M = a.m;
+    float* __restrict__ V = a.v;
+    const float lr_geo[10] = {a.lr[0], a.lr[0], a.lr[0], a.lr[1], a.lr[1], a.lr[1], a.lr[2], a.lr[2], a.lr[2], a.lr[3]};
+    adam_rows<10>(P, M, V, N, i, 0, ch.g, lr_geo, a.c1, a.c2);
+    float lr_sh[8];
 #pragma unroll
-    for (int r = 0; r < 10; ++r) adam_row(a, r, r * N + i, ch.g[r]);
+    for (int k = 0; k < 8; ++k) lr_sh[k] = a.lr[5];
 #pragma unroll
-    for (int c = 0; c < 3; ++c)
+    for (int c = 0; c < 3; ++c) {
 #pragma unroll
-        for (int k = 0; k < kShStride; ++k) {
-            int row = GSN_SH_INDEX + c * kShStride + k;
-            adam_row(a, row, row * N + i, k < K ? ch.grgb[c] * ch.basis[k] : 0.0f);
+        for (int half = 0; half < 2; ++half) {
+            float g8[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) g8[k] = half * 8 + k < K ? ch.grgb[c] * ch.basis[half * 8 + k] : 0.0f;
+            lr_sh[0] = half == 0 ? a.lr[4] : a.lr[5];
+            adam_rows<8>(P, M, V, N, i, GSN_SH_INDEX + c * kShStride + half * 8, g8, lr_sh, a.c1, a.c2);
         }
+    }
 }
 
 __global__ void remap_moments_kernel(const int* __restrict__ parents, const float* __restrict__ prev_m,

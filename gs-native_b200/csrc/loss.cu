@@ -24,15 +24,20 @@ __constant__ float c_window[11] = {1.028380120e-03f, 7.598758210e-03f, 3.6000773
                                    2.130055430e-01f, 2.660117150e-01f, 2.130055430e-01f, 1.093606870e-01f,
                                    3.600077330e-02f, 7.598758210e-03f, 1.028380120e-03f};
 
-constexpr int kTw = 16;                // output tile width
-constexpr int kTh = 32;                // output tile height
-constexpr int kThreads = kTw * kTh;    // 512
-constexpr int kInW = kTw + 20;         // raw input incl. 10-pixel halo
-constexpr int kInH = kTh + 20;
-constexpr int kMomW = kTw + 10;        // moment columns (centres incl. 5-pixel halo)
-constexpr int kCenH = kTh + 10;        // centre rows
+constexpr int kT = 32;                 // output tile edge
+constexpr int kThreads = 256;
+constexpr int kIn = kT + 20;           // raw input edge incl. the 10-pixel halo
+constexpr int kCen = kT + 10;          // SSIM centres per edge incl. the 5-pixel halo
+constexpr int kSeg1 = 7;               // outputs per thread in the moment passes (42 = 6 x 7)
+constexpr int kSeg2 = 4;               // outputs per thread in the back-filter passes (32 = 8 x 4)
 constexpr float kC1 = 0.0001f;
 constexpr float kC2 = 0.0009f;
+// shared arena (floats): raw image + target, five moment planes, three partial
+// planes; the back-filtered partials reuse the moment planes.
+constexpr int kRaw = kIn * kIn;
+constexpr int kMom = kIn * kCen;
+constexpr int kPart = kCen * kCen;
+constexpr size_t kSmemBytes = sizeof(float) * (2 * kRaw + 5 * kMom + 3 * kPart);
 
 __device__ __forceinline__ double block_sum(double v, double* red) {
     for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -46,27 +51,27 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
     return s;
 }
 
-__global__ void __launch_bounds__(kThreads, 3) loss_gradient_kernel(const float* __restrict__ image,
+// One block per 32x32 output tile and colour channel. Every filter output is
+// produced by one thread from a register window of its row (or column), with
+// the 11 taps accumulated in ascending order as in solver.cu:65-161.
+__global__ void __launch_bounds__(kThreads, 2) loss_gradient_kernel(const float* __restrict__ image,
                                                                    const uint8_t* __restrict__ target,
                                                                    float* __restrict__ grad, int width, int height,
                                                                    double* __restrict__ sums) {
-    // one arena, reused by the three stages
-    __shared__ float s[5 * kInH * kMomW];
+    extern __shared__ float smem[];
     __shared__ double red[kThreads / 32];
+    float* raw_i = smem;                 // [kIn][kIn]
+    float* raw_t = raw_i + kRaw;         // [kIn][kIn]
+    float* mom = raw_t + kRaw;           // [5][kIn][kCen]
+    float* part = mom + 5 * kMom;        // [3][kCen][kCen]
+    float* back = mom;                   // [3][kCen][kT] (after the moments are consumed)
     const int t = threadIdx.x;
     const int ch = blockIdx.z;
-    const int ox = blockIdx.x * kTw, oy = blockIdx.y * kTh;
-    const int x = ox + t % kTw, y = oy + t / kTw;
-    const bool inside = x < width && y < height;
-    const int64_t pix = (static_cast<int64_t>(y) * width + x) * 3 + ch;
-    const float I = inside ? image[pix] : 0.0f;
-    const float R = inside ? target[pix] * (1.0f / 255.0f) : 0.0f;
+    const int ox = blockIdx.x * kT, oy = blockIdx.y * kT;
 
-    // stage 0: raw image / target with a 10-pixel zero-padded halo
-    float* raw_i = s;
-    float* raw_t = s + kInH * kInW;
-    for (int j = t; j < kInH * kInW; j += kThreads) {
-        int hx = ox + j % kInW - 10, hy = oy + j / kInW - 10;
+    // raw inputs with a zero-padded halo
+    for (int j = t; j < kRaw; j += kThreads) {
+        int hx = ox + j % kIn - 10, hy = oy + j / kIn - 10;
         bool ok = hx >= 0 && hy >= 0 && hx < width && hy < height;
         int64_t k = (static_cast<int64_t>(hy) * width + hx) * 3 + ch;
         raw_i[j] = ok ? image[k] : 0.0f;
@@ -74,134 +79,146 @@ __global__ void __launch_bounds__(kThreads, 3) loss_gradient_kernel(const float*
     }
     __syncthreads();
 
-    // stage 1: horizontal filter of the five moments over kInH x kMomW
-    constexpr int kHSlots = (kInH * kMomW + kThreads - 1) / kThreads;
-    float h[kHSlots][5];
+    // horizontal pass over the five moments: kIn rows x kCen centres
+    for (int item = t; item < kIn * (kCen / kSeg1); item += kThreads) {
+        const int r = item / (kCen / kSeg1);
+        const int c0 = (item % (kCen / kSeg1)) * kSeg1;
+        float a[kSeg1 + 10], b[kSeg1 + 10];
 #pragma unroll
-    for (int q = 0; q < kHSlots; ++q) {
+        for (int k = 0; k < kSeg1 + 10; ++k) {
+            a[k] = raw_i[r * kIn + c0 + k];
+            b[k] = raw_t[r * kIn + c0 + k];
+        }
 #pragma unroll
-        for (int m = 0; m < 5; ++m) h[q][m] = 0.0f;
-        int j = t + q * kThreads;
-        if (j < kInH * kMomW) {
-            int base = (j / kMomW) * kInW + j % kMomW;
+        for (int o = 0; o < kSeg1; ++o) {
+            float h0 = 0.f, h1 = 0.f, h2 = 0.f, h3 = 0.f, h4 = 0.f;
 #pragma unroll
             for (int dx = 0; dx < 11; ++dx) {
                 float w = c_window[dx];
-                float a = raw_i[base + dx];
-                float b = raw_t[base + dx];
-                h[q][0] += w * a;
-                h[q][1] += w * b;
-                h[q][2] += w * a * a;
-                h[q][3] += w * b * b;
-                h[q][4] += w * a * b;
+                float av = a[o + dx], bv = b[o + dx];
+                h0 += w * av;
+                h1 += w * bv;
+                h2 += w * av * av;
+                h3 += w * bv * bv;
+                h4 += w * av * bv;
             }
+            const int idx = r * kCen + c0 + o;
+            mom[0 * kMom + idx] = h0;
+            mom[1 * kMom + idx] = h1;
+            mom[2 * kMom + idx] = h2;
+            mom[3 * kMom + idx] = h3;
+            mom[4 * kMom + idx] = h4;
         }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int q = 0; q < kHSlots; ++q) {
-        int j = t + q * kThreads;
-        if (j < kInH * kMomW)
-#pragma unroll
-            for (int m = 0; m < 5; ++m) s[m * kInH * kMomW + j] = h[q][m];
     }
     __syncthreads();
 
-    // stage 2: vertical filter -> moments at the kCenH x kMomW centres, then the
-    // SSIM partials of every centre inside the image
-    constexpr int kSSlots = (kCenH * kMomW + kThreads - 1) / kThreads;
-    float mo[kSSlots][5];
+    // vertical pass -> moments at the centres, then the SSIM partials
+    double ssim_sum = 0.0;
+    for (int item = t; item < (kCen / kSeg1) * kCen; item += kThreads) {
+        const int cx = item % kCen;
+        const int r0 = (item / kCen) * kSeg1;
+        float M[5][kSeg1];
 #pragma unroll
-    for (int q = 0; q < kSSlots; ++q) {
+        for (int m = 0; m < 5; ++m) {
+            float col[kSeg1 + 10];
 #pragma unroll
-        for (int m = 0; m < 5; ++m) mo[q][m] = 0.0f;
-        int j = t + q * kThreads;
-        if (j < kCenH * kMomW) {
+            for (int k = 0; k < kSeg1 + 10; ++k) col[k] = mom[m * kMom + (r0 + k) * kCen + cx];
 #pragma unroll
-            for (int dy = 0; dy < 11; ++dy) {
-                float w = c_window[dy];
-                int k = (j / kMomW + dy) * kMomW + j % kMomW;
+            for (int o = 0; o < kSeg1; ++o) {
+                float acc = 0.0f;
 #pragma unroll
-                for (int m = 0; m < 5; ++m) mo[q][m] += w * s[m * kInH * kMomW + k];
+                for (int dy = 0; dy < 11; ++dy) acc += c_window[dy] * col[o + dy];
+                M[m][o] = acc;
             }
         }
-    }
-    double ssim_sum = 0.0;
-    __syncthreads();
+        const int hx = ox + cx - 5;
 #pragma unroll
-    for (int q = 0; q < kSSlots; ++q) {
-        int j = t + q * kThreads;
-        if (j < kCenH * kMomW) {
-            int cx = j % kMomW, cy = j / kMomW;
-            int hx = ox + cx - 5, hy = oy + cy - 5;
+        for (int o = 0; o < kSeg1; ++o) {
+            const int cy = r0 + o;
+            const int hy = oy + cy - 5;
             float pa = 0.0f, pb = 0.0f, pc = 0.0f;
             if (hx >= 0 && hy >= 0 && hx < width && hy < height) {
-                float m = mo[q][0], n = mo[q][1];
+                float m = M[0][o], n = M[1][o];
                 float inv_d = 1.0f / (m * m + n * n + kC1);
-                float inv_e = 1.0f / (mo[q][2] - m * m + mo[q][3] - n * n + kC2);
+                float inv_e = 1.0f / (M[2][o] - m * m + M[3][o] - n * n + kC2);
                 float lum = (2 * m * n + kC1) * inv_d;
-                float cs = (2 * (mo[q][4] - m * n) + kC2) * inv_e;
+                float cs = (2 * (M[4][o] - m * n) + kC2) * inv_e;
                 float dmu = 2 * (n - m * lum) * inv_d * cs;
                 pb = 2 * lum * inv_e;
                 pc = -lum * cs * inv_e;
                 pa = dmu - n * pb - 2 * m * pc;
-                if (sums && cx >= 5 && cx < 5 + kTw && cy >= 5 && cy < 5 + kTh)
+                if (sums && cx >= 5 && cx < 5 + kT && cy >= 5 && cy < 5 + kT)
                     ssim_sum += static_cast<double>(lum) * static_cast<double>(cs);
             }
-            s[j] = pa;
-            s[kCenH * kMomW + j] = pb;
-            s[2 * kCenH * kMomW + j] = pc;
+            const int idx = cy * kCen + cx;
+            part[0 * kPart + idx] = pa;
+            part[1 * kPart + idx] = pb;
+            part[2 * kPart + idx] = pc;
         }
     }
     __syncthreads();
 
-    // stage 3: horizontal filter of the partials over kCenH x kTw
-    constexpr int kGSlots = (kCenH * kTw + kThreads - 1) / kThreads;
-    float g[kGSlots][3];
+    // horizontal back-filter of the partials: kCen rows x kT columns
+    for (int item = t; item < kCen * (kT / kSeg2); item += kThreads) {
+        const int r = item / (kT / kSeg2);
+        const int c0 = (item % (kT / kSeg2)) * kSeg2;
 #pragma unroll
-    for (int q = 0; q < kGSlots; ++q) {
-        g[q][0] = g[q][1] = g[q][2] = 0.0f;
-        int j = t + q * kThreads;
-        if (j < kCenH * kTw) {
+        for (int p = 0; p < 3; ++p) {
+            float v[kSeg2 + 10];
 #pragma unroll
-            for (int dx = 0; dx < 11; ++dx) {
-                float w = c_window[dx];
-                int k = (j / kTw) * kMomW + j % kTw + dx;
+            for (int k = 0; k < kSeg2 + 10; ++k) v[k] = part[p * kPart + r * kCen + c0 + k];
 #pragma unroll
-                for (int c = 0; c < 3; ++c) g[q][c] += w * s[c * kCenH * kMomW + k];
+            for (int o = 0; o < kSeg2; ++o) {
+                float acc = 0.0f;
+#pragma unroll
+                for (int dx = 0; dx < 11; ++dx) acc += c_window[dx] * v[o + dx];
+                back[p * kCen * kT + r * kT + c0 + o] = acc;
             }
         }
     }
     __syncthreads();
-#pragma unroll
-    for (int q = 0; q < kGSlots; ++q) {
-        int j = t + q * kThreads;
-        if (j < kCenH * kTw)
-#pragma unroll
-            for (int c = 0; c < 3; ++c) s[c * kCenH * kTw + j] = g[q][c];
-    }
-    __syncthreads();
 
-    // stage 4: vertical filter at the output pixel and the combined gradient
-    if (inside) {
-        float f[3] = {0.0f, 0.0f, 0.0f};
+    // vertical back-filter at the output pixels and the combined gradient
+    double l1_sum = 0.0, sq_sum = 0.0;
+    const float norm = 1.0f / (3.0f * static_cast<float>(width) * height);
+    for (int item = t; item < (kT / kSeg2) * kT; item += kThreads) {
+        const int x = item % kT;
+        const int y0 = (item / kT) * kSeg2;
+        float f[3][kSeg2];
 #pragma unroll
-        for (int dy = 0; dy < 11; ++dy) {
-            float w = c_window[dy];
-            int k = (t / kTw + dy) * kTw + t % kTw;
+        for (int p = 0; p < 3; ++p) {
+            float v[kSeg2 + 10];
 #pragma unroll
-            for (int c = 0; c < 3; ++c) f[c] += w * s[c * kCenH * kTw + k];
+            for (int k = 0; k < kSeg2 + 10; ++k) v[k] = back[p * kCen * kT + (y0 + k) * kT + x];
+#pragma unroll
+            for (int o = 0; o < kSeg2; ++o) {
+                float acc = 0.0f;
+#pragma unroll
+                for (int dy = 0; dy < 11; ++dy) acc += c_window[dy] * v[o + dy];
+                f[p][o] = acc;
+            }
         }
-        float r = I - R;
-        float l1 = static_cast<float>(r > 0) - static_cast<float>(r < 0);
-        float dssim = -(f[0] + R * f[1] + 2 * I * f[2]);
-        float norm = 1.0f / (3.0f * static_cast<float>(width) * height);
-        grad[pix] = (0.8f * l1 + 0.2f * dssim) * norm;
+#pragma unroll
+        for (int o = 0; o < kSeg2; ++o) {
+            const int px = ox + x, py = oy + y0 + o;
+            if (px < width && py < height) {
+                const float I = raw_i[(y0 + o + 10) * kIn + x + 10];
+                const float R = raw_t[(y0 + o + 10) * kIn + x + 10];
+                float r = I - R;
+                float l1 = static_cast<float>(r > 0) - static_cast<float>(r < 0);
+                float dssim = -(f[0][o] + R * f[1][o] + 2 * I * f[2][o]);
+                grad[(static_cast<int64_t>(py) * width + px) * 3 + ch] = (0.8f * l1 + 0.2f * dssim) * norm;
+                if (sums) {
+                    double d = static_cast<double>(I) - static_cast<double>(R);
+                    l1_sum += fabs(d);
+                    sq_sum += d * d;
+                }
+            }
+        }
     }
     if (sums) {
-        double d = inside ? static_cast<double>(I) - static_cast<double>(R) : 0.0;
-        double l1s = block_sum(fabs(d), red);
-        double sq = block_sum(d * d, red);
+        double l1s = block_sum(l1_sum, red);
+        double sq = block_sum(sq_sum, red);
         double ss = block_sum(ssim_sum, red);
         if (t == 0) {
             atomicAdd(sums + 0, l1s);
@@ -226,8 +243,18 @@ int launch_loss_gradient(const float* image, const uint8_t* target, float* grad,
                          double* sums, cudaStream_t stream) {
     if (width <= 0 || height <= 0) return GSN_ERR_INVALID_ARGUMENT;
     if (sums && cudaMemsetAsync(sums, 0, 3 * sizeof(double), stream) != cudaSuccess) return GSN_ERR_CUDA;
-    dim3 grid(ceil_div(width, kTw), ceil_div(height, kTh), 3);
-    loss_gradient_kernel<<<grid, kThreads, 0, stream>>>(image, target, grad, width, height, sums);
+    // the dynamic shared-memory opt-in is a per-device function attribute
+    static bool configured[64] = {};
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess) return GSN_ERR_CUDA;
+    if (device < 0 || device >= 64 || !configured[device]) {
+        if (cudaFuncSetAttribute(loss_gradient_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(kSmemBytes)) != cudaSuccess)
+            return GSN_ERR_CUDA;
+        if (device >= 0 && device < 64) configured[device] = true;
+    }
+    dim3 grid(ceil_div(width, kT), ceil_div(height, kT), 3);
+    loss_gradient_kernel<<<grid, kThreads, kSmemBytes, stream>>>(image, target, grad, width, height, sums);
     return launched(1);
 }
 

@@ -1,25 +1,31 @@
 // (c) Per-tile front-to-back alpha blending.
 //
-// One CTA per 16x16 tile, one thread per pixel. The tile's sorted records are
-// staged into shared memory in batches of 256; while a batch is blended, every
-// thread already holds its slot of the next batch in registers (software
-// pipelining of the id -> record gather), so the gather latency overlaps the
-// blend. A CTA stops as soon as all of its pixels are saturated.
+// One 64-thread CTA per 16x16 tile, four pixels per thread, warp w owning the
+// 16x8 pixel strip of rows 8w..8w+7 (raster_common.cuh). The tile's sorted
+// records are staged into shared memory in batches of 128; while a batch is
+// blended every thread already holds its two slots of the next batch in
+// registers, so the id -> record gather overlaps the blend. Each record read from
+// shared memory serves the thread's four pixels.
+//
+// Per batch each warp tests the records against its strip (conservative
+// alpha >= 1/255 box) with four ballots and walks only the set bits, in order;
+// per pixel, powers below the record's alpha floor are rejected before expf.
+// Both tests only drop evaluations the exact per-pixel test would have skipped,
+// so the result is unchanged. A CTA stops as soon as all of its pixels are
+// saturated.
 //
 // The per-pixel arithmetic (power, alpha clamp at 0.99, the 1/255 skip and the
 // 1e-4 transmittance stop) is evaluated exactly as the reference does
 // (renderer.cu:273-338), so images are bit-identical for identical inputs.
 // Besides the image the kernel records, per pixel, how many records were
-// consumed before the pixel stopped contributing; the backward pass uses it to
-// bound its replay.
-#include "common.cuh"
+// consumed up to its last contribution; the backward pass bounds its replay
+// with it.
+#include "raster_common.cuh"
 #include "kernels.h"
 
 namespace gsn {
 
 namespace {
-
-constexpr int kBatch = 256;
 
 struct Staged {
     float2 mean;
@@ -43,68 +49,98 @@ __device__ __forceinline__ Staged fetch(const RasterForwardArgs& a, int64_t r, i
     return s;
 }
 
-__global__ void __launch_bounds__(kTilePixels) raster_forward_kernel(RasterForwardArgs a) {
-    __shared__ float2 s_mean[kBatch];
-    __shared__ float4 s_conic[kBatch];
-    __shared__ float3 s_color[kBatch];
+__global__ void __launch_bounds__(kRasterThreads) raster_forward_kernel(RasterForwardArgs a) {
+    __shared__ float2 s_mean[kRasterBatch];
+    __shared__ float4 s_conic[kRasterBatch];
+    __shared__ float3 s_color[kRasterBatch];
+    __shared__ float4 s_box[kRasterBatch];
+    __shared__ float s_floor[kRasterBatch];
 
     const int t = threadIdx.x;
-    const int tile = blockIdx.x;
-    const int tx = tile % a.cam.tile_count_x;
-    const int ty = tile / a.cam.tile_count_x;
-    const int px = tx * kTile + (t % kTile);
-    const int py = ty * kTile + (t / kTile);
-    const bool inside = px < a.cam.width && py < a.cam.height;
-    const float fx = static_cast<float>(px);
-    const float fy = static_cast<float>(py);
+    const int lane = t & 31;
+    const TileGeometry g = tile_geometry(a.cam);
+    const float fx = static_cast<float>(g.px);
+    float fy[kPixPerThread];
+    bool done[kPixPerThread];
+    float T[kPixPerThread];
+    float3 C[kPixPerThread];
+    int consumed[kPixPerThread];
+#pragma unroll
+    for (int p = 0; p < kPixPerThread; ++p) {
+        fy[p] = static_cast<float>(g.py[p]);
+        done[p] = !(g.px < a.cam.width && g.py[p] < a.cam.height);
+        T[p] = 1.0f;
+        C[p] = make_float3(0.f, 0.f, 0.f);
+        consumed[p] = 0;
+    }
 
-    const int64_t begin = a.tile_offsets[tile];
-    const int64_t end = a.tile_offsets[tile + 1];
+    const int64_t begin = a.tile_offsets[g.tile];
+    const int64_t end = a.tile_offsets[g.tile + 1];
 
-    bool done = !inside;
-    float T = 1.0f;
-    float3 C = make_float3(0.f, 0.f, 0.f);
-    int consumed = 0;  // 1 + index of the last contributing record
-
-    Staged next = fetch(a, begin + t, end);
-    for (int64_t base = begin; base < end; base += kBatch) {
-        if (__syncthreads_count(done) == kTilePixels) break;
-        s_mean[t] = next.mean;
-        s_conic[t] = next.conic;
-        s_color[t] = next.color;
+    Staged n0 = fetch(a, begin + t, end);
+    Staged n1 = fetch(a, begin + t + kRasterThreads, end);
+    for (int64_t base = begin; base < end; base += kRasterBatch) {
+        const bool mine = done[0] && done[1] && done[2] && done[3];
+        if (__syncthreads_and(mine)) break;
+        s_mean[t] = n0.mean;
+        s_conic[t] = n0.conic;
+        s_color[t] = n0.color;
+        s_box[t] = alpha_box(n0.mean, n0.conic);
+        s_floor[t] = alpha_floor(n0.conic.w);
+        s_mean[t + kRasterThreads] = n1.mean;
+        s_conic[t + kRasterThreads] = n1.conic;
+        s_color[t + kRasterThreads] = n1.color;
+        s_box[t + kRasterThreads] = alpha_box(n1.mean, n1.conic);
+        s_floor[t + kRasterThreads] = alpha_floor(n1.conic.w);
         __syncthreads();
-        next = fetch(a, base + kBatch + t, end);
-        const int batch = static_cast<int>(min(static_cast<int64_t>(kBatch), end - base));
-        for (int j = 0; !done && j < batch; ++j) {
-            float dx = s_mean[j].x - fx;
-            float dy = s_mean[j].y - fy;
-            float4 q = s_conic[j];
-            float power = -0.5f * (q.x * dx * dx + q.z * dy * dy) - q.y * dx * dy;
-            if (power > 0.0f) continue;
-            float alpha = fminf(kAlphaMax, q.w * expf(power));
-            if (alpha < kAlphaMin) continue;
-            float nextT = T * (1.0f - alpha);
-            if (nextT < kTransmittanceMin) {
-                done = true;
-                continue;
+        n0 = fetch(a, base + kRasterBatch + t, end);
+        n1 = fetch(a, base + kRasterBatch + kRasterThreads + t, end);
+        const int batch = static_cast<int>(min(static_cast<int64_t>(kRasterBatch), end - base));
+#pragma unroll 1
+        for (int k = 0; k < kRasterBatch / 32; ++k) {
+            const int jl = k * 32 + lane;
+            uint32_t m = __ballot_sync(0xffffffffu, jl < batch && box_hits(s_box[jl], g.sx0, g.sx1, g.sy0, g.sy1));
+            while (m && !(done[0] && done[1] && done[2] && done[3])) {
+                const int j = k * 32 + __ffs(m) - 1;
+                m &= m - 1;
+                const float2 mu = s_mean[j];
+                const float4 q = s_conic[j];
+                const float lim = s_floor[j];
+                const float dx = mu.x - fx;
+#pragma unroll
+                for (int p = 0; p < kPixPerThread; ++p) {
+                    if (done[p]) continue;
+                    float dy = mu.y - fy[p];
+                    float power = -0.5f * (q.x * dx * dx + q.z * dy * dy) - q.y * dx * dy;
+                    if (power > 0.0f || power < lim) continue;
+                    float alpha = fminf(kAlphaMax, q.w * expf(power));
+                    if (alpha < kAlphaMin) continue;
+                    float nextT = T[p] * (1.0f - alpha);
+                    if (nextT < kTransmittanceMin) {
+                        done[p] = true;
+                        continue;
+                    }
+                    float w = alpha * T[p];
+                    float3 c = s_color[j];
+                    C[p].x += c.x * w;
+                    C[p].y += c.y * w;
+                    C[p].z += c.z * w;
+                    T[p] = nextT;
+                    consumed[p] = static_cast<int>(base - begin) + j + 1;
+                }
             }
-            float w = alpha * T;
-            float3 c = s_color[j];
-            C.x += c.x * w;
-            C.y += c.y * w;
-            C.z += c.z * w;
-            T = nextT;
-            consumed = static_cast<int>(base - begin) + j + 1;
         }
     }
-    if (inside) {
-        const int64_t pix = static_cast<int64_t>(py) * a.cam.width + px;
+#pragma unroll
+    for (int p = 0; p < kPixPerThread; ++p) {
+        if (!(g.px < a.cam.width && g.py[p] < a.cam.height)) continue;
+        const int64_t pix = static_cast<int64_t>(g.py[p]) * a.cam.width + g.px;
         float* out = a.image + pix * 3;
-        out[0] = C.x + T * a.background.x;
-        out[1] = C.y + T * a.background.y;
-        out[2] = C.z + T * a.background.z;
-        if (a.final_transmittance) a.final_transmittance[pix] = T;
-        if (a.contributors) a.contributors[pix] = consumed;
+        out[0] = C[p].x + T[p] * a.background.x;
+        out[1] = C[p].y + T[p] * a.background.y;
+        out[2] = C[p].z + T[p] * a.background.z;
+        if (a.final_transmittance) a.final_transmittance[pix] = T[p];
+        if (a.contributors) a.contributors[pix] = consumed[p];
     }
 }
 
@@ -113,7 +149,7 @@ __global__ void __launch_bounds__(kTilePixels) raster_forward_kernel(RasterForwa
 int launch_raster_forward(const RasterForwardArgs& a, cudaStream_t stream) {
     int64_t tiles = static_cast<int64_t>(a.cam.tile_count_x) * a.cam.tile_count_y;
     if (tiles <= 0) return GSN_OK;
-    raster_forward_kernel<<<static_cast<unsigned>(tiles), kTilePixels, 0, stream>>>(a);
+    raster_forward_kernel<<<static_cast<unsigned>(tiles), kRasterThreads, 0, stream>>>(a);
     return launched(1);
 }
 

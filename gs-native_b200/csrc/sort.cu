@@ -117,9 +117,12 @@ __global__ void __launch_bounds__(kSortThreads) radix_scan(const int* n_dev, int
 }
 
 // Stable scatter. Warp w owns the w-th 512-key slice of the block's chunk and
-// walks it in 32-key steps; __match_any_sync ranks equal digits inside a step and
+// walks it in 32-key steps; eight ballots (one per digit bit) find the lanes with
+// an equal digit inside a step, and
 // warp-private counters carry the rank across steps, which keeps the original
-// order among equal digits.
+// order among equal digits. The ranked keys are first placed digit-sorted in
+// shared memory and then written out linearly, so each warp store covers a run
+// of consecutive addresses of one digit bucket instead of 32 scattered words.
 template <bool kIdentityValues>
 __global__ void __launch_bounds__(kSortThreads) radix_downsweep(
     const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ values_in,
@@ -127,10 +130,14 @@ __global__ void __launch_bounds__(kSortThreads) radix_downsweep(
     int bit, const uint32_t* __restrict__ block_hist, size_t hist_stride) {
     __shared__ uint32_t counts[kSortWarps][kBins];
     __shared__ uint32_t global_base[kBins];
+    __shared__ uint32_t local_base[kBins];
+    __shared__ uint32_t s_keys[kSortChunk];
+    __shared__ uint32_t s_vals[kSortChunk];
     const int n = load_count(n_dev, n_host);
     const int64_t start = static_cast<int64_t>(blockIdx.x) * kSortChunk;
     if (start >= n) return;
     const int64_t end = min(static_cast<int64_t>(n), start + kSortChunk);
+    const int total = static_cast<int>(end - start);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int i = threadIdx.x; i < kSortWarps * kBins; i += kSortThreads) (&counts[0][0])[i] = 0;
     global_base[threadIdx.x] = block_hist[threadIdx.x * hist_stride + blockIdx.x];
@@ -146,19 +153,23 @@ __global__ void __launch_bounds__(kSortThreads) radix_downsweep(
         key[s] = valid ? keys_in[idx] : 0u;
         if (kIdentityValues) val[s] = static_cast<uint32_t>(idx);
         else val[s] = valid ? values_in[idx] : 0u;
-        uint32_t digit = valid ? ((key[s] >> bit) & 0xFF) : 0x100u;
-        uint32_t peers = __match_any_sync(0xffffffffu, digit);
+        uint32_t digit = valid ? ((key[s] >> bit) & 0xFF) : 0u;
+        // lanes holding the same digit: intersect the eight per-bit ballots
+        uint32_t peers = __ballot_sync(0xffffffffu, valid);
+#pragma unroll
+        for (int b = 0; b < 8; ++b) {
+            uint32_t bal = __ballot_sync(0xffffffffu, (digit >> b) & 1u);
+            peers &= ((digit >> b) & 1u) ? bal : ~bal;
+        }
         uint32_t before = 0;
         if (valid) before = counts[warp][digit];
         __syncwarp();
-        rank[s] = before + __popc(peers & lt);
+        rank[s] = valid ? before + __popc(peers & lt) : 0xFFFFFFFFu;
         if (valid && (peers & lt) == 0) counts[warp][digit] = before + __popc(peers);
         __syncwarp();
-        key[s] = valid ? key[s] : 0xFFFFFFFFu;
-        if (!valid) rank[s] = 0xFFFFFFFFu;
     }
     __syncthreads();
-    {   // exclusive prefix over warps, one thread per digit
+    {   // exclusive prefix over warps per digit, then over digits for the block
         const int d = threadIdx.x;
         uint32_t run = 0;
 #pragma unroll
@@ -167,15 +178,38 @@ __global__ void __launch_bounds__(kSortThreads) radix_downsweep(
             counts[w][d] = run;
             run += c;
         }
+        // block-wide exclusive scan of the per-digit totals
+        uint32_t inc = run;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += y;
+        }
+        __shared__ uint32_t warp_tot[kSortWarps];
+        if (lane == 31) warp_tot[warp] = inc;
+        __syncthreads();
+        uint32_t prefix = 0;
+#pragma unroll
+        for (int w = 0; w < kSortWarps; ++w)
+            if (w < warp) prefix += warp_tot[w];
+        local_base[d] = prefix + inc - run;
     }
     __syncthreads();
 #pragma unroll
     for (int s = 0; s < kSortItems; ++s) {
         if (rank[s] == 0xFFFFFFFFu) continue;
         uint32_t digit = (key[s] >> bit) & 0xFF;
-        uint32_t pos = global_base[digit] + counts[warp][digit] + rank[s];
-        keys_out[pos] = key[s];
-        values_out[pos] = val[s];
+        uint32_t pos = local_base[digit] + counts[warp][digit] + rank[s];
+        s_keys[pos] = key[s];
+        s_vals[pos] = val[s];
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < total; j += kSortThreads) {
+        uint32_t k = s_keys[j];
+        uint32_t digit = (k >> bit) & 0xFF;
+        uint32_t pos = global_base[digit] + (j - local_base[digit]);
+        keys_out[pos] = k;
+        values_out[pos] = s_vals[j];
     }
 }
 
