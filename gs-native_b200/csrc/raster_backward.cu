@@ -119,34 +119,42 @@ __global__ void __launch_bounds__(kRasterThreads) raster_backward_kernel(RasterB
                 float v[kVals];
 #pragma unroll
                 for (int i = 0; i < kVals; ++i) v[i] = 0.0f;
-                bool has = false;
+                // four pixels evaluated without branches (selects only) so their
+                // dependency chains interleave
+                float pw[kPixPerThread], dyv[kPixPerThread];
+                bool act[kPixPerThread];
+                bool any = false;
 #pragma unroll
                 for (int p = 0; p < kPixPerThread; ++p) {
-                    if (!done[p] && rel + j >= limit[p]) done[p] = true;
-                    if (done[p]) continue;
-                    float dy = mu.y - fy[p];
-                    float power = -0.5f * (q.x * dx * dx + q.z * dy * dy) - q.y * dx * dy;
-                    if (power > 0.0f || power < lim) continue;
-                    float raw = q.w * expf(power);
-                    float alpha = fminf(kAlphaMax, raw);
-                    if (alpha < kAlphaMin) continue;
-                    float nextT = T[p] * (1.0f - alpha);
-                    if (nextT < kTransmittanceMin) {
-                        done[p] = true;
-                        continue;
-                    }
-                    has = true;
-                    float w = alpha * T[p];
-                    float inv = 1.0f / (1.0f - alpha);
-                    float dalpha = 0.0f;
+                    done[p] = done[p] || rel + j >= limit[p];
+                    dyv[p] = mu.y - fy[p];
+                    pw[p] = -0.5f * (q.x * dx * dx + q.z * dyv[p] * dyv[p]) - q.y * dx * dyv[p];
+                    act[p] = !done[p] && !(pw[p] > 0.0f) && !(pw[p] < lim);
+                    any |= act[p];
+                }
+                bool has = false;
+                if (any) {
 #pragma unroll
-                    for (int c = 0; c < 3; ++c) {
-                        dalpha += gI[p][c] * (prefix[p][c] + T[p] * cc[c] - fin[p][c]);
-                        v[6 + c] += w * gI[p][c];
-                    }
-                    dalpha *= inv;
-                    if (raw < kAlphaMax) {
-                        float common = dalpha * raw;
+                    for (int p = 0; p < kPixPerThread; ++p) {
+                        const float dy = dyv[p];
+                        float raw = q.w * expf(pw[p]);
+                        float alpha = fminf(kAlphaMax, raw);
+                        bool take = act[p] && !(alpha < kAlphaMin);
+                        float nextT = T[p] * (1.0f - alpha);
+                        bool stop = take && nextT < kTransmittanceMin;
+                        done[p] = done[p] || stop;
+                        take = take && !stop;
+                        has |= take;
+                        float w = alpha * T[p];
+                        float inv = __frcp_rn(1.0f - alpha);
+                        float dalpha = 0.0f;
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) {
+                            dalpha += gI[p][c] * (prefix[p][c] + T[p] * cc[c] - fin[p][c]);
+                            v[6 + c] += take ? w * gI[p][c] : 0.0f;
+                        }
+                        dalpha *= inv;
+                        float common = (take && raw < kAlphaMax) ? dalpha * raw : 0.0f;
                         float qx = q.x * dx + q.y * dy;
                         float qy = q.y * dx + q.z * dy;
                         v[0] += -common * qx;
@@ -157,10 +165,10 @@ __global__ void __launch_bounds__(kRasterThreads) raster_backward_kernel(RasterB
                         v[5] += common * (1.0f - q.w);
                         v[9] += fabsf(common * qx);
                         v[10] += fabsf(common * qy);
-                    }
 #pragma unroll
-                    for (int c = 0; c < 3; ++c) prefix[p][c] += cc[c] * w;
-                    T[p] = nextT;
+                        for (int c = 0; c < 3; ++c) prefix[p][c] = take ? prefix[p][c] + cc[c] * w : prefix[p][c];
+                        T[p] = take ? nextT : T[p];
+                    }
                 }
                 if (__any_sync(0xffffffffu, has)) {
                     // butterfly reduce-scatter of the 12 slots (slot 11 is padding)

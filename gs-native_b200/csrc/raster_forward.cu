@@ -106,27 +106,36 @@ __global__ void __launch_bounds__(kRasterThreads) raster_forward_kernel(RasterFo
                 const float2 mu = s_mean[j];
                 const float4 q = s_conic[j];
                 const float lim = s_floor[j];
+                const float3 c = s_color[j];
                 const float dx = mu.x - fx;
+                // the four pixels are evaluated without branches (selects only),
+                // so their dependency chains interleave; values of a pixel that
+                // does not take the record are computed but discarded
+                float pw[kPixPerThread];
+                bool act[kPixPerThread];
+                bool any = false;
 #pragma unroll
                 for (int p = 0; p < kPixPerThread; ++p) {
-                    if (done[p]) continue;
                     float dy = mu.y - fy[p];
-                    float power = -0.5f * (q.x * dx * dx + q.z * dy * dy) - q.y * dx * dy;
-                    if (power > 0.0f || power < lim) continue;
-                    float alpha = fminf(kAlphaMax, q.w * expf(power));
-                    if (alpha < kAlphaMin) continue;
+                    pw[p] = -0.5f * (q.x * dx * dx + q.z * dy * dy) - q.y * dx * dy;
+                    act[p] = !done[p] && !(pw[p] > 0.0f) && !(pw[p] < lim);
+                    any |= act[p];
+                }
+                if (!any) continue;
+#pragma unroll
+                for (int p = 0; p < kPixPerThread; ++p) {
+                    float alpha = fminf(kAlphaMax, q.w * expf(pw[p]));
+                    bool take = act[p] && !(alpha < kAlphaMin);
                     float nextT = T[p] * (1.0f - alpha);
-                    if (nextT < kTransmittanceMin) {
-                        done[p] = true;
-                        continue;
-                    }
+                    bool stop = take && nextT < kTransmittanceMin;
+                    done[p] = done[p] || stop;
+                    take = take && !stop;
                     float w = alpha * T[p];
-                    float3 c = s_color[j];
-                    C[p].x += c.x * w;
-                    C[p].y += c.y * w;
-                    C[p].z += c.z * w;
-                    T[p] = nextT;
-                    consumed[p] = static_cast<int>(base - begin) + j + 1;
+                    C[p].x = take ? C[p].x + c.x * w : C[p].x;
+                    C[p].y = take ? C[p].y + c.y * w : C[p].y;
+                    C[p].z = take ? C[p].z + c.z * w : C[p].z;
+                    T[p] = take ? nextT : T[p];
+                    consumed[p] = take ? static_cast<int>(base - begin) + j + 1 : consumed[p];
                 }
             }
         }
