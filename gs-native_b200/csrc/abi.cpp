@@ -7,6 +7,7 @@
 
 #include "core/render/renderer.h"
 #include "core/solver/solver.h"
+#include "kernels.h"
 #include "profile.h"
 
 struct gsn_renderer {
@@ -70,6 +71,29 @@ int gsn_profile_collect(double* ms, int count) {
 const char* gsn_stage_name(int stage) { return gsn::stage_name(stage); }
 
 int gsn_stage_count(void) { return gsn::kStageCount; }
+
+int gsn_sort_pairs_workspace(int max_count, size_t* bytes) {
+    if (!bytes || max_count < 0) return GSN_ERR_INVALID_ARGUMENT;
+    *bytes = gsn::radix_sort_scratch_bytes(max_count);
+    return GSN_OK;
+}
+
+int gsn_sort_pairs(uint32_t* keys, uint32_t* values, uint32_t* keys_alt, uint32_t* values_alt, int count,
+                   int begin_bit, int end_bit, void* workspace, size_t workspace_bytes, int* result_in_alt,
+                   void* stream) {
+    if (!result_in_alt || count < 0 || begin_bit < 0 || end_bit > 32 || end_bit < begin_bit) return GSN_ERR_INVALID_ARGUMENT;
+    *result_in_alt = 0;
+    if (count == 0 || end_bit == begin_bit) return GSN_OK;
+    if (!keys || !values || !keys_alt || !values_alt || !workspace ||
+        workspace_bytes < gsn::radix_sort_scratch_bytes(count))
+        return GSN_ERR_INVALID_ARGUMENT;
+    gsn::RadixSortScratch scratch = gsn::radix_sort_scratch(workspace, count);
+    bool alt = false;
+    int status = gsn::launch_radix_sort(keys, values, keys_alt, values_alt, false, count, nullptr, begin_bit, end_bit,
+                                        scratch, &alt, AsStream(stream));
+    *result_in_alt = alt ? 1 : 0;
+    return status;
+}
 
 int gsn_renderer_create(gsn_renderer** out) {
     if (!out) return GSN_ERR_INVALID_ARGUMENT;

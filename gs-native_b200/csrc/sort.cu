@@ -38,7 +38,7 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
 
 // Per-block digit histogram of one 8-bit digit.
 __global__ void __launch_bounds__(kSortThreads) radix_upsweep(const uint32_t* __restrict__ keys,
-                                                              const int* n_dev, int n_host, int bit,
+                                                              const int* n_dev, int n_host, int bit, uint32_t mask,
                                                               uint32_t* __restrict__ block_hist,
                                                               size_t hist_stride,
                                                               uint32_t* __restrict__ digit_total) {
@@ -53,7 +53,7 @@ __global__ void __launch_bounds__(kSortThreads) radix_upsweep(const uint32_t* __
 #pragma unroll 4
     for (int k = 0; k < kSortItems; ++k) {
         int64_t idx = start + k * kSortThreads + threadIdx.x;
-        if (idx < end) atomicAdd(&hist[warp][(__ldg(keys + idx) >> bit) & 0xFF], 1u);
+        if (idx < end) atomicAdd(&hist[warp][(__ldg(keys + idx) >> bit) & mask], 1u);
     }
     __syncthreads();
     const int d = threadIdx.x;
@@ -127,7 +127,7 @@ template <bool kIdentityValues>
 __global__ void __launch_bounds__(kSortThreads) radix_downsweep(
     const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ values_in,
     uint32_t* __restrict__ keys_out, uint32_t* __restrict__ values_out, const int* n_dev, int n_host,
-    int bit, const uint32_t* __restrict__ block_hist, size_t hist_stride) {
+    int bit, uint32_t mask, const uint32_t* __restrict__ block_hist, size_t hist_stride) {
     __shared__ uint32_t counts[kSortWarps][kBins];
     __shared__ uint32_t global_base[kBins];
     __shared__ uint32_t local_base[kBins];
@@ -153,7 +153,7 @@ __global__ void __launch_bounds__(kSortThreads) radix_downsweep(
         key[s] = valid ? keys_in[idx] : 0u;
         if (kIdentityValues) val[s] = static_cast<uint32_t>(idx);
         else val[s] = valid ? values_in[idx] : 0u;
-        uint32_t digit = valid ? ((key[s] >> bit) & 0xFF) : 0u;
+        uint32_t digit = valid ? ((key[s] >> bit) & mask) : 0u;
         // lanes holding the same digit: intersect the eight per-bit ballots
         uint32_t peers = __ballot_sync(0xffffffffu, valid);
 #pragma unroll
@@ -198,7 +198,7 @@ __global__ void __launch_bounds__(kSortThreads) radix_downsweep(
 #pragma unroll
     for (int s = 0; s < kSortItems; ++s) {
         if (rank[s] == 0xFFFFFFFFu) continue;
-        uint32_t digit = (key[s] >> bit) & 0xFF;
+        uint32_t digit = (key[s] >> bit) & mask;
         uint32_t pos = local_base[digit] + counts[warp][digit] + rank[s];
         s_keys[pos] = key[s];
         s_vals[pos] = val[s];
@@ -206,7 +206,7 @@ __global__ void __launch_bounds__(kSortThreads) radix_downsweep(
     __syncthreads();
     for (int j = threadIdx.x; j < total; j += kSortThreads) {
         uint32_t k = s_keys[j];
-        uint32_t digit = (k >> bit) & 0xFF;
+        uint32_t digit = (k >> bit) & mask;
         uint32_t pos = global_base[digit] + (j - local_base[digit]);
         keys_out[pos] = k;
         values_out[pos] = s_vals[j];
@@ -387,17 +387,19 @@ int launch_radix_sort(uint32_t* keys, uint32_t* values, uint32_t* keys_alt, uint
     uint32_t *kin = keys, *vin = values, *kout = keys_alt, *vout = values_alt;
     for (int p = 0; p < passes; ++p) {
         int bit = begin_bit + 8 * p;
+        // the last pass only looks at the bits below end_bit
+        uint32_t mask = end_bit - bit >= 8 ? 0xFFu : ((1u << (end_bit - bit)) - 1u);
         uint32_t* dt = scratch.digit_total + kBins * p;
-        radix_upsweep<<<blocks, kSortThreads, 0, stream>>>(kin, count_device, max_count, bit,
+        radix_upsweep<<<blocks, kSortThreads, 0, stream>>>(kin, count_device, max_count, bit, mask,
                                                            scratch.block_hist, scratch.max_blocks, dt);
         radix_scan<<<kBins, kSortThreads, 0, stream>>>(count_device, max_count, scratch.block_hist,
                                                        scratch.max_blocks, dt);
         if (identity_values && p == 0)
             radix_downsweep<true><<<blocks, kSortThreads, 0, stream>>>(
-                kin, nullptr, kout, vout, count_device, max_count, bit, scratch.block_hist, scratch.max_blocks);
+                kin, nullptr, kout, vout, count_device, max_count, bit, mask, scratch.block_hist, scratch.max_blocks);
         else
             radix_downsweep<false><<<blocks, kSortThreads, 0, stream>>>(
-                kin, vin, kout, vout, count_device, max_count, bit, scratch.block_hist, scratch.max_blocks);
+                kin, vin, kout, vout, count_device, max_count, bit, mask, scratch.block_hist, scratch.max_blocks);
         uint32_t* tk = kin; kin = kout; kout = tk;
         uint32_t* tv = vin; vin = vout; vout = tv;
     }

@@ -83,6 +83,8 @@ def lib():
         "gsn_profile_collect": ([P(ctypes.c_double), i32], i32),
         "gsn_stage_name": ([i32], ctypes.c_char_p),
         "gsn_stage_count": ([], i32),
+        "gsn_sort_pairs_workspace": ([i32, P(ctypes.c_size_t)], i32),
+        "gsn_sort_pairs": ([vp, vp, vp, vp, i32, i32, i32, vp, ctypes.c_size_t, P(i32), vp], i32),
         "gsn_renderer_create": ([P(vp)], i32),
         "gsn_renderer_destroy": ([vp], i32),
         "gsn_renderer_set_stream": ([vp, vp], i32),
@@ -179,6 +181,22 @@ def profile_collect():
     ms = (ctypes.c_double * n)()
     _check(lib().gsn_profile_collect(ms, n), "profile_collect")
     return {lib().gsn_stage_name(k).decode(): ms[k] for k in range(n)}
+
+
+def sort_pairs_workspace(max_count):
+    b = ctypes.c_size_t()
+    _check(lib().gsn_sort_pairs_workspace(int(max_count), ctypes.byref(b)), "sort_pairs_workspace")
+    return b.value
+
+
+def sort_pairs(keys, values, keys_alt, values_alt, count, begin_bit, end_bit, workspace, workspace_bytes, stream=0):
+    """Returns (status, result_in_alt)."""
+    alt = ctypes.c_int()
+    st = lib().gsn_sort_pairs(ctypes.c_void_p(keys), ctypes.c_void_p(values), ctypes.c_void_p(keys_alt),
+                              ctypes.c_void_p(values_alt), int(count), int(begin_bit), int(end_bit),
+                              ctypes.c_void_p(workspace), ctypes.c_size_t(workspace_bytes), ctypes.byref(alt),
+                              ctypes.c_void_p(stream))
+    return st, alt.value
 
 
 def memcpy_async(dst, src, nbytes, stream):

@@ -53,6 +53,24 @@ int gsn_profile_collect(double* ms, int count);
 const char* gsn_stage_name(int stage);
 int gsn_stage_count(void);
 
+/* ------------------------------------------------------------------ ordering
+ * Stable LSD radix sort of (uint32 key, uint32 value) pairs: the ordering
+ * primitive of the tile records, used where the reference calls
+ * cub::DeviceRadixSort::SortPairs (renderer.cu:541-563). Keys are sorted on bits
+ * [begin_bit, end_bit) (end_bit - begin_bit <= 32), ties keep their input order.
+ * The data ping-pongs between (keys, values) and (keys_alt, values_alt); on
+ * return *result_in_alt (host int) tells which pair holds the sorted output.
+ * All arrays are device memory of `count` elements.
+ */
+
+/* Device workspace bytes gsn_sort_pairs needs for up to max_count pairs. */
+int gsn_sort_pairs_workspace(int max_count, size_t* bytes);
+
+/* Sorts with a caller-provided device workspace of gsn_sort_pairs_workspace bytes. */
+int gsn_sort_pairs(uint32_t* keys, uint32_t* values, uint32_t* keys_alt, uint32_t* values_alt, int count,
+                   int begin_bit, int end_bit, void* workspace, size_t workspace_bytes, int* result_in_alt,
+                   void* stream);
+
 /* ------------------------------------------------------------------ renderer
  * Replaces gs_native::Renderer (reference src/core/render/renderer.h:10-89).
  */
