@@ -95,6 +95,20 @@ int gsn_sort_pairs(uint32_t* keys, uint32_t* values, uint32_t* keys_alt, uint32_
     return status;
 }
 
+int gsn_sort_pairs_noalloc(uint32_t* keys, uint32_t* values, uint32_t* keys_alt, uint32_t* values_alt, int count,
+                           int begin_bit, int end_bit, int* result_in_alt, void* stream) {
+    if (!result_in_alt || count < 0 || begin_bit < 0 || end_bit > 32 || end_bit < begin_bit) return GSN_ERR_INVALID_ARGUMENT;
+    *result_in_alt = 0;
+    if (count > gsn::noalloc_sort_max_count()) return GSN_ERR_CAPACITY;
+    if (count == 0 || end_bit == begin_bit) return GSN_OK;
+    if (!keys || !values || !keys_alt || !values_alt) return GSN_ERR_INVALID_ARGUMENT;
+    bool alt = false;
+    int status = gsn::launch_radix_sort_noalloc(keys, values, keys_alt, values_alt, count, begin_bit, end_bit, &alt,
+                                                AsStream(stream));
+    *result_in_alt = alt ? 1 : 0;
+    return status;
+}
+
 int gsn_renderer_create(gsn_renderer** out) {
     if (!out) return GSN_ERR_INVALID_ARGUMENT;
     *out = new (std::nothrow) gsn_renderer();

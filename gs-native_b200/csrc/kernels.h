@@ -45,6 +45,12 @@ int launch_radix_sort(uint32_t* keys, uint32_t* values, uint32_t* keys_alt, uint
                       int end_bit, const RadixSortScratch& scratch, bool* result_in_alt,
                       cudaStream_t stream);
 
+// Same sort with its scratch in a static device array of the library (no
+// allocation); count <= noalloc_sort_max_count(), else GSN_ERR_CAPACITY.
+int noalloc_sort_max_count();
+int launch_radix_sort_noalloc(uint32_t* keys, uint32_t* values, uint32_t* keys_alt, uint32_t* values_alt, int count,
+                              int begin_bit, int end_bit, bool* result_in_alt, cudaStream_t stream);
+
 // Exclusive prefix sum of 32-bit integers, in -> out (in-place allowed), n + 1
 // outputs with out[n] = total. `gather` (optional) reads in[gather[i]] instead of
 // in[i]. Scratch: scan_scratch_bytes(n).

@@ -16,6 +16,8 @@
 #include "common.cuh"
 #include "kernels.h"
 
+#include <mutex>
+
 namespace gsn {
 
 namespace {
@@ -405,6 +407,45 @@ int launch_radix_sort(uint32_t* keys, uint32_t* values, uint32_t* keys_alt, uint
     }
     *result_in_alt = (passes % 2) == 1;
     return launched(3 * passes);
+}
+
+// ---------------------------------------------------------------- no-alloc sort
+// Scratch of gsn_sort_pairs_noalloc: the digit totals and per-block histograms
+// of the sort for up to kNoAllocMaxCount pairs, in a file-scope device array
+// (4.2 MB on every GPU that loads the library, held until exit). Host code
+// cannot use the array's name as a device address, so its address is looked up
+// once per device with cudaGetSymbolAddress.
+constexpr int kNoAllocMaxCount = 1 << 24;
+constexpr size_t kNoAllocScratchWords =
+    static_cast<size_t>(kBins) * (kNoAllocMaxCount / kSortChunk) + kBins * 4 + 64;
+static __device__ __align__(256) uint32_t g_noalloc_sort_scratch[kNoAllocScratchWords];
+
+int noalloc_sort_max_count() { return kNoAllocMaxCount; }
+
+int launch_radix_sort_noalloc(uint32_t* keys, uint32_t* values, uint32_t* keys_alt, uint32_t* values_alt, int count,
+                              int begin_bit, int end_bit, bool* result_in_alt, cudaStream_t stream) {
+    *result_in_alt = false;
+    if (count > kNoAllocMaxCount) return GSN_ERR_CAPACITY;
+    static std::mutex mutex;
+    static void* scratch_address[64] = {};
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= 64) return GSN_ERR_CUDA;
+    void* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(mutex);
+        if (!scratch_address[device]) {
+            void* p = nullptr;
+            if (cudaGetSymbolAddress(&p, g_noalloc_sort_scratch) != cudaSuccess || !p) return GSN_ERR_CUDA;
+            scratch_address[device] = p;
+        }
+        base = scratch_address[device];
+    }
+    // the layout for `count` pairs is a prefix of the array; the digit totals
+    // are cleared by launch_radix_sort and every histogram word is written
+    // before it is read, so nothing left by an earlier call is used
+    RadixSortScratch scratch = radix_sort_scratch(base, count);
+    return launch_radix_sort(keys, values, keys_alt, values_alt, false, count, nullptr, begin_bit, end_bit, scratch,
+                             result_in_alt, stream);
 }
 
 size_t scan_scratch_bytes(int n) {

@@ -71,6 +71,29 @@ int gsn_sort_pairs(uint32_t* keys, uint32_t* values, uint32_t* keys_alt, uint32_
                    int begin_bit, int end_bit, void* workspace, size_t workspace_bytes, int* result_in_alt,
                    void* stream);
 
+/* Allocation-free variant of gsn_sort_pairs (no counterpart in the reference).
+ *
+ * For callers that cannot allocate device memory themselves or let a library do
+ * it: code running under an allocator that owns the whole device budget (a
+ * framework's caching allocator or a fixed arena, where a stray cudaMalloc would
+ * exceed the budget or fragment the pool), and latency-critical loops that cannot
+ * take the device-wide synchronisation that cudaMalloc/cudaFree imply. The caller
+ * still passes all four key/value arrays; the sort's histogram scratch lives in a
+ * static device array inside the library, sized for at most
+ * GSN_SORT_NOALLOC_MAX_COUNT pairs (4.2 MB, reserved on every GPU that loads the
+ * library until the process exits). Larger counts return GSN_ERR_CAPACITY and
+ * launch nothing. The function calls no cudaMalloc/cudaFree.
+ *
+ * The first call on a device looks up the scratch array's device address
+ * (cudaGetSymbolAddress, with that device current); make that first call before
+ * any stream capture. All calls share the one array and it keeps the previous
+ * call's contents (the sort clears what it needs): calls that overlap on the GPU,
+ * on different streams of the same device, race on it and must be serialised by
+ * the caller. Results are identical to gsn_sort_pairs. */
+#define GSN_SORT_NOALLOC_MAX_COUNT 16777216
+int gsn_sort_pairs_noalloc(uint32_t* keys, uint32_t* values, uint32_t* keys_alt, uint32_t* values_alt, int count,
+                           int begin_bit, int end_bit, int* result_in_alt, void* stream);
+
 /* ------------------------------------------------------------------ renderer
  * Replaces gs_native::Renderer (reference src/core/render/renderer.h:10-89).
  */
