@@ -5,6 +5,7 @@
 
 #include <new>
 
+#include "core/density/density_controller.h"
 #include "core/render/renderer.h"
 #include "core/solver/solver.h"
 #include "kernels.h"
@@ -16,6 +17,10 @@ struct gsn_renderer {
 
 struct gsn_solver {
     gs_native::Solver impl;
+};
+
+struct gsn_density {
+    gs_native::DensityController impl;
 };
 
 namespace {
@@ -51,6 +56,15 @@ int gsn_memcpy_async(void* dst, const void* src, size_t bytes, void* stream) {
     return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, AsStream(stream)) == cudaSuccess ? GSN_OK
                                                                                                : GSN_ERR_CUDA;
 }
+
+int gsn_device_alloc(size_t bytes, void** out) {
+    if (!out) return GSN_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    if (bytes == 0) return GSN_OK;
+    return cudaMalloc(out, bytes) == cudaSuccess ? GSN_OK : GSN_ERR_OUT_OF_MEMORY;
+}
+
+int gsn_device_free(void* ptr) { return cudaFree(ptr) == cudaSuccess ? GSN_OK : GSN_ERR_CUDA; }
 
 int gsn_stream_synchronize(void* stream) {
     return cudaStreamSynchronize(AsStream(stream)) == cudaSuccess ? GSN_OK : GSN_ERR_CUDA;
@@ -274,6 +288,83 @@ int gsn_solver_moments(gsn_solver* s, float** first, float** second, uint64_t* i
     *first = s->impl.GetFirstMoments();
     *second = s->impl.GetSecondMoments();
     *iteration = s->impl.GetIteration();
+    return GSN_OK;
+}
+
+int gsn_density_create(gsn_density** out) {
+    if (!out) return GSN_ERR_INVALID_ARGUMENT;
+    *out = new (std::nothrow) gsn_density();
+    return *out ? GSN_OK : GSN_ERR_OUT_OF_MEMORY;
+}
+
+int gsn_density_destroy(gsn_density* d) {
+    delete d;
+    return GSN_OK;
+}
+
+int gsn_density_set_stream(gsn_density* d, void* stream) {
+    if (!d) return GSN_ERR_INVALID_ARGUMENT;
+    d->impl.SetStream(AsStream(stream));
+    return GSN_OK;
+}
+
+int gsn_density_initialize(gsn_density* d, int count, int capacity) {
+    if (!d) return GSN_ERR_INVALID_ARGUMENT;
+    return d->impl.Initialize(count, capacity) ? GSN_OK : GSN_ERR_INVALID_ARGUMENT;
+}
+
+int gsn_density_accumulate(gsn_density* d, const float* statistics, const float* absolute_statistics, int count) {
+    if (!d) return GSN_ERR_INVALID_ARGUMENT;
+    return d->impl.AccumulateStatistics(statistics, absolute_statistics, count) ? GSN_OK : GSN_ERR_INVALID_ARGUMENT;
+}
+
+int gsn_density_accumulate_observations(gsn_density* d, const float* gradients, const float* radii, const int* ids,
+                                        int observations) {
+    if (!d) return GSN_ERR_INVALID_ARGUMENT;
+    return d->impl.AccumulateStatistics(gradients, radii, ids, observations) ? GSN_OK : GSN_ERR_INVALID_ARGUMENT;
+}
+
+int gsn_density_reset_opacity(gsn_density* d, float* params, int stride, float max_opacity) {
+    if (!d) return GSN_ERR_INVALID_ARGUMENT;
+    return d->impl.ResetOpacity(params, stride, max_opacity) ? GSN_OK : GSN_ERR_INVALID_ARGUMENT;
+}
+
+int gsn_density_control(gsn_density* d, float** params, int* count, float scene_extent, float gradient_threshold,
+                        float percent_dense, float min_opacity, float max_screen_size, unsigned long long seed,
+                        int* changes, float absolute_gradient_threshold) {
+    if (!d || !params || !count) return GSN_ERR_INVALID_ARGUMENT;
+    gs_native::GaussianBuffers g;
+    g.gaussians_ = *params;
+    g.gaussian_count_ = *count;
+    if (!d->impl.ControlDensity(g, scene_extent, gradient_threshold, percent_dense, min_opacity, max_screen_size, seed,
+                                changes, absolute_gradient_threshold))
+        return GSN_ERR_INVALID_ARGUMENT;
+    *params = g.gaussians_;
+    *count = g.gaussian_count_;
+    return GSN_OK;
+}
+
+int gsn_density_buffers(gsn_density* d, const int** history_parent_ids, const int** control, const int** parent_ids) {
+    if (!d || !history_parent_ids || !control || !parent_ids) return GSN_ERR_INVALID_ARGUMENT;
+    *history_parent_ids = d->impl.GetHistoryParentIds();
+    *control = d->impl.GetGaussianCount();
+    *parent_ids = d->impl.GetParentIds();
+    return GSN_OK;
+}
+
+int gsn_density_set_max_gaussians(gsn_density* d, int max_gaussians) {
+    if (!d || max_gaussians < 0) return GSN_ERR_INVALID_ARGUMENT;
+    d->impl.SetMaxGaussians(max_gaussians);
+    return GSN_OK;
+}
+
+int gsn_density_internals(gsn_density* d, const float** samples, float** gradient_sums, float** absolute_sums,
+                          unsigned int** observation_counts) {
+    if (!d || !samples || !gradient_sums || !absolute_sums || !observation_counts) return GSN_ERR_INVALID_ARGUMENT;
+    *samples = d->impl.GetSamples();
+    *gradient_sums = d->impl.GetGradientSums();
+    *absolute_sums = d->impl.GetAbsoluteGradientSums();
+    *observation_counts = d->impl.GetObservationCounts();
     return GSN_OK;
 }
 

@@ -1,0 +1,72 @@
+// Launchers of the density-control kernels (density.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "kernels.h"
+
+namespace gsn {
+
+struct DensityThresholds {
+    float gradient_threshold;           // mean view-space gradient for densification
+    float split_threshold;              // percent_dense * scene extent
+    float min_opacity;
+    float max_world_size;               // 0.1 * scene extent
+    float absolute_gradient_threshold;  // > 0: splits use the absolute statistic
+    bool prune_large;
+};
+
+// Control block: int[8] (count, next count, status, split-sampled, survivors,
+// clones, kept splits, previous count) followed by two u64 Philox offsets.
+constexpr size_t kDensityControlBytes = 8 * sizeof(int) + 2 * sizeof(unsigned long long);
+
+struct DensityDecideArgs {
+    const float* params;
+    const float* sums;
+    const float* abs_sums;
+    const unsigned int* obs;
+    int* control;
+    int4* counts;       // [n + 1] (keep, clone, split sampled, split kept)
+    int4* offsets;      // [n + 1] exclusive scan of counts
+    int4* scan_scratch;  // density_scan_scratch_bytes(n)
+    int* additions;     // [n + 1] (cap only)
+    void* int_scan_scratch;  // scan_scratch_bytes(n) (cap only)
+    int n;
+    int max_count;      // 0 = no cap
+    int random_blocks;
+    DensityThresholds th;
+};
+
+struct DensityApplyArgs {
+    const float* params;
+    const int4* counts;
+    const int4* offsets;
+    int* control;
+    float* samples;     // >= 6 * n floats
+    float* out;         // 58 x out_stride
+    int* history_parents;  // may be null
+    int* parents;
+    float* new_flags;
+    float* sums;
+    float* abs_sums;
+    unsigned int* obs;
+    int n;
+    int out_stride;
+    int random_blocks;
+    unsigned long long seed;
+};
+
+int launch_density_init(int* control, int count, cudaStream_t s);
+int launch_density_accumulate(const float* stats, const float* abs_stats, const int* control, float* sums,
+                              float* abs_sums, unsigned int* counts, int n, cudaStream_t s);
+int launch_density_accumulate_observations(const float* grads, const float* radii, const int* ids, const int* control,
+                                           float* sums, unsigned int* counts, int observations, cudaStream_t s);
+size_t density_scan_scratch_bytes(int n);
+int launch_density_decide(const DensityDecideArgs& a, cudaStream_t s);
+int launch_density_prepare(const int4* offsets, int* control, int n, int random_blocks, cudaStream_t s);
+int launch_density_apply(const DensityApplyArgs& a, cudaStream_t s);
+int launch_density_reset_opacity(const int* control, float* params, int stride, float max_logit, cudaStream_t s);
+
+}  // namespace gsn

@@ -78,6 +78,8 @@ def lib():
         "gsn_memcpy": ([vp, vp, ctypes.c_size_t], i32),
         "gsn_memcpy_async": ([vp, vp, ctypes.c_size_t, vp], i32),
         "gsn_stream_synchronize": ([vp], i32),
+        "gsn_device_alloc": ([ctypes.c_size_t, P(vp)], i32),
+        "gsn_device_free": ([vp], i32),
         "gsn_kernel_launch_count": ([], ctypes.c_uint64),
         "gsn_profile_enable": ([i32], i32),
         "gsn_profile_collect": ([P(ctypes.c_double), i32], i32),
@@ -199,6 +201,16 @@ def sort_pairs(keys, values, keys_alt, values_alt, count, begin_bit, end_bit, wo
     return st, alt.value
 
 
+def device_alloc(nbytes):
+    p = ctypes.c_void_p()
+    _check(lib().gsn_device_alloc(ctypes.c_size_t(nbytes), ctypes.byref(p)), "gsn_device_alloc")
+    return p.value or 0
+
+
+def device_free(ptr):
+    _check(lib().gsn_device_free(ctypes.c_void_p(ptr)), "gsn_device_free")
+
+
 def memcpy_async(dst, src, nbytes, stream):
     _check(lib().gsn_memcpy_async(ctypes.c_void_p(dst), ctypes.c_void_p(src), ctypes.c_size_t(nbytes),
                                   ctypes.c_void_p(stream)), "gsn_memcpy_async")
@@ -284,3 +296,81 @@ class Solver:
         a, b, it = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_uint64()
         _check(lib().gsn_solver_moments(self.handle, ctypes.byref(a), ctypes.byref(b), ctypes.byref(it)), "moments")
         return a.value, b.value, it.value
+
+
+class Density:
+    """Handle over gs_native::DensityController (reference density_controller.h:9-83)."""
+
+    def __init__(self):
+        L = lib()
+        vp, i32, f32, P = ctypes.c_void_p, ctypes.c_int, ctypes.c_float, ctypes.POINTER
+        sigs = {
+            "gsn_density_create": [P(vp)], "gsn_density_destroy": [vp], "gsn_density_set_stream": [vp, vp],
+            "gsn_density_initialize": [vp, i32, i32], "gsn_density_accumulate": [vp, vp, vp, i32],
+            "gsn_density_accumulate_observations": [vp, vp, vp, vp, i32],
+            "gsn_density_reset_opacity": [vp, vp, i32, f32],
+            "gsn_density_control": [vp, P(vp), P(i32), f32, f32, f32, f32, f32, ctypes.c_ulonglong, P(i32), f32],
+            "gsn_density_buffers": [vp, P(vp), P(vp), P(vp)], "gsn_density_set_max_gaussians": [vp, i32],
+            "gsn_density_internals": [vp, P(vp), P(vp), P(vp), P(vp)],
+        }
+        for name, args in sigs.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = i32
+        h = ctypes.c_void_p()
+        _check(L.gsn_density_create(ctypes.byref(h)), "gsn_density_create")
+        self.handle = h
+
+    def close(self):
+        if self.handle:
+            lib().gsn_density_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream):
+        _check(lib().gsn_density_set_stream(self.handle, ctypes.c_void_p(stream)), "set_stream")
+
+    def initialize(self, count, capacity):
+        return lib().gsn_density_initialize(self.handle, int(count), int(capacity))
+
+    def accumulate(self, stats_ptr, abs_ptr, count):
+        return lib().gsn_density_accumulate(self.handle, ctypes.c_void_p(stats_ptr), ctypes.c_void_p(abs_ptr),
+                                            int(count))
+
+    def accumulate_observations(self, grads_ptr, radii_ptr, ids_ptr, observations):
+        return lib().gsn_density_accumulate_observations(self.handle, ctypes.c_void_p(grads_ptr),
+                                                         ctypes.c_void_p(radii_ptr), ctypes.c_void_p(ids_ptr),
+                                                         int(observations))
+
+    def reset_opacity(self, params_ptr, stride, max_opacity=0.01):
+        return lib().gsn_density_reset_opacity(self.handle, ctypes.c_void_p(params_ptr), int(stride),
+                                               float(max_opacity))
+
+    def control(self, params_ptr, count, extent, grad_thr=0.0002, percent_dense=0.01, min_opacity=0.005,
+                max_screen_size=0.0, seed=0, abs_thr=0.0):
+        """Returns (status, new params ptr, new count, [added, removed])."""
+        p = ctypes.c_void_p(params_ptr)
+        c = ctypes.c_int(int(count))
+        ch = (ctypes.c_int * 2)()
+        st = lib().gsn_density_control(self.handle, ctypes.byref(p), ctypes.byref(c), float(extent), float(grad_thr),
+                                       float(percent_dense), float(min_opacity), float(max_screen_size),
+                                       ctypes.c_ulonglong(seed), ch, float(abs_thr))
+        return st, (p.value or 0), c.value, [ch[0], ch[1]]
+
+    def buffers(self):
+        a, b, c = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+        _check(lib().gsn_density_buffers(self.handle, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)), "buffers")
+        return a.value, b.value, c.value
+
+    def set_max_gaussians(self, n):
+        _check(lib().gsn_density_set_max_gaussians(self.handle, int(n)), "set_max_gaussians")
+
+    def internals(self):
+        ps = [ctypes.c_void_p() for _ in range(4)]
+        _check(lib().gsn_density_internals(self.handle, *[ctypes.byref(p) for p in ps]), "internals")
+        return [p.value for p in ps]

@@ -38,6 +38,12 @@ int gsn_memcpy(void* dst, const void* src, size_t bytes);
  * be pinned for the copy to overlap. */
 int gsn_memcpy_async(void* dst, const void* src, size_t bytes, void* stream);
 
+/* Raw device allocation (cudaMalloc / cudaFree). Parameter blocks handed to
+ * gsn_density_control change owner (the controller keeps the caller's old block
+ * and frees it itself), so they must come from this allocator or cudaMalloc. */
+int gsn_device_alloc(size_t bytes, void** out);
+int gsn_device_free(void* ptr);
+
 /* Blocks until all work on `stream` is done. */
 int gsn_stream_synchronize(void* stream);
 
@@ -192,6 +198,53 @@ int gsn_solver_map_gradients(gsn_solver* s, const gsn_camera* camera, gsn_render
 
 /* Adam state (device, 58 x count each) and the step counter. */
 int gsn_solver_moments(gsn_solver* s, float** first, float** second, uint64_t* iteration);
+
+
+/* ------------------------------------------------------------------ density
+ * Replaces gs_native::DensityController (reference
+ * src/core/density/density_controller.h:9-83).
+ */
+typedef struct gsn_density gsn_density;
+
+int gsn_density_create(gsn_density** out);
+int gsn_density_destroy(gsn_density* d);
+int gsn_density_set_stream(gsn_density* d, void* stream);
+
+/* Initialize (density_controller.cu:410-438). */
+int gsn_density_initialize(gsn_density* d, int count, int capacity);
+
+/* AccumulateStatistics(statistics, absolute_statistics, count)
+ * (density_controller.cu:613-631): device float[2 * count] + float[count]. */
+int gsn_density_accumulate(gsn_density* d, const float* statistics, const float* absolute_statistics, int count);
+
+/* AccumulateStatistics(gradients, radii, ids, observations)
+ * (density_controller.cu:440-459): per-observation 2D gradients. */
+int gsn_density_accumulate_observations(gsn_density* d, const float* gradients, const float* radii, const int* ids,
+                                        int observations);
+
+/* ResetOpacity (density_controller.cu:633-647). */
+int gsn_density_reset_opacity(gsn_density* d, float* params, int stride, float max_opacity);
+
+/* ControlDensity (density_controller.cu:461-611). On success *params / *count
+ * receive the new parameter block (owned by the caller from now on) and the
+ * caller's previous block becomes the controller's spare (ownership ping-pong);
+ * all pruned: *params = NULL, *count = 0. changes (optional host int[2]) =
+ * {added, removed}. */
+int gsn_density_control(gsn_density* d, float** params, int* count, float scene_extent, float gradient_threshold,
+                        float percent_dense, float min_opacity, float max_screen_size, unsigned long long seed,
+                        int* changes, float absolute_gradient_threshold);
+
+/* GetHistoryParentIds / GetGaussianCount (control block) / GetParentIds (device). */
+int gsn_density_buffers(gsn_density* d, const int** history_parent_ids, const int** control, const int** parent_ids);
+
+/* Cap on the Gaussian count (0 = unlimited, the reference behaviour): additions
+ * beyond the cap are dropped in id order. */
+int gsn_density_set_max_gaussians(gsn_density* d, int max_gaussians);
+
+/* The normal samples of the last ControlDensity (device float[6 * sampled]) and
+ * the accumulated statistics (device float[capacity] x2, uint[capacity]). */
+int gsn_density_internals(gsn_density* d, const float** samples, float** gradient_sums, float** absolute_sums,
+                          unsigned int** observation_counts);
 
 #ifdef __cplusplus
 }
