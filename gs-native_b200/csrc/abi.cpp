@@ -6,9 +6,11 @@
 #include <new>
 
 #include "core/density/density_controller.h"
+#include "core/knn/knn.h"
 #include "core/render/renderer.h"
 #include "core/solver/solver.h"
 #include "kernels.h"
+#include "knn_kernels.h"
 #include "profile.h"
 
 struct gsn_renderer {
@@ -121,6 +123,21 @@ int gsn_sort_pairs_noalloc(uint32_t* keys, uint32_t* values, uint32_t* keys_alt,
                                                 AsStream(stream));
     *result_in_alt = alt ? 1 : 0;
     return status;
+}
+
+int gsn_knn3_workspace(int count, size_t* bytes) {
+    if (!bytes || count < 0) return GSN_ERR_INVALID_ARGUMENT;
+    *bytes = gsn::knn_layout(count).total;
+    return GSN_OK;
+}
+
+int gsn_knn3(const float* points, int count, float* mean_dist2, int* neighbors, void* workspace, void* stream) {
+    if (count < 0 || (count > 0 && (!points || !mean_dist2 || !workspace))) return GSN_ERR_INVALID_ARGUMENT;
+    return gsn::launch_knn3(points, count, mean_dist2, neighbors, workspace, AsStream(stream));
+}
+
+int gsn_knn3_host(const float* points, int count, float* mean_dist2, int* neighbors) {
+    return gs_native::ComputeMeanDist2(points, count, mean_dist2, neighbors) ? GSN_OK : GSN_ERR_INVALID_ARGUMENT;
 }
 
 int gsn_renderer_create(gsn_renderer** out) {

@@ -374,3 +374,19 @@ class Density:
         ps = [ctypes.c_void_p() for _ in range(4)]
         _check(lib().gsn_density_internals(self.handle, *[ctypes.byref(p) for p in ps]), "internals")
         return [p.value for p in ps]
+
+
+def knn3_host(points, neighbors=False):
+    """points: (n, 3) float32 host array -> (mean_dist2[n], neighbors[n, 3] or None)."""
+    import numpy as np
+    L = lib()
+    fn = L.gsn_knn3_host
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    fn.restype = ctypes.c_int
+    pts = np.ascontiguousarray(points, dtype=np.float32)
+    n = pts.shape[0]
+    d = np.zeros(n, dtype=np.float32)
+    nb = np.zeros((n, 3), dtype=np.int32) if neighbors else None
+    _check(fn(ctypes.c_void_p(pts.ctypes.data), n, ctypes.c_void_p(d.ctypes.data),
+              ctypes.c_void_p(nb.ctypes.data) if nb is not None else None), "gsn_knn3_host")
+    return d, nb

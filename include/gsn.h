@@ -100,6 +100,19 @@ int gsn_sort_pairs(uint32_t* keys, uint32_t* values, uint32_t* keys_alt, uint32_
 int gsn_sort_pairs_noalloc(uint32_t* keys, uint32_t* values, uint32_t* keys_alt, uint32_t* values_alt, int count,
                            int begin_bit, int end_bit, int* result_in_alt, void* stream);
 
+/* ------------------------------------------------------------------ 3-NN
+ * LBVH 3-nearest-neighbour search (replaces ComputeMeanDist2Cuda, reference
+ * src/core/knn/knn.h:9 and knn.cu:180-255). points: device float[3 * count]
+ * (xyz); mean_dist2: device float[count], the mean of the up to three smallest
+ * squared distances (0 when count < 2); neighbors: optional device
+ * int[3 * count] with the neighbour indices (ties to the smaller index, -1 when
+ * missing); workspace: device memory of gsn_knn3_workspace bytes. */
+int gsn_knn3_workspace(int count, size_t* bytes);
+int gsn_knn3(const float* points, int count, float* mean_dist2, int* neighbors, void* workspace, void* stream);
+
+/* Host-to-host convenience form of the same search (allocates internally). */
+int gsn_knn3_host(const float* points, int count, float* mean_dist2, int* neighbors);
+
 /* ------------------------------------------------------------------ renderer
  * Replaces gs_native::Renderer (reference src/core/render/renderer.h:10-89).
  */
