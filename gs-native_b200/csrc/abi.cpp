@@ -4,8 +4,12 @@
 #include <cuda_runtime.h>
 
 #include <new>
+#include <string>
+#include <vector>
 
 #include "core/density/density_controller.h"
+#include "core/gaussian_splatting.h"
+#include "io/ply.h"
 #include "core/knn/knn.h"
 #include "core/render/renderer.h"
 #include "core/solver/solver.h"
@@ -23,6 +27,10 @@ struct gsn_solver {
 
 struct gsn_density {
     gs_native::DensityController impl;
+};
+
+struct gsn_trainer {
+    gs_native::GaussianSplatting impl;
 };
 
 namespace {
@@ -382,6 +390,172 @@ int gsn_density_internals(gsn_density* d, const float** samples, float** gradien
     *gradient_sums = d->impl.GetGradientSums();
     *absolute_sums = d->impl.GetAbsoluteGradientSums();
     *observation_counts = d->impl.GetObservationCounts();
+    return GSN_OK;
+}
+
+int gsn_training_options_default(gsn_training_options* out) {
+    if (!out) return GSN_ERR_INVALID_ARGUMENT;
+    gs_native::TrainingOptions o;
+    out->sh_degree_interval = o.sh_degree_interval;
+    out->max_sh_degree = o.max_sh_degree;
+    out->position_lr_init = o.position_lr_init;
+    out->position_lr_final = o.position_lr_final;
+    out->position_lr_steps = o.position_lr_steps;
+    out->lr_scale = o.lr.scale;
+    out->lr_rotation = o.lr.rotation;
+    out->lr_opacity = o.lr.opacity;
+    out->lr_sh_dc = o.lr.sh_dc;
+    out->lr_sh_rest = o.lr.sh_rest;
+    out->densify_from = o.densify_from;
+    out->densify_until = o.densify_until;
+    out->densify_interval = o.densify_interval;
+    out->gradient_threshold = o.gradient_threshold;
+    out->absolute_gradient_threshold = o.absolute_gradient_threshold;
+    out->percent_dense = o.percent_dense;
+    out->min_opacity = o.min_opacity;
+    out->prune_large_after = o.prune_large_after;
+    out->opacity_cap_interval = o.opacity_cap_interval;
+    out->opacity_cap = o.opacity_cap;
+    out->opacity_reset_interval = o.opacity_reset_interval;
+    out->opacity_reset = o.opacity_reset;
+    for (int c = 0; c < 3; ++c) out->background[c] = o.background[c];
+    out->max_gaussians = o.max_gaussians;
+    out->density_seed = o.density_seed;
+    out->initial_opacity = o.initial_opacity;
+    return GSN_OK;
+}
+
+namespace {
+gs_native::TrainingOptions ToOptions(const gsn_training_options& in) {
+    gs_native::TrainingOptions o;
+    o.sh_degree_interval = in.sh_degree_interval;
+    o.max_sh_degree = in.max_sh_degree;
+    o.position_lr_init = in.position_lr_init;
+    o.position_lr_final = in.position_lr_final;
+    o.position_lr_steps = in.position_lr_steps;
+    o.lr.scale = in.lr_scale;
+    o.lr.rotation = in.lr_rotation;
+    o.lr.opacity = in.lr_opacity;
+    o.lr.sh_dc = in.lr_sh_dc;
+    o.lr.sh_rest = in.lr_sh_rest;
+    o.densify_from = in.densify_from;
+    o.densify_until = in.densify_until;
+    o.densify_interval = in.densify_interval;
+    o.gradient_threshold = in.gradient_threshold;
+    o.absolute_gradient_threshold = in.absolute_gradient_threshold;
+    o.percent_dense = in.percent_dense;
+    o.min_opacity = in.min_opacity;
+    o.prune_large_after = in.prune_large_after;
+    o.opacity_cap_interval = in.opacity_cap_interval;
+    o.opacity_cap = in.opacity_cap;
+    o.opacity_reset_interval = in.opacity_reset_interval;
+    o.opacity_reset = in.opacity_reset;
+    for (int c = 0; c < 3; ++c) o.background[c] = in.background[c];
+    o.max_gaussians = in.max_gaussians;
+    o.density_seed = in.density_seed;
+    o.initial_opacity = in.initial_opacity;
+    return o;
+}
+}  // namespace
+
+int gsn_trainer_create(gsn_trainer** out) {
+    if (!out) return GSN_ERR_INVALID_ARGUMENT;
+    *out = new (std::nothrow) gsn_trainer();
+    return *out ? GSN_OK : GSN_ERR_OUT_OF_MEMORY;
+}
+
+int gsn_trainer_destroy(gsn_trainer* t) {
+    delete t;
+    return GSN_OK;
+}
+
+int gsn_trainer_set_stream(gsn_trainer* t, void* stream) {
+    if (!t) return GSN_ERR_INVALID_ARGUMENT;
+    t->impl.SetStream(AsStream(stream));
+    return GSN_OK;
+}
+
+int gsn_trainer_initialize(gsn_trainer* t, const gsn_camera* cameras, const uint8_t* const* images,
+                           int camera_count, const float* points, const float* colors, int point_count,
+                           const gsn_training_options* options) {
+    if (!t || !cameras || !images || camera_count <= 0 || !points || !colors || point_count <= 0)
+        return GSN_ERR_INVALID_ARGUMENT;
+    gs_native::TrainingScene scene;
+    for (int k = 0; k < camera_count; ++k) {
+        scene.train_cameras.push_back(AsCamera(cameras + k));
+        scene.train_images.push_back(images[k]);
+    }
+    scene.point_positions = points;
+    scene.point_colors = colors;
+    scene.point_count = point_count;
+    gs_native::TrainingOptions o;
+    if (options) o = ToOptions(*options);
+    return t->impl.Initialize(scene, o) ? GSN_OK : GSN_ERR_INVALID_ARGUMENT;
+}
+
+int gsn_trainer_train(gsn_trainer* t, int iterations) {
+    if (!t) return GSN_ERR_INVALID_ARGUMENT;
+    return t->impl.Train(iterations) ? GSN_OK : GSN_ERR_INVALID_ARGUMENT;
+}
+
+int gsn_trainer_render(gsn_trainer* t, const gsn_camera* camera, float* image) {
+    if (!t || !camera) return GSN_ERR_INVALID_ARGUMENT;
+    return t->impl.Render(AsCamera(camera), image) ? GSN_OK : GSN_ERR_INVALID_ARGUMENT;
+}
+
+int gsn_trainer_evaluate(gsn_trainer* t, const gsn_camera* cameras, const uint8_t* const* images, int count,
+                         double* psnr, double* loss) {
+    if (!t || !cameras || !images || count <= 0 || !psnr) return GSN_ERR_INVALID_ARGUMENT;
+    std::vector<gs_native::CameraParams> cams;
+    std::vector<const uint8_t*> imgs;
+    for (int k = 0; k < count; ++k) {
+        cams.push_back(AsCamera(cameras + k));
+        imgs.push_back(images[k]);
+    }
+    return t->impl.Evaluate(cams, imgs, psnr, loss) ? GSN_OK : GSN_ERR_INVALID_ARGUMENT;
+}
+
+int gsn_trainer_save(gsn_trainer* t, const char* path) {
+    if (!t || !path) return GSN_ERR_INVALID_ARGUMENT;
+    return t->impl.Save(path) ? GSN_OK : GSN_ERR_IO;
+}
+
+int gsn_trainer_load(gsn_trainer* t, const char* path) {
+    if (!t || !path) return GSN_ERR_INVALID_ARGUMENT;
+    return t->impl.Load(path) ? GSN_OK : GSN_ERR_IO;
+}
+
+int gsn_trainer_state(gsn_trainer* t, float** params, int* count, int* completed, int* sh_degree,
+                      float* scene_extent) {
+    if (!t) return GSN_ERR_INVALID_ARGUMENT;
+    if (params) *params = t->impl.GetGaussians().gaussians_;
+    if (count) *count = t->impl.GetGaussians().gaussian_count_;
+    if (completed) *completed = t->impl.GetCompleted();
+    if (sh_degree) *sh_degree = t->impl.GetShDegree();
+    if (scene_extent) *scene_extent = t->impl.GetSceneExtent();
+    return GSN_OK;
+}
+
+int gsn_ply_write(const char* path, const float* params, int count) {
+    if (!path || count < 0 || (count > 0 && !params)) return GSN_ERR_INVALID_ARGUMENT;
+    return gs_native::WriteGaussiansPly(path, gs_native::UnpackGaussians(params, count)) ? GSN_OK : GSN_ERR_IO;
+}
+
+int gsn_ply_read_count(const char* path, int* count) {
+    if (!path || !count) return GSN_ERR_INVALID_ARGUMENT;
+    std::vector<gs_native::Gaussian> g;
+    if (!gs_native::ReadGaussiansPly(path, g)) return GSN_ERR_IO;
+    *count = static_cast<int>(g.size());
+    return GSN_OK;
+}
+
+int gsn_ply_read(const char* path, float* params, int count) {
+    if (!path || !params || count <= 0) return GSN_ERR_INVALID_ARGUMENT;
+    std::vector<gs_native::Gaussian> g;
+    if (!gs_native::ReadGaussiansPly(path, g)) return GSN_ERR_IO;
+    if (static_cast<int>(g.size()) != count) return GSN_ERR_INVALID_ARGUMENT;
+    std::vector<float> p = gs_native::PackGaussians(g);
+    std::copy(p.begin(), p.end(), params);
     return GSN_OK;
 }
 

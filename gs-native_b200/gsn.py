@@ -390,3 +390,142 @@ def knn3_host(points, neighbors=False):
     _check(fn(ctypes.c_void_p(pts.ctypes.data), n, ctypes.c_void_p(d.ctypes.data),
               ctypes.c_void_p(nb.ctypes.data) if nb is not None else None), "gsn_knn3_host")
     return d, nb
+
+
+class TrainingOptions(ctypes.Structure):
+    """gsn_training_options (include/gsn.h)."""
+
+    _fields_ = [
+        ("sh_degree_interval", ctypes.c_int), ("max_sh_degree", ctypes.c_int),
+        ("position_lr_init", ctypes.c_float), ("position_lr_final", ctypes.c_float),
+        ("position_lr_steps", ctypes.c_int),
+        ("lr_scale", ctypes.c_float), ("lr_rotation", ctypes.c_float), ("lr_opacity", ctypes.c_float),
+        ("lr_sh_dc", ctypes.c_float), ("lr_sh_rest", ctypes.c_float),
+        ("densify_from", ctypes.c_int), ("densify_until", ctypes.c_int), ("densify_interval", ctypes.c_int),
+        ("gradient_threshold", ctypes.c_float), ("absolute_gradient_threshold", ctypes.c_float),
+        ("percent_dense", ctypes.c_float), ("min_opacity", ctypes.c_float), ("prune_large_after", ctypes.c_int),
+        ("opacity_cap_interval", ctypes.c_int), ("opacity_cap", ctypes.c_float),
+        ("opacity_reset_interval", ctypes.c_int), ("opacity_reset", ctypes.c_float),
+        ("background", ctypes.c_float * 3), ("max_gaussians", ctypes.c_int),
+        ("density_seed", ctypes.c_ulonglong), ("initial_opacity", ctypes.c_float),
+    ]
+
+    @classmethod
+    def defaults(cls, **overrides):
+        o = cls()
+        fn = lib().gsn_training_options_default
+        fn.argtypes = [ctypes.POINTER(cls)]
+        fn.restype = ctypes.c_int
+        _check(fn(ctypes.byref(o)), "gsn_training_options_default")
+        for k, v in overrides.items():
+            if k == "background":
+                for c in range(3):
+                    o.background[c] = float(v[c])
+            else:
+                setattr(o, k, v)
+        return o
+
+
+class Trainer:
+    """Handle over gs_native::GaussianSplatting (reference gaussian_splatting.h:14-53)."""
+
+    def __init__(self):
+        L = lib()
+        vp, i32, P = ctypes.c_void_p, ctypes.c_int, ctypes.POINTER
+        sigs = {
+            "gsn_trainer_create": [P(vp)], "gsn_trainer_destroy": [vp], "gsn_trainer_set_stream": [vp, vp],
+            "gsn_trainer_initialize": [vp, P(Camera), P(vp), i32, vp, vp, i32, P(TrainingOptions)],
+            "gsn_trainer_train": [vp, i32], "gsn_trainer_render": [vp, P(Camera), vp],
+            "gsn_trainer_evaluate": [vp, P(Camera), P(vp), i32, P(ctypes.c_double), P(ctypes.c_double)],
+            "gsn_trainer_save": [vp, ctypes.c_char_p], "gsn_trainer_load": [vp, ctypes.c_char_p],
+            "gsn_trainer_state": [vp, P(vp), P(i32), P(i32), P(i32), P(ctypes.c_float)],
+        }
+        for name, args in sigs.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = i32
+        h = ctypes.c_void_p()
+        _check(L.gsn_trainer_create(ctypes.byref(h)), "gsn_trainer_create")
+        self.handle = h
+
+    def close(self):
+        if self.handle:
+            lib().gsn_trainer_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream):
+        _check(lib().gsn_trainer_set_stream(self.handle, ctypes.c_void_p(stream)), "set_stream")
+
+    @staticmethod
+    def _views(cameras, images):
+        import numpy as np
+        cams = (Camera * len(cameras))(*cameras)
+        keep = [np.ascontiguousarray(im, dtype=np.uint8) for im in images]
+        ptrs = (ctypes.c_void_p * len(keep))(*[im.ctypes.data for im in keep])
+        return cams, ptrs, keep
+
+    def initialize(self, cameras, images, points, colors, options=None):
+        import numpy as np
+        cams, ptrs, keep = self._views(cameras, images)
+        pts = np.ascontiguousarray(points, dtype=np.float32)
+        col = np.ascontiguousarray(colors, dtype=np.float32)
+        opt = ctypes.byref(options) if options is not None else None
+        return lib().gsn_trainer_initialize(self.handle, cams, ptrs, len(cameras), ctypes.c_void_p(pts.ctypes.data),
+                                            ctypes.c_void_p(col.ctypes.data), pts.shape[0], opt)
+
+    def train(self, iterations):
+        return lib().gsn_trainer_train(self.handle, int(iterations))
+
+    def render(self, camera, image_ptr):
+        return lib().gsn_trainer_render(self.handle, ctypes.byref(camera), ctypes.c_void_p(image_ptr))
+
+    def evaluate(self, cameras, images):
+        cams, ptrs, keep = self._views(cameras, images)
+        psnr, loss = ctypes.c_double(), ctypes.c_double()
+        _check(lib().gsn_trainer_evaluate(self.handle, cams, ptrs, len(cameras), ctypes.byref(psnr),
+                                          ctypes.byref(loss)), "evaluate")
+        return psnr.value, loss.value
+
+    def save(self, path):
+        return lib().gsn_trainer_save(self.handle, str(path).encode())
+
+    def load(self, path):
+        return lib().gsn_trainer_load(self.handle, str(path).encode())
+
+    def state(self):
+        p, n, c, s, e = ctypes.c_void_p(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_float()
+        _check(lib().gsn_trainer_state(self.handle, ctypes.byref(p), ctypes.byref(n), ctypes.byref(c),
+                                       ctypes.byref(s), ctypes.byref(e)), "state")
+        return dict(params=p.value or 0, count=n.value, completed=c.value, sh_degree=s.value, extent=e.value)
+
+
+def ply_write(path, params):
+    import numpy as np
+    L = lib()
+    L.gsn_ply_write.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_int]
+    L.gsn_ply_write.restype = ctypes.c_int
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    return L.gsn_ply_write(str(path).encode(), ctypes.c_void_p(p.ctypes.data), p.shape[1])
+
+
+def ply_read(path):
+    """Returns (status, (58, n) float32 array or None)."""
+    import numpy as np
+    L = lib()
+    L.gsn_ply_read_count.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)]
+    L.gsn_ply_read_count.restype = ctypes.c_int
+    L.gsn_ply_read.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_int]
+    L.gsn_ply_read.restype = ctypes.c_int
+    n = ctypes.c_int()
+    st = L.gsn_ply_read_count(str(path).encode(), ctypes.byref(n))
+    if st != 0:
+        return st, None
+    out = np.zeros((58, n.value), dtype=np.float32)
+    st = L.gsn_ply_read(str(path).encode(), ctypes.c_void_p(out.ctypes.data), n.value)
+    return st, out

@@ -1,0 +1,232 @@
+// gs_native::GaussianSplatting trainer (reference behaviour:
+// src/core/gaussian_splatting.cpp:23-342).
+#include "core/gaussian_splatting.h"
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <limits>
+#include <numeric>
+#include <random>
+
+#include "core/knn/knn.h"
+#include "io/ply.h"
+
+namespace gs_native {
+
+GaussianSplatting::~GaussianSplatting() { cudaFree(gaussians_.gaussians_); }
+
+void GaussianSplatting::SetStream(cudaStream_t stream) {
+    stream_ = stream;
+    renderer_.SetStream(stream);
+    solver_.SetStream(stream);
+    density_.SetStream(stream);
+}
+
+bool GaussianSplatting::Initialize(const TrainingScene& scene, const TrainingOptions& options) {
+    if (gaussians_.gaussians_ || scene.train_cameras.empty() || scene.train_cameras.size() != scene.train_images.size() ||
+        scene.point_count <= 0 || !scene.point_positions || !scene.point_colors)
+        return false;
+    size_t pixels = 0;
+    for (size_t i = 0; i < scene.train_cameras.size(); ++i) {
+        const CameraParams& c = scene.train_cameras[i];
+        if (!scene.train_images[i] || c.width_ <= 0 || c.height_ <= 0 || c.tile_count_x_ != (c.width_ + 15) / 16 ||
+            c.tile_count_y_ != (c.height_ + 15) / 16)
+            return false;
+        pixels = std::max(pixels, static_cast<size_t>(c.width_) * c.height_);
+    }
+    options_ = options;
+    cameras_ = scene.train_cameras;
+    // scene extent: 1.1 x the largest camera-centre distance from the mean centre
+    // (gaussian_splatting.cpp:46-71)
+    double mean[3] = {0, 0, 0};
+    std::vector<std::array<double, 3>> centers(cameras_.size());
+    for (size_t k = 0; k < cameras_.size(); ++k) {
+        for (int a = 0; a < 3; ++a) {
+            double c = 0;
+            for (int r = 0; r < 3; ++r) c -= double(cameras_[k].R_c_w_[r * 3 + a]) * cameras_[k].t_c_w_[r];
+            centers[k][a] = c;
+            mean[a] += c / cameras_.size();
+        }
+    }
+    double extent = 0;
+    for (const auto& c : centers)
+        extent = std::max(extent, std::sqrt((c[0] - mean[0]) * (c[0] - mean[0]) + (c[1] - mean[1]) * (c[1] - mean[1]) +
+                                            (c[2] - mean[2]) * (c[2] - mean[2])));
+    scene_extent_ = static_cast<float>(extent) * 1.1f;
+    if (scene_extent_ == 0.0f) {
+        for (int i = 0; i < scene.point_count; ++i) {
+            const float* p = scene.point_positions + 3 * i;
+            double d = std::sqrt((p[0] - mean[0]) * (p[0] - mean[0]) + (p[1] - mean[1]) * (p[1] - mean[1]) +
+                                 (p[2] - mean[2]) * (p[2] - mean[2]));
+            scene_extent_ = std::max(scene_extent_, static_cast<float>(d));
+        }
+        scene_extent_ = std::max(scene_extent_, 1e-6f);
+    }
+    // resident training targets
+    target_stride_ = pixels * 3;
+    if (!targets_.Reserve(target_stride_ * cameras_.size()) || !image_.Reserve(pixels * 3)) return false;
+    image_capacity_ = pixels * 3;
+    for (size_t k = 0; k < cameras_.size(); ++k) {
+        const size_t bytes = static_cast<size_t>(cameras_[k].width_) * cameras_[k].height_ * 3;
+        if (cudaMemcpyAsync(targets_.get() + k * target_stride_, scene.train_images[k], bytes, cudaMemcpyHostToDevice,
+                            stream_) != cudaSuccess)
+            return false;
+    }
+    camera_order_.resize(cameras_.size());
+    std::iota(camera_order_.begin(), camera_order_.end(), 0);
+    camera_cursor_ = static_cast<int>(camera_order_.size());
+    completed_ = 0;
+    sh_degree_ = 0;
+    solver_.SetLearningRates(options_.lr);
+    density_.SetMaxGaussians(options_.max_gaussians);
+    if (!InitializeGaussians(scene.point_positions, scene.point_colors, scene.point_count)) return false;
+    return cudaStreamSynchronize(stream_) == cudaSuccess;
+}
+
+bool GaussianSplatting::InitializeGaussians(const float* positions, const float* colors, int count) {
+    std::vector<float> dist(static_cast<size_t>(count), 0.0f);
+    if (count >= 2 && !ComputeMeanDist2(positions, count, dist.data(), nullptr, stream_)) return false;
+    const size_t N = static_cast<size_t>(count);
+    std::vector<float> p(N * kMaxParamCount, 0.0f);
+    const float logit = std::log(options_.initial_opacity / (1.0f - options_.initial_opacity));
+    for (size_t i = 0; i < N; ++i) {
+        const float scale = 0.5f * std::log(std::max(dist[i], 1e-7f));
+        for (int a = 0; a < 3; ++a) {
+            p[a * N + i] = positions[3 * i + a];
+            p[(kLogScaleIndex + a) * N + i] = scale;
+            p[(kShIndex + a * 16) * N + i] = (colors[3 * i + a] - 0.5f) / 0.28209479177387814f;
+        }
+        p[kOpacityIndex * N + i] = logit;
+    }
+    void* block = nullptr;
+    if (DeviceAlloc(&block, p.size() * sizeof(float)) != cudaSuccess) return false;
+    if (cudaMemcpy(block, p.data(), p.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess ||
+        !density_.Initialize(count, count) || !solver_.RemapGaussians(nullptr, count)) {
+        cudaFree(block);
+        return false;
+    }
+    cudaFree(gaussians_.gaussians_);
+    gaussians_.gaussians_ = static_cast<float*>(block);
+    gaussians_.gaussian_count_ = count;
+    return true;
+}
+
+bool GaussianSplatting::Train(int iterations) {
+    if (iterations < 0 || !gaussians_.gaussians_ || cameras_.empty()) return false;
+    std::mt19937 generator(0);
+    for (int it = 0; it < iterations; ++it) {
+        if (gaussians_.gaussian_count_ == 0) return false;
+        if (camera_cursor_ >= static_cast<int>(camera_order_.size())) {
+            std::shuffle(camera_order_.begin(), camera_order_.end(), generator);
+            camera_cursor_ = 0;
+        }
+        if (!Step()) return false;
+    }
+    return cudaStreamSynchronize(stream_) == cudaSuccess;
+}
+
+bool GaussianSplatting::Step() {
+    const int index = camera_order_[camera_cursor_];
+    const CameraParams& camera = cameras_[index];
+    const int next = completed_ + 1;
+    sh_degree_ = std::min(options_.max_sh_degree, next / options_.sh_degree_interval);
+    const float fraction = std::min(1.0f, static_cast<float>(next) / static_cast<float>(options_.position_lr_steps));
+    const float lr = scene_extent_ * std::exp(std::log(options_.position_lr_init) * (1.0f - fraction) +
+                                              std::log(options_.position_lr_final) * fraction);
+    const uint8_t* target = targets_.get() + static_cast<size_t>(index) * target_stride_;
+    if (!renderer_.Render(gaussians_, camera, options_.background, image_.get(), sh_degree_)) return false;
+    const bool accumulate = next < options_.densify_until;
+    if (accumulate)
+        solver_.SetDensityAccumulators(density_.GetGradientSums(), density_.GetAbsoluteGradientSums(),
+                                       density_.GetObservationCounts());
+    else
+        solver_.SetDensityAccumulators(nullptr, nullptr, nullptr);
+    if (!solver_.Iterate(camera, renderer_, image_.get(), target, gaussians_, lr, sh_degree_)) return false;
+    completed_ = next;
+    ++camera_cursor_;
+    if (completed_ < options_.densify_until) {
+        if (completed_ > options_.densify_from && completed_ % options_.densify_interval == 0 && !ControlDensity())
+            return false;
+        if (completed_ % options_.opacity_cap_interval == 0) {
+            const float cap =
+                completed_ % options_.opacity_reset_interval == 0 ? options_.opacity_reset : options_.opacity_cap;
+            if (!density_.ResetOpacity(gaussians_.gaussians_, gaussians_.gaussian_count_, cap) ||
+                !solver_.ResetOpacityHistory())
+                return false;
+        }
+    }
+    return true;
+}
+
+bool GaussianSplatting::ControlDensity() {
+    int changes[2] = {};
+    if (!density_.ControlDensity(gaussians_, scene_extent_, options_.gradient_threshold, options_.percent_dense,
+                                 options_.min_opacity, completed_ > options_.prune_large_after ? 20.0f : 0.0f,
+                                 options_.density_seed, changes, options_.absolute_gradient_threshold))
+        return false;
+    return solver_.RemapGaussians(density_.GetHistoryParentIds(), gaussians_.gaussian_count_);
+}
+
+bool GaussianSplatting::Render(const CameraParams& camera, float* device_image) {
+    if (!gaussians_.gaussians_ || !device_image) return false;
+    return renderer_.Render(gaussians_, camera, options_.background, device_image, sh_degree_);
+}
+
+bool GaussianSplatting::Evaluate(const std::vector<CameraParams>& cameras, const std::vector<const uint8_t*>& images,
+                                 double* psnr, double* loss) {
+    if (!psnr || cameras.size() != images.size() || cameras.empty() || !gaussians_.gaussians_) return false;
+    double sum_psnr = 0.0, sum_loss = 0.0;
+    DeviceArray<uint8_t> target;
+    DeviceArray<float> image;
+    Solver metric;
+    metric.SetStream(stream_);
+    metric.SetComputeLoss(true);
+    for (size_t k = 0; k < cameras.size(); ++k) {
+        const CameraParams& c = cameras[k];
+        const size_t px = static_cast<size_t>(c.width_) * c.height_;
+        if (!images[k] || !target.Reserve(px * 3) || !image.Reserve(px * 3)) return false;
+        if (cudaMemcpyAsync(target.get(), images[k], px * 3, cudaMemcpyHostToDevice, stream_) != cudaSuccess)
+            return false;
+        if (!Render(c, image.get()) || !metric.ComputeImageGradients(c, image.get(), target.get())) return false;
+        double out[4];
+        if (cudaMemcpyAsync(out, metric.GetLossDevice(), sizeof(out), cudaMemcpyDeviceToHost, stream_) !=
+                cudaSuccess ||
+            cudaStreamSynchronize(stream_) != cudaSuccess)
+            return false;
+        sum_loss += out[0];
+        sum_psnr += out[3];
+    }
+    *psnr = sum_psnr / cameras.size();
+    if (loss) *loss = sum_loss / cameras.size();
+    return true;
+}
+
+bool GaussianSplatting::Save(const std::string& path) {
+    const int count = gaussians_.gaussian_count_;
+    if (count <= 0 || !gaussians_.gaussians_) return false;
+    std::vector<float> p(static_cast<size_t>(count) * kMaxParamCount);
+    if (cudaMemcpy(p.data(), gaussians_.gaussians_, p.size() * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return false;
+    return WriteGaussiansPly(path, UnpackGaussians(p.data(), count));
+}
+
+bool GaussianSplatting::Load(const std::string& path) {
+    std::vector<Gaussian> g;
+    if (!ReadGaussiansPly(path, g)) return false;
+    std::vector<float> p = PackGaussians(g);
+    const int count = static_cast<int>(g.size());
+    void* block = nullptr;
+    if (DeviceAlloc(&block, p.size() * sizeof(float)) != cudaSuccess) return false;
+    if (cudaMemcpy(block, p.data(), p.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess ||
+        !density_.Initialize(count, count) || !solver_.RemapGaussians(nullptr, count)) {
+        cudaFree(block);
+        return false;
+    }
+    cudaFree(gaussians_.gaussians_);
+    gaussians_.gaussians_ = static_cast<float*>(block);
+    gaussians_.gaussian_count_ = count;
+    return true;
+}
+
+}  // namespace gs_native

@@ -1,0 +1,118 @@
+// Drop-in trainer gs_native::GaussianSplatting (reference:
+// src/core/gaussian_splatting.h:14-53, gaussian_splatting.cpp:23-342), without
+// OpenCV: the scene is given as camera parameters, host u8 HWC images and a
+// host point cloud instead of cv::Mat / Camera objects.
+//
+// Same schedule as the reference (all values configurable through
+// TrainingOptions, defaults equal to the reference's constants): one training
+// camera per iteration in a std::mt19937(0) shuffled order that is re-drawn when
+// exhausted (the generator is re-created at every Train call, as in the
+// reference); SH degree min(3, it / 1000); position learning rate
+// extent * exp(lerp(log 1.6e-4, log 1.6e-6, it / 30000)); statistics accumulated
+// while it < 15000; density control every 100 iterations after 500 with
+// prune-large after 3000; opacity capped at 0.8 every 500 and 0.01 every 3000
+// iterations. Training images stay resident in device memory; the reference
+// uploads one per iteration from pageable host memory.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "core/density/density_controller.h"
+#include "core/render/renderer.h"
+#include "core/solver/solver.h"
+#include "core/types/buffers.h"
+#include "util/device_array.h"
+
+namespace gs_native {
+
+struct TrainingScene {
+    std::vector<CameraParams> train_cameras;
+    std::vector<const uint8_t*> train_images;  // host HWC u8 (width * height * 3 bytes), not owned
+    const float* point_positions = nullptr;     // host xyz, point_count entries
+    const float* point_colors = nullptr;        // host rgb in [0, 1]
+    int point_count = 0;
+};
+
+struct TrainingOptions {
+    int sh_degree_interval = 1000;
+    int max_sh_degree = 3;
+    float position_lr_init = 0.00016f;
+    float position_lr_final = 0.0000016f;
+    int position_lr_steps = 30000;
+    LearningRates lr;  // non-position groups (solver.cu:666-681)
+    int densify_from = 500;       // density control when it > densify_from ...
+    int densify_until = 15000;    // ... and it < densify_until (statistics too)
+    int densify_interval = 100;
+    float gradient_threshold = 0.0002f;
+    float absolute_gradient_threshold = 0.0008f;
+    float percent_dense = 0.01f;
+    float min_opacity = 0.005f;
+    int prune_large_after = 3000;
+    int opacity_cap_interval = 500;
+    float opacity_cap = 0.8f;
+    int opacity_reset_interval = 3000;
+    float opacity_reset = 0.01f;
+    float background[3] = {0.0f, 0.0f, 0.0f};
+    int max_gaussians = 0;  // 0 = unlimited (reference behaviour)
+    unsigned long long density_seed = 0;
+    float initial_opacity = 0.1f;  // initial opacity logit log(o / (1 - o))
+};
+
+class GaussianSplatting {
+public:
+    GaussianSplatting() = default;
+    ~GaussianSplatting();
+
+    GaussianSplatting(const GaussianSplatting&) = delete;
+    GaussianSplatting& operator=(const GaussianSplatting&) = delete;
+
+    bool Initialize(const TrainingScene& scene, const TrainingOptions& options = TrainingOptions());
+    bool Train(int iterations);
+    // Renders into a device fp32 HWC image of camera.width_ * camera.height_ * 3.
+    bool Render(const CameraParams& camera, float* device_image);
+    bool Save(const std::string& path);
+    // Replaces the model by a PLY file (Adam history and statistics reset).
+    bool Load(const std::string& path);
+    // Mean PSNR (dB, FP64 reduction) of the current model over the given views
+    // (host u8 HWC images).
+    bool Evaluate(const std::vector<CameraParams>& cameras, const std::vector<const uint8_t*>& images, double* psnr,
+                  double* loss = nullptr);
+
+    void SetStream(cudaStream_t stream);
+    const GaussianBuffers& GetGaussians() const { return gaussians_; }
+    int GetCompleted() const { return completed_; }
+    int GetShDegree() const { return sh_degree_; }
+    float GetSceneExtent() const { return scene_extent_; }
+    Renderer& GetRenderer() { return renderer_; }
+    Solver& GetSolver() { return solver_; }
+    DensityController& GetDensity() { return density_; }
+    const TrainingOptions& GetOptions() const { return options_; }
+
+private:
+    bool InitializeGaussians(const float* positions, const float* colors, int count);
+    bool ControlDensity();
+    bool Step();
+
+    cudaStream_t stream_ = nullptr;
+    TrainingOptions options_;
+    std::vector<CameraParams> cameras_;
+    DeviceArray<uint8_t> targets_;
+    size_t target_stride_ = 0;  // bytes per resident training image
+    GaussianBuffers gaussians_;
+    Renderer renderer_;
+    Solver solver_;
+    DensityController density_;
+    DeviceArray<float> image_;
+    size_t image_capacity_ = 0;
+    std::vector<int> camera_order_;
+    int camera_cursor_ = 0;
+    int completed_ = 0;
+    int sh_degree_ = 0;
+    float scene_extent_ = 0.0f;
+};
+
+}  // namespace gs_native

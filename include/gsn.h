@@ -259,6 +259,71 @@ int gsn_density_set_max_gaussians(gsn_density* d, int max_gaussians);
 int gsn_density_internals(gsn_density* d, const float** samples, float** gradient_sums, float** absolute_sums,
                           unsigned int** observation_counts);
 
+
+/* ------------------------------------------------------------------ trainer
+ * Replaces gs_native::GaussianSplatting (reference
+ * src/core/gaussian_splatting.h:14-53), without OpenCV: the scene is camera
+ * parameters, host u8 HWC images and a host point cloud. Defaults of
+ * gsn_training_options_default equal the reference's hard-coded schedule
+ * (gaussian_splatting.cpp:130-198, 262-287; solver.cu:666-681).
+ */
+typedef struct gsn_training_options {
+    int sh_degree_interval;          /* 1000 */
+    int max_sh_degree;               /* 3 */
+    float position_lr_init;          /* 1.6e-4 (times the scene extent) */
+    float position_lr_final;         /* 1.6e-6 */
+    int position_lr_steps;           /* 30000 */
+    float lr_scale, lr_rotation, lr_opacity, lr_sh_dc, lr_sh_rest; /* 0.005 0.001 0.025 0.0025 0.0025/20 */
+    int densify_from;                /* 500 */
+    int densify_until;               /* 15000 */
+    int densify_interval;            /* 100 */
+    float gradient_threshold;        /* 2e-4 */
+    float absolute_gradient_threshold; /* 8e-4 */
+    float percent_dense;             /* 0.01 */
+    float min_opacity;               /* 0.005 */
+    int prune_large_after;           /* 3000 */
+    int opacity_cap_interval;        /* 500 */
+    float opacity_cap;               /* 0.8 */
+    int opacity_reset_interval;      /* 3000 */
+    float opacity_reset;             /* 0.01 */
+    float background[3];             /* 0 0 0 */
+    int max_gaussians;               /* 0 = unlimited */
+    unsigned long long density_seed; /* 0 */
+    float initial_opacity;           /* 0.1 */
+} gsn_training_options;
+
+int gsn_training_options_default(gsn_training_options* out);
+
+typedef struct gsn_trainer gsn_trainer;
+int gsn_trainer_create(gsn_trainer** out);
+int gsn_trainer_destroy(gsn_trainer* t);
+int gsn_trainer_set_stream(gsn_trainer* t, void* stream);
+/* Initialize (gaussian_splatting.cpp:23-128): images[k] is a host u8 HWC image
+ * of cameras[k]; points / colors are host float[3 * point_count]. */
+int gsn_trainer_initialize(gsn_trainer* t, const gsn_camera* cameras, const uint8_t* const* images,
+                           int camera_count, const float* points, const float* colors, int point_count,
+                           const gsn_training_options* options);
+/* Train (gaussian_splatting.cpp:130-198). */
+int gsn_trainer_train(gsn_trainer* t, int iterations);
+/* Render into a device fp32 HWC image (gaussian_splatting.cpp:200-232). */
+int gsn_trainer_render(gsn_trainer* t, const gsn_camera* camera, float* image);
+/* Mean PSNR / loss over views with host u8 HWC images (FP64 reductions). */
+int gsn_trainer_evaluate(gsn_trainer* t, const gsn_camera* cameras, const uint8_t* const* images, int count,
+                         double* psnr, double* loss);
+/* Save to / load from a Gaussian PLY (gaussian_splatting.cpp:234-260). */
+int gsn_trainer_save(gsn_trainer* t, const char* path);
+int gsn_trainer_load(gsn_trainer* t, const char* path);
+/* Current device parameter block and schedule state. */
+int gsn_trainer_state(gsn_trainer* t, float** params, int* count, int* completed, int* sh_degree,
+                      float* scene_extent);
+
+/* ------------------------------------------------------------------ PLY
+ * WriteGaussiansPly / ReadGaussiansPly (reference src/io/data_io.cpp:420-590)
+ * on a host 58 x count SoA block. */
+int gsn_ply_write(const char* path, const float* params, int count);
+int gsn_ply_read_count(const char* path, int* count);
+int gsn_ply_read(const char* path, float* params, int count);
+
 #ifdef __cplusplus
 }
 #endif
