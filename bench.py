@@ -39,6 +39,10 @@ UNIT = "iters/sec"
 SH_DEGREE = 3
 TARGET_GAUSSIANS = 1_500_000
 MODEL_GAUSSIANS = 1_200_000
+# DRAM bytes (read + write) of one gaussian_update launch on this workload, from
+# the ncu capture summarised in profiles/gaussian_update_plain_1.2M.md.
+NCU_TRAFFIC = {"gaussian_update": 900_431_104 + 801_656_576}
+NCU_TRAFFIC_SOURCE = "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/gaussian_update_plain_1.2M.md"
 
 
 def parse():
@@ -353,7 +357,9 @@ def run_gsn(args):
     top_hbm = max(hbm_stages, key=hbm_stages.get)
     achieved = alg[top_hbm] / (stages[top_hbm] / 1000.0) / 1e9
     roofline = {"bound": "hbm", "kernel": top_hbm, "achieved": round(achieved, 1), "peak": peak,
-                "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                "unit": "GB/s", "frac": round(achieved / peak, 4),
+                "traffic": NCU_TRAFFIC.get(top_hbm) if n == MODEL_GAUSSIANS else None,
+                "traffic_source": NCU_TRAFFIC_SOURCE if top_hbm in NCU_TRAFFIC else None,
                 "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured" else
                 "fallback 6650 GB/s",
                 "dominant_kernel": dominant,

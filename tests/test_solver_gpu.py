@@ -220,6 +220,46 @@ def test_iterate_matches_reference_solver():
     assert np.isfinite(mine).all()
 
 
+@pytest.mark.parametrize("n", [4099, 4096 + 66, 130, 61, 3])
+def test_adam_matches_fp32_adam_of_mapped_gradients_on_ragged_counts(n):
+    """Counts that are not multiples of the warp or CTA width (rows starting at
+    every 16-byte phase, partial last blocks): the fused update must equal FP32
+    Adam (solver.cu:651-689) applied to the kernel's own mapped gradients."""
+    t = torch()
+    _, cam = scenes.single_step_scene()
+    params = scenes.random_gaussians(n, 5)
+    target = seeded_target(cam)
+    f = Frame(params, cam, target, [1, 1, 1], 3)
+    f.screen()
+    grads = empty((58, n), t.float32)
+    f.solver.map_gradients(cam, f.renderer, f.p.data_ptr(), n, 3, grads.data_ptr())
+    sync()
+    g = grads.cpu().numpy()
+    run_step(f, lr=1e-4)
+    m_ptr, v_ptr, it = f.solver.moments()
+    assert it == 1
+    m = host(m_ptr, np.float32, 58 * n).reshape(58, n)
+    v = host(v_ptr, np.float32, 58 * n).reshape(58, n)
+    p = f.p.cpu().numpy()
+    lr = np.empty((58, 1), np.float32)
+    lr[0:3], lr[3:6], lr[6:9], lr[9] = 1e-4, 0.005, 0.001, 0.025
+    lr[10:] = 0.0025 / 20
+    lr[[10, 26, 42]] = 0.0025
+    f32 = np.float32
+    em = f32(0.1) * g
+    ev = f32(0.001) * g * g
+    c1, c2 = f32(1 / (1 - 0.9)), f32(1 / (1 - 0.999))
+    ep = params - lr * (em * c1) / (np.sqrt(ev * c2) + f32(1e-15))
+    # screen gradients are re-accumulated by the iterate (atomic order), so
+    # compare to rounding; a misplaced row or tile would be off by O(1)
+    assert np.mean(np.abs(m - em) <= 1e-3 * np.abs(em) + 1e-12) > 0.999
+    assert np.mean(np.abs(v - ev) <= 2e-3 * np.abs(ev) + 1e-18) > 0.999
+    assert np.mean(np.abs(p - ep) <= 1e-6 + 1e-3 * np.abs(ep - params)) > 0.999
+    # rows with exactly zero gradient keep their value and zero moments
+    zero = g == 0
+    assert np.array_equal(p[zero], params[zero]) and not m[zero].any() and not v[zero].any()
+
+
 @pytest.mark.parametrize("sh", [0, 1, 2, 3])
 def test_update_directions_match_finite_differences(sh):
     # solver_test.cu:58-95
