@@ -13,6 +13,12 @@ means N(0, 3^2)); 200 cameras on a ring of radius 8 at elevation +/-15 deg,
 hidden model and quantised to u8. The model being optimised is a 1.2M-Gaussian
 draw of the same distribution (seed 8).
 
+Two forms of the same iteration are timed: `plain_fp32` (eager launches from
+the host) and `graph_fp32` (the iteration captured once as a CUDA graph over a
+fixed record capacity and replayed from a device schedule of views). `value`
+is the faster form that completed without a record overflow; both are in
+`forms`.
+
 Printed JSON line: `value` is iterations/s with targets resident in HBM,
 `e2e` the same through host buffers (pinned H2D target upload and a D2H loss
 read every step), plus per-stage device times, the roofline of the dominant
@@ -327,13 +333,60 @@ def run_gsn(args):
     value_e2e = world * args.steps / (ms_e2e / 1000.0)
     psnr = float(loss_host[3])
 
+    b = renderer.buffers()
+    records = int(b.record_count_host)
+
+    # batched form: the same iteration captured once as a CUDA graph over a
+    # fixed record capacity, replayed from a device schedule of views
+    graph = gsn.Graph()
+    capacity = int(records * 1.5) + 65536
+    graph.capture(renderer, solver, params.data_ptr(), n, train, targets.data_ptr(), 1064 * 1600 * 3,
+                  [0, 0, 0], img.data_ptr(), SH_DEGREE, capacity, sp)
+    schedule = [(args.warmup + k) % len(train) for k in range(args.steps)]
+    graph.run(schedule[:max(3, args.warmup)], [lr] * max(3, args.warmup))
+    barrier()
+    torch.cuda.synchronize()
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = gsn.launch_count()
+    g0.record(stream)
+    graph.run(schedule, [lr] * args.steps)
+    g1.record(stream)
+    torch.cuda.synchronize()
+    graph_launches = gsn.launch_count() - launches0
+    barrier()
+    ms_graph = g0.elapsed_time(g1)
+    if dist is not None:
+        t = torch.tensor([ms_graph], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_graph = float(t.item())
+    graph_status = graph.check()
+    # end-to-end: pinned target upload, one replay and the loss read per step
+    barrier()
+    torch.cuda.synchronize()
+    g0.record(stream)
+    for k in range(args.steps):
+        v = schedule[k]
+        targets[v].copy_(host_targets[v], non_blocking=True)
+        graph.run([v], [lr])
+        gsn.memcpy_async(loss_host.data_ptr(), solver.loss_device(), 32, sp)
+        stream.synchronize()
+    g1.record(stream)
+    torch.cuda.synchronize()
+    ms_graph_e2e = g0.elapsed_time(g1)
+    if dist is not None:
+        t = torch.tensor([ms_graph_e2e], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_graph_e2e = float(t.item())
+    graph_status = graph_status or graph.check()
+    launches_per_step = graph.launches_per_step()
+    graph.close()
+    value_graph = world * args.steps / (ms_graph / 1000.0)
+    value_graph_e2e = world * args.steps / (ms_graph_e2e / 1000.0)
+
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
         return
-
-    b = renderer.buffers()
-    records = int(b.record_count_host)
     cam = train[0]
     tiles = cam.tile_count_x * cam.tile_count_y
     pixels = cam.width * cam.height
@@ -370,17 +423,29 @@ def run_gsn(args):
         tgt0 = targets[0].cpu().numpy()
         res = cpu_baseline(model, train[0], tgt0, extent, steps=1)
         cpu = {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    graph_ok = graph_status == 0
+    forms = {
+        "plain_fp32": {"value": round(value, 3), "ms_per_step": round(ms / args.steps, 4),
+                       "e2e": round(value_e2e, 3), "gpu_launches": int(launches)},
+        "graph_fp32": {"value": round(value_graph, 3), "ms_per_step": round(ms_graph / args.steps, 4),
+                       "e2e": round(value_graph_e2e, 3), "gpu_launches": int(graph_launches),
+                       "launches_per_step": launches_per_step, "record_capacity": capacity,
+                       "status": graph_status},
+    }
+    chosen = "graph_fp32" if graph_ok and value_graph > value else "plain_fp32"
     out = {
-        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True,
+        "metric": METRIC, "value": forms[chosen]["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": forms[chosen]["ms_per_step"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": ("plain FP32 training step (render, L1+SSIM gradient, backward, Adam) at the "
+        "config": {"workload": ("FP32 training step (render, L1+SSIM gradient, backward, Adam) at the "
                                 "1.2M-Gaussian cap, 1600x1064, SH degree 3, one ring view per step"),
-                   "form": "plain_fp32", "gaussians": n, "width": 1600, "height": 1064,
+                   "form": chosen, "gaussians": n, "width": 1600, "height": 1064,
                    "records_per_step": records, "visible_gaussians": vis, "parallelism": f"replicas{world}",
                    "l2": "inputs larger than L2 (params + Adam moments 835 MB, a new 5 MB target per step)"},
-        "gpu_launches": int(launches),
-        "e2e": {"value": round(value_e2e, 3), "unit": UNIT, "h2d_bytes_per_step": 1600 * 1064 * 3,
+        "gpu_launches": forms[chosen]["gpu_launches"],
+        "forms": forms,
+        "chosen_over_plain": round(forms[chosen]["value"] / value, 4),
+        "e2e": {"value": forms[chosen]["e2e"], "unit": UNIT, "h2d_bytes_per_step": 1600 * 1064 * 3,
                 "d2h_bytes_per_step": 32, "psnr_db_last_step": round(psnr, 3)},
         "roofline": roofline,
         "stages": stage_table,

@@ -9,6 +9,7 @@
 
 #include "core/density/density_controller.h"
 #include "core/gaussian_splatting.h"
+#include "core/graph/training_graph.h"
 #include "io/ply.h"
 #include "core/knn/knn.h"
 #include "core/render/renderer.h"
@@ -31,6 +32,11 @@ struct gsn_density {
 
 struct gsn_trainer {
     gs_native::GaussianSplatting impl;
+};
+
+struct gsn_graph {
+    gs_native::TrainingGraph impl;
+    gs_native::GaussianBuffers gaussians;
 };
 
 namespace {
@@ -556,6 +562,50 @@ int gsn_ply_read(const char* path, float* params, int count) {
     if (static_cast<int>(g.size()) != count) return GSN_ERR_INVALID_ARGUMENT;
     std::vector<float> p = gs_native::PackGaussians(g);
     std::copy(p.begin(), p.end(), params);
+    return GSN_OK;
+}
+
+// ---------------------------------------------------------------- batched form
+int gsn_graph_create(gsn_graph** out) {
+    if (!out) return GSN_ERR_INVALID_ARGUMENT;
+    *out = new (std::nothrow) gsn_graph();
+    return *out ? GSN_OK : GSN_ERR_OUT_OF_MEMORY;
+}
+
+int gsn_graph_destroy(gsn_graph* g) {
+    delete g;
+    return GSN_OK;
+}
+
+int gsn_graph_capture(gsn_graph* g, gsn_renderer* renderer, gsn_solver* solver, float* params, int count,
+                      const gsn_camera* cameras, int camera_count, const uint8_t* device_targets,
+                      size_t target_stride, const float* background, float* device_image, int sh_degree,
+                      int64_t record_capacity, void* stream) {
+    if (!g || !renderer || !solver || !params || count <= 0 || !cameras || camera_count <= 0 || !background)
+        return GSN_ERR_INVALID_ARGUMENT;
+    std::vector<gs_native::CameraParams> cams(static_cast<size_t>(camera_count));
+    for (int k = 0; k < camera_count; ++k) cams[k] = AsCamera(cameras + k);
+    g->gaussians = View(params, count);
+    return g->impl.Capture(renderer->impl, solver->impl, g->gaussians, cams, device_targets, target_stride,
+                           background, device_image, sh_degree, record_capacity, AsStream(stream))
+               ? GSN_OK
+               : GSN_ERR_INVALID_ARGUMENT;
+}
+
+int gsn_graph_run(gsn_graph* g, const int* views, const float* position_lrs, int steps) {
+    if (!g) return GSN_ERR_INVALID_ARGUMENT;
+    if (!g->impl.Captured()) return GSN_ERR_NOT_READY;
+    return g->impl.Run(views, position_lrs, steps) ? GSN_OK : GSN_ERR_INVALID_ARGUMENT;
+}
+
+int gsn_graph_check(gsn_graph* g) {
+    if (!g) return GSN_ERR_INVALID_ARGUMENT;
+    return g->impl.Check();
+}
+
+int gsn_graph_launches_per_step(gsn_graph* g, int* out) {
+    if (!g || !out) return GSN_ERR_INVALID_ARGUMENT;
+    *out = g->impl.LaunchesPerStep();
     return GSN_OK;
 }
 

@@ -269,13 +269,14 @@ __global__ void __launch_bounds__(256, 2) gaussian_update_kernel(GaussianUpdateA
     float in[9] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y, s1.z, s1.w, s2.x};
     float adu = s2.y, adv = s2.z;
     const bool visible = a.tile_counts[i] > 0;
+    const gsn_camera cam = a.frame ? a.frame->cam : a.cam;
 
     // view-space statistics (solver.cu:468-490) and round accumulation
     // (density_controller.cu:280-295)
-    float x = in[0] * (0.5f * a.cam.width);
-    float y = in[1] * (0.5f * a.cam.height);
-    float ax = adu * (0.5f * a.cam.width);
-    float ay = adv * (0.5f * a.cam.height);
+    float x = in[0] * (0.5f * cam.width);
+    float y = in[1] * (0.5f * cam.height);
+    float ax = adu * (0.5f * cam.width);
+    float ay = adv * (0.5f * cam.height);
     float signed_len = sqrtf(x * x + y * y);
     float abs_len = sqrtf(ax * ax + ay * ay);
     if (a.stats) {
@@ -297,7 +298,7 @@ __global__ void __launch_bounds__(256, 2) gaussian_update_kernel(GaussianUpdateA
     for (int k = 0; k < 9; ++k) active = active || in[k] != 0.0f;
     Chain ch;
     if (active) {
-        chain_rule<D>(a.params, N, i, a.cam, in, ch);
+        chain_rule<D>(a.params, N, i, cam, in, ch);
     } else {
 #pragma unroll
         for (int k = 0; k < 10; ++k) ch.g[k] = 0.0f;
@@ -319,8 +320,11 @@ __global__ void __launch_bounds__(256, 2) gaussian_update_kernel(GaussianUpdateA
     float* __restrict__ P = a.params;
     float* __restrict__ M = a.m;
     float* __restrict__ V = a.v;
-    const float lr_geo[10] = {a.lr[0], a.lr[0], a.lr[0], a.lr[1], a.lr[1], a.lr[1], a.lr[2], a.lr[2], a.lr[2], a.lr[3]};
-    adam_rows<10>(P, M, V, N, i, 0, ch.g, lr_geo, a.c1, a.c2);
+    const float lr0 = a.frame ? a.frame->position_lr : a.lr[0];
+    const float c1 = a.frame ? a.frame->c1 : a.c1;
+    const float c2 = a.frame ? a.frame->c2 : a.c2;
+    const float lr_geo[10] = {lr0, lr0, lr0, a.lr[1], a.lr[1], a.lr[1], a.lr[2], a.lr[2], a.lr[2], a.lr[3]};
+    adam_rows<10>(P, M, V, N, i, 0, ch.g, lr_geo, c1, c2);
     float lr_sh[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) lr_sh[k] = a.lr[5];
@@ -332,7 +336,7 @@ __global__ void __launch_bounds__(256, 2) gaussian_update_kernel(GaussianUpdateA
 #pragma unroll
             for (int k = 0; k < 8; ++k) g8[k] = half * 8 + k < K ? ch.grgb[c] * ch.basis[half * 8 + k] : 0.0f;
             lr_sh[0] = half == 0 ? a.lr[4] : a.lr[5];
-            adam_rows<8>(P, M, V, N, i, GSN_SH_INDEX + c * kShStride + half * 8, g8, lr_sh, a.c1, a.c2);
+            adam_rows<8>(P, M, V, N, i, GSN_SH_INDEX + c * kShStride + half * 8, g8, lr_sh, c1, c2);
         }
     }
 }

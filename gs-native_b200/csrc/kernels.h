@@ -11,6 +11,38 @@
 
 namespace gsn {
 
+// ---------------------------------------------------------------- step frame
+// Per-iteration values that the batched (CUDA graph) form keeps in device
+// memory, so that one captured iteration serves every step: the view's camera,
+// its resident training target and the step's scalars. Kernels given a frame
+// read these instead of their by-value arguments. All views of one graph share
+// the resolution (and so the tile grid and record layout) it was captured with.
+struct StepFrame {
+    gsn_camera cam;
+    const uint8_t* target;
+    float position_lr;
+    float c1, c2;  // Adam bias corrections of this step
+    int view;
+    int step;      // index into the schedule
+};
+
+// Host-written schedule read by the frame kernel at the start of each step.
+struct StepSchedule {
+    const gsn_camera* cameras;  // [view_count]
+    const uint8_t* targets;     // view v's target at targets + v * target_stride
+    int64_t target_stride;
+    const int* views;           // [steps]
+    const float* position_lr;   // [steps]
+    const float* c1;            // [steps]
+    const float* c2;            // [steps]
+    int* cursor;                // next step; advanced by the frame kernel
+    int* status;                // sticky GSN_ERR_CAPACITY: schedule, view index or records ran out
+    const int* overflow;        // the renderer's record-overflow flag of the previous step
+    int steps;
+    int view_count;
+};
+int launch_advance_frame(const StepSchedule& s, StepFrame* frame, cudaStream_t stream);
+
 // ---------------------------------------------------------------- projection
 struct ProjectOutputs {
     float2* means;           // [N] pixel-space centre (u, v)
@@ -22,7 +54,8 @@ struct ProjectOutputs {
     uint32_t* depth_keys;    // [N] float bits of z, 0xFFFFFFFF when culled
     float* radii;            // [N] optional 3-sigma pixel radius (0 = culled), may be null
 };
-int launch_project(const float* params, int n, const gsn_camera& cam, int sh_degree,
+// cam_dev (optional): device camera read instead of `cam` (batched form).
+int launch_project(const float* params, int n, const gsn_camera& cam, const gsn_camera* cam_dev, int sh_degree,
                    const ProjectOutputs& out, cudaStream_t stream);
 
 // ---------------------------------------------------------------- sorting
@@ -88,8 +121,9 @@ int launch_raster_forward(const RasterForwardArgs& a, cudaStream_t stream);
 // dL/dimage of 0.8 * L1 + 0.2 * (1 - SSIM) for an fp32 HWC image against a u8
 // HWC target. `sums` (optional, 3 doubles, zeroed by the launcher) receives
 // sum|I - T|, sum SSIM and sum (I - T)^2 in FP64.
-int launch_loss_gradient(const float* image, const uint8_t* target, float* grad, int width, int height,
-                         double* sums, cudaStream_t stream);
+// frame (optional): the target is frame->target instead of `target`.
+int launch_loss_gradient(const float* image, const uint8_t* target, const StepFrame* frame, float* grad, int width,
+                         int height, double* sums, cudaStream_t stream);
 // out[0..3] = loss, mean L1, mean SSIM, PSNR (dB) from the sums above.
 int launch_finalize_loss(const double* sums, int width, int height, double* out, cudaStream_t stream);
 
@@ -125,6 +159,7 @@ struct GaussianUpdateArgs {
     float* abs_sums;
     unsigned int* obs_counts;
     float* grads_out;         // optional 58 x n mapped parameter gradients
+    const StepFrame* frame;   // optional: camera, lr[0], c1 and c2 come from the device frame
 };
 int launch_gaussian_update(const GaussianUpdateArgs& a, int sh_degree, cudaStream_t stream);
 

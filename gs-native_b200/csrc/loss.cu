@@ -55,10 +55,12 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
 // produced by one thread from a register window of its row (or column), with
 // the 11 taps accumulated in ascending order as in solver.cu:65-161.
 __global__ void __launch_bounds__(kThreads, 2) loss_gradient_kernel(const float* __restrict__ image,
-                                                                   const uint8_t* __restrict__ target,
+                                                                   const uint8_t* __restrict__ target_arg,
+                                                                   const StepFrame* __restrict__ frame,
                                                                    float* __restrict__ grad, int width, int height,
                                                                    double* __restrict__ sums) {
     extern __shared__ float smem[];
+    const uint8_t* __restrict__ target = frame ? frame->target : target_arg;
     __shared__ double red[kThreads / 32];
     float* raw_i = smem;                 // [kIn][kIn]
     float* raw_t = raw_i + kRaw;         // [kIn][kIn]
@@ -239,8 +241,8 @@ __global__ void finalize_loss_kernel(const double* sums, int width, int height, 
 
 }  // namespace
 
-int launch_loss_gradient(const float* image, const uint8_t* target, float* grad, int width, int height,
-                         double* sums, cudaStream_t stream) {
+int launch_loss_gradient(const float* image, const uint8_t* target, const StepFrame* frame, float* grad, int width,
+                         int height, double* sums, cudaStream_t stream) {
     if (width <= 0 || height <= 0) return GSN_ERR_INVALID_ARGUMENT;
     if (sums && cudaMemsetAsync(sums, 0, 3 * sizeof(double), stream) != cudaSuccess) return GSN_ERR_CUDA;
     // the dynamic shared-memory opt-in is a per-device function attribute
@@ -254,7 +256,7 @@ int launch_loss_gradient(const float* image, const uint8_t* target, float* grad,
         if (device >= 0 && device < 64) configured[device] = true;
     }
     dim3 grid(ceil_div(width, kT), ceil_div(height, kT), 3);
-    loss_gradient_kernel<<<grid, kThreads, kSmemBytes, stream>>>(image, target, grad, width, height, sums);
+    loss_gradient_kernel<<<grid, kThreads, kSmemBytes, stream>>>(image, target, frame, grad, width, height, sums);
     return launched(1);
 }
 

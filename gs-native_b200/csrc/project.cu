@@ -43,10 +43,11 @@ __device__ __forceinline__ void sh_basis(float x, float y, float z, float b[16])
 
 template <int D>
 __global__ void __launch_bounds__(256) project_kernel(const float* __restrict__ params,
-                                                      gsn_camera cam, int n,
-                                                      ProjectOutputs out) {
+                                                      gsn_camera cam_arg, const gsn_camera* __restrict__ cam_dev,
+                                                      int n, ProjectOutputs out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    const gsn_camera cam = cam_dev ? *cam_dev : cam_arg;
     const int64_t N = n;
     out.tile_counts[i] = 0;
     out.depth_keys[i] = 0xFFFFFFFFu;
@@ -143,15 +144,15 @@ __global__ void __launch_bounds__(256) project_kernel(const float* __restrict__ 
 
 }  // namespace
 
-int launch_project(const float* params, int n, const gsn_camera& cam, int sh_degree,
+int launch_project(const float* params, int n, const gsn_camera& cam, const gsn_camera* cam_dev, int sh_degree,
                    const ProjectOutputs& out, cudaStream_t stream) {
     if (n <= 0) return GSN_OK;
     dim3 grid(ceil_div(n, 256));
     switch (sh_degree < 0 ? 0 : (sh_degree > 3 ? 3 : sh_degree)) {
-        case 0: project_kernel<0><<<grid, 256, 0, stream>>>(params, cam, n, out); break;
-        case 1: project_kernel<1><<<grid, 256, 0, stream>>>(params, cam, n, out); break;
-        case 2: project_kernel<2><<<grid, 256, 0, stream>>>(params, cam, n, out); break;
-        default: project_kernel<3><<<grid, 256, 0, stream>>>(params, cam, n, out); break;
+        case 0: project_kernel<0><<<grid, 256, 0, stream>>>(params, cam, cam_dev, n, out); break;
+        case 1: project_kernel<1><<<grid, 256, 0, stream>>>(params, cam, cam_dev, n, out); break;
+        case 2: project_kernel<2><<<grid, 256, 0, stream>>>(params, cam, cam_dev, n, out); break;
+        default: project_kernel<3><<<grid, 256, 0, stream>>>(params, cam, cam_dev, n, out); break;
     }
     return launched(1);
 }

@@ -529,3 +529,64 @@ def ply_read(path):
     out = np.zeros((58, n.value), dtype=np.float32)
     st = L.gsn_ply_read(str(path).encode(), ctypes.c_void_p(out.ctypes.data), n.value)
     return st, out
+
+
+class Graph:
+    """Batched form: one CUDA graph per training iteration, replayed from a
+    device schedule (gs-native extension, include/gsn.h "batched form")."""
+
+    def __init__(self):
+        L = lib()
+        vp, i32, i64, P = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.POINTER
+        sigs = {
+            "gsn_graph_create": [P(vp)], "gsn_graph_destroy": [vp],
+            "gsn_graph_capture": [vp, vp, vp, vp, i32, P(Camera), i32, vp, ctypes.c_size_t, c_float_p, vp, i32,
+                                  i64, vp],
+            "gsn_graph_run": [vp, P(i32), P(ctypes.c_float), i32], "gsn_graph_check": [vp],
+            "gsn_graph_launches_per_step": [vp, P(i32)],
+        }
+        for name, args in sigs.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = i32
+        h = ctypes.c_void_p()
+        _check(L.gsn_graph_create(ctypes.byref(h)), "gsn_graph_create")
+        self.handle = h
+        self._keep = []
+
+    def close(self):
+        if self.handle:
+            lib().gsn_graph_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def capture(self, renderer, solver, params_ptr, count, cameras, targets_ptr, target_stride, background,
+                image_ptr, sh_degree, record_capacity, stream=0):
+        cams = (Camera * len(cameras))(*cameras)
+        bg = floats3(background)
+        self._keep = [cams, bg, renderer, solver]
+        _check(lib().gsn_graph_capture(self.handle, renderer.handle, solver.handle, ctypes.c_void_p(params_ptr),
+                                       int(count), cams, len(cameras), ctypes.c_void_p(targets_ptr),
+                                       int(target_stride), bg, ctypes.c_void_p(image_ptr), int(sh_degree),
+                                       int(record_capacity), ctypes.c_void_p(stream)), "gsn_graph_capture")
+
+    def run(self, views, position_lrs):
+        n = len(views)
+        assert len(position_lrs) == n
+        v = (ctypes.c_int * n)(*[int(x) for x in views])
+        lr = (ctypes.c_float * n)(*[float(x) for x in position_lrs])
+        _check(lib().gsn_graph_run(self.handle, v, lr, n), "gsn_graph_run")
+
+    def check(self):
+        """0, or the gsn status (GSN_ERR_CAPACITY = -4 on a record overflow)."""
+        return lib().gsn_graph_check(self.handle)
+
+    def launches_per_step(self):
+        out = ctypes.c_int()
+        _check(lib().gsn_graph_launches_per_step(self.handle, ctypes.byref(out)), "launches_per_step")
+        return out.value

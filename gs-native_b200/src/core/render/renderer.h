@@ -52,6 +52,10 @@ public:
     // frame whose records exceed the capacity sets the overflow flag instead.
     // 0 restores the default grow-on-demand mode.
     bool SetRecordCapacity(int64_t records);
+    // Batched form: projection reads the camera from this device pointer (the
+    // step frame) instead of the host camera; the host camera still fixes the
+    // resolution and tile grid. nullptr restores the host camera.
+    void SetDeviceCamera(const gsn_camera* camera) { device_camera_ = camera; }
     const int* GetTileCounts() const { return tile_counts_.get(); }
     const int4* GetTileRects() const { return rects_.get(); }
     const float* GetDepths() const { return depths_.get(); }
@@ -73,6 +77,7 @@ private:
     size_t tile_capacity_ = 0;
     int64_t record_capacity_ = 0;
     bool fixed_capacity_ = false;
+    const gsn_camera* device_camera_ = nullptr;
     int64_t last_records_ = 0;
     int last_count_ = 0;
 

@@ -66,7 +66,7 @@ bool Solver::ComputeImageGradients(const CameraParams& camera, const float* imag
         sums = loss_.get();
     }
     gsn::stage_mark(stream_, gsn::kStageLossGradient);
-    if (gsn::launch_loss_gradient(image, target, image_gradients_.get(), camera.width_, camera.height_, sums,
+    if (gsn::launch_loss_gradient(image, target, frame_, image_gradients_.get(), camera.width_, camera.height_, sums,
                                   stream_) != GSN_OK)
         return false;
     if (sums && gsn::launch_finalize_loss(sums, camera.width_, camera.height_, loss_.get() + 3, stream_) != GSN_OK)
@@ -138,6 +138,7 @@ bool Solver::UpdateGaussians(const CameraParams& camera, const Renderer& rendere
         a.obs_counts = acc_count_;
     }
     a.grads_out = grads_out;
+    a.frame = frame_;
     gsn::stage_mark(stream_, gsn::kStageGaussianUpdate);
     if (gsn::launch_gaussian_update(a, std::clamp(sh_degree, 0, 3), stream_) != GSN_OK) return false;
     gsn::stage_mark(stream_, gsn::kStageOther);

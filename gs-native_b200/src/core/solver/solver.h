@@ -23,6 +23,10 @@
 #include "core/types/buffers.h"
 #include "util/device_array.h"
 
+namespace gsn {
+struct StepFrame;
+}
+
 namespace gs_native {
 
 // Learning rates per parameter group; position comes from Iterate().
@@ -74,6 +78,10 @@ public:
     float* GetSecondMoments() { return v_.get(); }
     int GetGaussianCapacity() const { return gaussian_count_; }
     uint64_t GetIteration() const { return iteration_; }
+    // Batched form: when set, the loss target, the camera of the update, the
+    // position learning rate and Adam's bias corrections are read from this
+    // device frame (written on the device at the start of each step).
+    void SetStepFrame(const gsn::StepFrame* frame) { frame_ = frame; }
     void SetIteration(uint64_t iteration) { iteration_ = iteration; }
 
     // Stage entry points (used by Iterate and by the C ABI).
@@ -102,6 +110,7 @@ private:
     float* acc_grad_ = nullptr;
     float* acc_abs_ = nullptr;
     unsigned int* acc_count_ = nullptr;
+    const gsn::StepFrame* frame_ = nullptr;
 };
 
 }  // namespace gs_native

@@ -317,6 +317,32 @@ int gsn_trainer_load(gsn_trainer* t, const char* path);
 int gsn_trainer_state(gsn_trainer* t, float** params, int* count, int* completed, int* sh_degree,
                       float* scene_extent);
 
+/* ------------------------------------------------------------------ batched form
+ * gs-native extension (the reference runs every stage from the host and reads
+ * the record count back each frame, renderer.cu:480-500): one CUDA graph holds
+ * a whole training iteration (projection, sorts, forward, loss, backward,
+ * Adam) over a fixed record capacity with device-side counts, and a device
+ * schedule supplies each replay's view, position learning rate and Adam step.
+ *
+ * gsn_graph_capture: the renderer and solver are bound to the graph (and their
+ * stream set to `stream`) until gsn_graph_destroy; `params` / `count` must stay
+ * the same block. cameras[0..camera_count) share one resolution; view v's u8
+ * HWC target is resident at device_targets + v * target_stride.
+ * gsn_graph_run: `steps` replays, view views[k] with position lr
+ * position_lrs[k] (host arrays); asynchronous on the capture stream.
+ * gsn_graph_check: synchronises; GSN_ERR_CAPACITY if any step since the last
+ * check exceeded record_capacity tile records. */
+typedef struct gsn_graph gsn_graph;
+int gsn_graph_create(gsn_graph** out);
+int gsn_graph_destroy(gsn_graph* g);
+int gsn_graph_capture(gsn_graph* g, gsn_renderer* renderer, gsn_solver* solver, float* params, int count,
+                      const gsn_camera* cameras, int camera_count, const uint8_t* device_targets,
+                      size_t target_stride, const float* background, float* device_image, int sh_degree,
+                      int64_t record_capacity, void* stream);
+int gsn_graph_run(gsn_graph* g, const int* views, const float* position_lrs, int steps);
+int gsn_graph_check(gsn_graph* g);
+int gsn_graph_launches_per_step(gsn_graph* g, int* out);
+
 /* ------------------------------------------------------------------ PLY
  * WriteGaussiansPly / ReadGaussiansPly (reference src/io/data_io.cpp:420-590)
  * on a host 58 x count SoA block. */
