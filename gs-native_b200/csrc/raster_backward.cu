@@ -16,7 +16,12 @@
 //     and tile, instead of one per warp;
 //   * each warp walks only the records whose conservative alpha >= 1/255 box
 //     reaches its 16x8 pixel strip, powers below a record's alpha floor skip
-//     expf, and the three divisions by (1 - alpha) share one reciprocal.
+//     expf, and the three divisions by (1 - alpha) share one reciprocal;
+//   * the colour term of dL/dalpha is carried per pixel as two scalars (the
+//     gradient-weighted final colour and the gradient-weighted colour in front
+//     of the record) instead of three channel sums;
+//   * 80 registers (12 CTAs, 24 warps per SM): measured 0.81 ms against 0.88 ms
+//     at the unconstrained 122 registers; 72 and 64 registers spill and lose.
 // Per-Gaussian output (12 floats, Gaussian-major): d(u, v), d(cov a, b, c),
 // d(opacity logit), d(r, g, b), sum|du|, sum|dv|, 0.
 #include "raster_common.cuh"
@@ -30,7 +35,7 @@ constexpr int kVals = 12;
 
 __device__ __forceinline__ float sel(bool c, float a, float b) { return c ? a : b; }
 
-__global__ void __launch_bounds__(kRasterThreads) raster_backward_kernel(RasterBackwardArgs a) {
+__global__ void __launch_bounds__(kRasterThreads, 12) raster_backward_kernel(RasterBackwardArgs a) {
     __shared__ uint32_t s_id[kRasterBatch];
     __shared__ float2 s_mean[kRasterBatch];
     __shared__ float4 s_conic[kRasterBatch];
@@ -48,7 +53,9 @@ __global__ void __launch_bounds__(kRasterThreads) raster_backward_kernel(RasterB
     const int64_t end_all = a.tile_offsets[g.tile + 1];
 
     float fy[kPixPerThread], T[kPixPerThread];
-    float fin[kPixPerThread][3], gI[kPixPerThread][3], prefix[kPixPerThread][3];
+    // per pixel: dL/dcolour, S = dL/dcolour . final colour and P = dL/dcolour .
+    // colour accumulated in front of the current record
+    float gI[kPixPerThread][3], S[kPixPerThread], P[kPixPerThread];
     int limit[kPixPerThread];
     bool done[kPixPerThread];
     int my_bound = 0;
@@ -58,14 +65,15 @@ __global__ void __launch_bounds__(kRasterThreads) raster_backward_kernel(RasterB
         T[p] = 1.0f;
         limit[p] = 0;
         const bool inside = g.px < a.cam.width && g.py[p] < a.cam.height;
+        S[p] = P[p] = 0.0f;
 #pragma unroll
-        for (int c = 0; c < 3; ++c) fin[p][c] = gI[p][c] = prefix[p][c] = 0.0f;
+        for (int c = 0; c < 3; ++c) gI[p][c] = 0.0f;
         if (inside) {
             const int64_t pix = static_cast<int64_t>(g.py[p]) * a.cam.width + g.px;
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                fin[p][c] = a.image[pix * 3 + c];
                 gI[p][c] = a.image_grad[pix * 3 + c];
+                S[p] += gI[p][c] * a.image[pix * 3 + c];
             }
             limit[p] = a.contributors ? a.contributors[pix] : static_cast<int>(end_all - begin);
         }
@@ -147,13 +155,12 @@ __global__ void __launch_bounds__(kRasterThreads) raster_backward_kernel(RasterB
                         has |= take;
                         float w = alpha * T[p];
                         float inv = __frcp_rn(1.0f - alpha);
-                        float dalpha = 0.0f;
+                        // dL/dalpha = (dL/dC . (colour in front + T c - final)) / (1 - alpha)
+                        const float G = gI[p][0] * cc[0] + gI[p][1] * cc[1] + gI[p][2] * cc[2];
+                        float dalpha = (P[p] + T[p] * G - S[p]) * inv;
+                        const float wt = take ? w : 0.0f;
 #pragma unroll
-                        for (int c = 0; c < 3; ++c) {
-                            dalpha += gI[p][c] * (prefix[p][c] + T[p] * cc[c] - fin[p][c]);
-                            v[6 + c] += take ? w * gI[p][c] : 0.0f;
-                        }
-                        dalpha *= inv;
+                        for (int c = 0; c < 3; ++c) v[6 + c] += wt * gI[p][c];
                         float common = (take && raw < kAlphaMax) ? dalpha * raw : 0.0f;
                         float qx = q.x * dx + q.y * dy;
                         float qy = q.y * dx + q.z * dy;
@@ -165,8 +172,7 @@ __global__ void __launch_bounds__(kRasterThreads) raster_backward_kernel(RasterB
                         v[5] += common * (1.0f - q.w);
                         v[9] += fabsf(common * qx);
                         v[10] += fabsf(common * qy);
-#pragma unroll
-                        for (int c = 0; c < 3; ++c) prefix[p][c] = take ? prefix[p][c] + cc[c] * w : prefix[p][c];
+                        P[p] += wt * G;
                         T[p] = take ? nextT : T[p];
                     }
                 }

@@ -24,8 +24,8 @@ namespace {
 
 constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / 32;
-constexpr int kSortItems = 16;                      // per thread
-constexpr int kSortChunk = kSortThreads * kSortItems;  // 4096 keys per block
+constexpr int kSortItems = 8;                       // per thread
+constexpr int kSortChunk = kSortThreads * kSortItems;  // 2048 keys per block
 constexpr int kBins = 256;
 
 // Device-resident counts are clamped to the host-side capacity the grid was sized
@@ -118,7 +118,7 @@ __global__ void __launch_bounds__(kSortThreads) radix_scan(const int* n_dev, int
     }
 }
 
-// Stable scatter. Warp w owns the w-th 512-key slice of the block's chunk and
+// Stable scatter. Warp w owns the w-th 256-key slice of the block's chunk and
 // walks it in 32-key steps; eight ballots (one per digit bit) find the lanes with
 // an equal digit inside a step, and
 // warp-private counters carry the rank across steps, which keeps the original
@@ -412,7 +412,7 @@ int launch_radix_sort(uint32_t* keys, uint32_t* values, uint32_t* keys_alt, uint
 // ---------------------------------------------------------------- no-alloc sort
 // Scratch of gsn_sort_pairs_noalloc: the digit totals and per-block histograms
 // of the sort for up to kNoAllocMaxCount pairs, in a file-scope device array
-// (4.2 MB on every GPU that loads the library, held until exit). Host code
+// (8.4 MB on every GPU that loads the library, held until exit). Host code
 // cannot use the array's name as a device address, so its address is looked up
 // once per device with cudaGetSymbolAddress.
 constexpr int kNoAllocMaxCount = 1 << 24;
