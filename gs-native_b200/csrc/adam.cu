@@ -230,6 +230,21 @@ __device__ __forceinline__ void chain_rule(const float* __restrict__ p, int64_t 
 // row0. All loads of the group are issued before any store, so the three
 // streams of every row are in flight together; the parameter block and the
 // two moment arrays never alias.
+//
+// The step lr * m_hat / (sqrt(v_hat) + 1e-15) uses the hardware approximate
+// square root and divide (div.approx: 2 ulp for divisors in [2^-126, 2^126];
+// the divisor here is >= 1e-15) instead of the IEEE-rounded sequences, whose
+// special-case branches made this kernel branch-resolution bound (0.52 ms ->
+// 0.40 ms at 1.2M Gaussians). Moments are formed exactly as in the reference;
+// the parameter step differs from the reference's by at most a few ulps of
+// the step.
+// PTX sqrt.approx.f32 (relative error within 2^-23 on normal inputs).
+__device__ __forceinline__ float sqrt_approx(float x) {
+    float y;
+    asm("sqrt.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 template <int CNT>
 __device__ __forceinline__ void adam_rows(float* __restrict__ P, float* __restrict__ M, float* __restrict__ V,
                                           int64_t N, int i, int row0, const float* g, const float* lr, float c1,
@@ -248,7 +263,7 @@ __device__ __forceinline__ void adam_rows(float* __restrict__ P, float* __restri
         float second = 0.999f * v[r] + 0.001f * g[r] * g[r];
         m[r] = first;
         v[r] = second;
-        p[r] -= lr[r] * (first * c1) / (sqrtf(second * c2) + 1e-15f);
+        p[r] -= __fdividef(lr[r] * (first * c1), sqrt_approx(second * c2) + 1e-15f);
     }
 #pragma unroll
     for (int r = 0; r < CNT; ++r) {
