@@ -208,6 +208,12 @@ int gsn_renderer_record_offsets(gsn_renderer* r, const int** out) {
     return *out ? GSN_OK : GSN_ERR_CUDA;
 }
 
+int gsn_renderer_set_bf16_sh(gsn_renderer* r, int enabled) {
+    if (!r) return GSN_ERR_INVALID_ARGUMENT;
+    r->impl.SetBf16Sh(enabled != 0);
+    return GSN_OK;
+}
+
 int gsn_renderer_set_record_capacity(gsn_renderer* r, int64_t records) {
     if (!r) return GSN_ERR_INVALID_ARGUMENT;
     return r->impl.SetRecordCapacity(records) ? GSN_OK : GSN_ERR_INVALID_ARGUMENT;
@@ -266,6 +272,12 @@ int gsn_solver_set_learning_rates(gsn_solver* s, float scale, float rotation, fl
     lr.sh_dc = sh_dc;
     lr.sh_rest = sh_rest;
     s->impl.SetLearningRates(lr);
+    return GSN_OK;
+}
+
+int gsn_solver_set_bf16_sh(gsn_solver* s, int enabled) {
+    if (!s) return GSN_ERR_INVALID_ARGUMENT;
+    s->impl.SetBf16Sh(enabled != 0);
     return GSN_OK;
 }
 
@@ -383,6 +395,12 @@ int gsn_density_buffers(gsn_density* d, const int** history_parent_ids, const in
     return GSN_OK;
 }
 
+int gsn_density_set_bf16_sh(gsn_density* d, int enabled) {
+    if (!d) return GSN_ERR_INVALID_ARGUMENT;
+    d->impl.SetBf16Sh(enabled != 0);
+    return GSN_OK;
+}
+
 int gsn_density_set_max_gaussians(gsn_density* d, int max_gaussians) {
     if (!d || max_gaussians < 0) return GSN_ERR_INVALID_ARGUMENT;
     d->impl.SetMaxGaussians(max_gaussians);
@@ -428,6 +446,8 @@ int gsn_training_options_default(gsn_training_options* out) {
     out->max_gaussians = o.max_gaussians;
     out->density_seed = o.density_seed;
     out->initial_opacity = o.initial_opacity;
+    out->precision = o.bf16_sh ? 1 : 0;
+    out->graph = o.graph ? 1 : 0;
     return GSN_OK;
 }
 
@@ -460,6 +480,8 @@ gs_native::TrainingOptions ToOptions(const gsn_training_options& in) {
     o.max_gaussians = in.max_gaussians;
     o.density_seed = in.density_seed;
     o.initial_opacity = in.initial_opacity;
+    o.bf16_sh = in.precision != 0;
+    o.graph = in.graph != 0;
     return o;
 }
 }  // namespace

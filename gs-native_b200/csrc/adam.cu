@@ -26,7 +26,7 @@ struct Chain {
     float grgb[3];    // dL/dcolour, zero where the unclamped colour is negative
 };
 
-template <int D>
+template <int D, bool kBf16>
 __device__ __forceinline__ void sh_with_derivatives(const float* __restrict__ p, int64_t N, int i, const gsn_camera& cam,
                                                     float* basis, float* color, float* dcol) {
     constexpr int s = (D + 1) * (D + 1);
@@ -105,7 +105,7 @@ __device__ __forceinline__ void sh_with_derivatives(const float* __restrict__ p,
         float dv[3] = {0.0f, 0.0f, 0.0f};
 #pragma unroll
         for (int j = 0; j < s; ++j) {
-            float coef = p[(GSN_SH_INDEX + ch * kShStride + j) * N + i];
+            float coef = load_sh<kBf16>(p, N, ch * kShStride + j, i);
             value += coef * basis[j];
 #pragma unroll
             for (int a2 = 0; a2 < 3; ++a2) dv[a2] += coef * der[j * 3 + a2];
@@ -119,7 +119,7 @@ __device__ __forceinline__ void sh_with_derivatives(const float* __restrict__ p,
 }
 
 // Chain rule of solver.cu:512-622 for one Gaussian with screen gradients in[0..8].
-template <int D>
+template <int D, bool kBf16>
 __device__ __forceinline__ void chain_rule(const float* __restrict__ p, int64_t N, int i, const gsn_camera& cam,
                                            const float in[9], Chain& out) {
     float rot[9], crot[9], cov[9], pos[3], s2[3];
@@ -163,7 +163,7 @@ __device__ __forceinline__ void chain_rule(const float* __restrict__ p, int64_t 
                 LP[r * 3 + c] += P[r * 3 + j] * crot[j * 3 + c];
             }
     float color[3], dcol[9];
-    sh_with_derivatives<D>(p, N, i, cam, out.basis, color, dcol);
+    sh_with_derivatives<D, kBf16>(p, N, i, cam, out.basis, color, dcol);
     float right[3];
 #pragma unroll
     for (int axis = 0; axis < 3; ++axis) {
@@ -274,7 +274,39 @@ __device__ __forceinline__ void adam_rows(float* __restrict__ P, float* __restri
     }
 }
 
-template <int D>
+// Precision form: the same step on bf16 rows (SH parameters and their
+// moments), computed in fp32 and written back with stochastic rounding.
+template <int CNT>
+__device__ __forceinline__ void adam_rows_bf16(__nv_bfloat16* __restrict__ P, __nv_bfloat16* __restrict__ M,
+                                               __nv_bfloat16* __restrict__ V, int64_t N, int i, int row0,
+                                               const float* g, const float* lr, float c1, float c2, uint32_t& rng) {
+    float p[CNT], m[CNT], v[CNT];
+#pragma unroll
+    for (int r = 0; r < CNT; ++r) {
+        const int64_t idx = static_cast<int64_t>(row0 + r) * N + i;
+        p[r] = __bfloat162float(P[idx]);
+        m[r] = __bfloat162float(M[idx]);
+        v[r] = __bfloat162float(V[idx]);
+    }
+#pragma unroll
+    for (int r = 0; r < CNT; ++r) {
+        float first = 0.9f * m[r] + 0.1f * g[r];
+        float second = 0.999f * v[r] + 0.001f * g[r] * g[r];
+        m[r] = first;
+        v[r] = second;
+        p[r] -= __fdividef(lr[r] * (first * c1), sqrt_approx(second * c2) + 1e-15f);
+    }
+#pragma unroll
+    for (int r = 0; r < CNT; ++r) {
+        const int64_t idx = static_cast<int64_t>(row0 + r) * N + i;
+        const uint32_t r1 = xorshift32(rng), r2 = xorshift32(rng);
+        P[idx] = bf16_stochastic(p[r], r1);
+        M[idx] = bf16_stochastic(m[r], r1 >> 16);
+        V[idx] = bf16_stochastic(v[r], r2);
+    }
+}
+
+template <int D, bool kBf16>
 __global__ void __launch_bounds__(256, 2) gaussian_update_kernel(GaussianUpdateArgs a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n) return;
@@ -313,7 +345,7 @@ __global__ void __launch_bounds__(256, 2) gaussian_update_kernel(GaussianUpdateA
     for (int k = 0; k < 9; ++k) active = active || in[k] != 0.0f;
     Chain ch;
     if (active) {
-        chain_rule<D>(a.params, N, i, cam, in, ch);
+        chain_rule<D, kBf16>(a.params, N, i, cam, in, ch);
     } else {
 #pragma unroll
         for (int k = 0; k < 10; ++k) ch.g[k] = 0.0f;
@@ -343,6 +375,11 @@ __global__ void __launch_bounds__(256, 2) gaussian_update_kernel(GaussianUpdateA
     float lr_sh[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) lr_sh[k] = a.lr[5];
+    uint32_t rng = 0;
+    if constexpr (kBf16) {
+        const uint32_t seed = a.frame ? a.frame->seed : a.seed;
+        rng = fmix32(static_cast<uint32_t>(i) * 0x9E3779B9u ^ fmix32(seed)) | 1u;
+    }
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
 #pragma unroll
@@ -351,20 +388,41 @@ __global__ void __launch_bounds__(256, 2) gaussian_update_kernel(GaussianUpdateA
 #pragma unroll
             for (int k = 0; k < 8; ++k) g8[k] = half * 8 + k < K ? ch.grgb[c] * ch.basis[half * 8 + k] : 0.0f;
             lr_sh[0] = half == 0 ? a.lr[4] : a.lr[5];
-            adam_rows<8>(P, M, V, N, i, GSN_SH_INDEX + c * kShStride + half * 8, g8, lr_sh, c1, c2);
+            if constexpr (kBf16) {
+                auto* Pb = reinterpret_cast<__nv_bfloat16*>(P + kGeometryRows * N);
+                auto* Mb = reinterpret_cast<__nv_bfloat16*>(M + kGeometryRows * N);
+                auto* Vb = reinterpret_cast<__nv_bfloat16*>(V + kGeometryRows * N);
+                adam_rows_bf16<8>(Pb, Mb, Vb, N, i, c * kShStride + half * 8, g8, lr_sh, c1, c2, rng);
+            } else {
+                adam_rows<8>(P, M, V, N, i, GSN_SH_INDEX + c * kShStride + half * 8, g8, lr_sh, c1, c2);
+            }
         }
     }
 }
 
+template <bool kBf16>
 __global__ void remap_moments_kernel(const int* __restrict__ parents, const float* __restrict__ prev_m,
                                      const float* __restrict__ prev_v, float* __restrict__ m, float* __restrict__ v,
                                      int prev_count, int count) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
-    const int row = blockIdx.y;
+    const int row = blockIdx.y;  // logical row 0..57
     const int parent = parents ? parents[i] : -1;
+    const bool take = parent >= 0 && parent < prev_count;
+    if (kBf16 && row >= kGeometryRows) {
+        const int k = row - kGeometryRows;
+        const auto* pm = reinterpret_cast<const __nv_bfloat16*>(prev_m + kGeometryRows * static_cast<int64_t>(prev_count));
+        const auto* pv = reinterpret_cast<const __nv_bfloat16*>(prev_v + kGeometryRows * static_cast<int64_t>(prev_count));
+        auto* dm = reinterpret_cast<__nv_bfloat16*>(m + kGeometryRows * static_cast<int64_t>(count));
+        auto* dv = reinterpret_cast<__nv_bfloat16*>(v + kGeometryRows * static_cast<int64_t>(count));
+        const int64_t dst = static_cast<int64_t>(k) * count + i;
+        const int64_t src = static_cast<int64_t>(k) * prev_count + parent;
+        dm[dst] = take ? pm[src] : __float2bfloat16_rn(0.0f);
+        dv[dst] = take ? pv[src] : __float2bfloat16_rn(0.0f);
+        return;
+    }
     const int64_t dst = static_cast<int64_t>(row) * count + i;
-    if (parent >= 0 && parent < prev_count) {
+    if (take) {
         const int64_t src = static_cast<int64_t>(row) * prev_count + parent;
         m[dst] = prev_m[src];
         v[dst] = prev_v[src];
@@ -379,20 +437,31 @@ __global__ void remap_moments_kernel(const int* __restrict__ parents, const floa
 int launch_gaussian_update(const GaussianUpdateArgs& a, int sh_degree, cudaStream_t stream) {
     if (a.n <= 0) return GSN_OK;
     dim3 grid(ceil_div(a.n, 256));
-    switch (sh_degree < 0 ? 0 : (sh_degree > 3 ? 3 : sh_degree)) {
-        case 0: gaussian_update_kernel<0><<<grid, 256, 0, stream>>>(a); break;
-        case 1: gaussian_update_kernel<1><<<grid, 256, 0, stream>>>(a); break;
-        case 2: gaussian_update_kernel<2><<<grid, 256, 0, stream>>>(a); break;
-        default: gaussian_update_kernel<3><<<grid, 256, 0, stream>>>(a); break;
+    const int d = sh_degree < 0 ? 0 : (sh_degree > 3 ? 3 : sh_degree);
+    if (a.bf16_sh) {
+        switch (d) {
+            case 0: gaussian_update_kernel<0, true><<<grid, 256, 0, stream>>>(a); break;
+            case 1: gaussian_update_kernel<1, true><<<grid, 256, 0, stream>>>(a); break;
+            case 2: gaussian_update_kernel<2, true><<<grid, 256, 0, stream>>>(a); break;
+            default: gaussian_update_kernel<3, true><<<grid, 256, 0, stream>>>(a); break;
+        }
+    } else {
+        switch (d) {
+            case 0: gaussian_update_kernel<0, false><<<grid, 256, 0, stream>>>(a); break;
+            case 1: gaussian_update_kernel<1, false><<<grid, 256, 0, stream>>>(a); break;
+            case 2: gaussian_update_kernel<2, false><<<grid, 256, 0, stream>>>(a); break;
+            default: gaussian_update_kernel<3, false><<<grid, 256, 0, stream>>>(a); break;
+        }
     }
     return launched(1);
 }
 
 int launch_remap_moments(const int* parents, const float* prev_m, const float* prev_v, float* m, float* v,
-                         int prev_count, int count, cudaStream_t stream) {
+                         int prev_count, int count, bool bf16_sh, cudaStream_t stream) {
     if (count <= 0) return GSN_OK;
     dim3 grid(ceil_div(count, 256), kParams);
-    remap_moments_kernel<<<grid, 256, 0, stream>>>(parents, prev_m, prev_v, m, v, prev_count, count);
+    if (bf16_sh) remap_moments_kernel<true><<<grid, 256, 0, stream>>>(parents, prev_m, prev_v, m, v, prev_count, count);
+    else remap_moments_kernel<false><<<grid, 256, 0, stream>>>(parents, prev_m, prev_v, m, v, prev_count, count);
     return launched(1);
 }
 

@@ -1,6 +1,7 @@
 // Shared device-side definitions for the gs-native B200 kernels (sm_100a).
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -46,6 +47,58 @@ inline int launch_status() {
 inline int launched(int kernels) {
     note_launch(kernels);
     return launch_status();
+}
+
+// ---------------------------------------------------------------- layouts
+// Parameter block layouts. The plain form uses the reference's 58 fp32 rows of
+// stride N. The precision form keeps the 10 geometry rows (position, log-scale,
+// axis-angle, opacity logit) in fp32 and stores the 48 SH rows as bf16 rows of
+// stride N right after them, so its block is 10 + 24 = 34 float rows. Adam's
+// moments use the same layout as the parameters.
+constexpr int kGeometryRows = GSN_SH_INDEX;  // 10
+constexpr int kShRows = 3 * kShStride;       // 48
+constexpr int kPrecisionPhysicalRows = kGeometryRows + kShRows / 2;  // 34
+
+template <bool kBf16>
+__host__ __device__ constexpr int physical_rows() { return kBf16 ? kPrecisionPhysicalRows : kParams; }
+
+template <bool kBf16>
+__device__ __forceinline__ float load_sh(const float* block, int64_t n, int k, int64_t i) {
+    if constexpr (kBf16) {
+        const __nv_bfloat16* sh = reinterpret_cast<const __nv_bfloat16*>(block + kGeometryRows * n);
+        return __bfloat162float(sh[k * n + i]);
+    } else {
+        return block[(kGeometryRows + k) * n + i];
+    }
+}
+
+// 32-bit xorshift generator (Marsaglia 2003) for stochastic rounding; seeded per
+// thread with the MurmurHash3 finaliser of (element, step).
+__device__ __forceinline__ uint32_t fmix32(uint32_t h) {
+    h ^= h >> 16;
+    h *= 0x85ebca6bu;
+    h ^= h >> 13;
+    h *= 0xc2b2ae35u;
+    h ^= h >> 16;
+    return h;
+}
+
+__device__ __forceinline__ uint32_t xorshift32(uint32_t& x) {
+    x ^= x << 13;
+    x ^= x >> 17;
+    x ^= x << 5;
+    return x;
+}
+
+// fp32 -> bf16 by stochastic rounding: the 16 dropped mantissa bits decide the
+// direction with probability equal to their fraction of an ulp, so the rounding
+// is unbiased and small Adam steps accumulate in expectation. Inf and NaN
+// convert as with round-to-nearest.
+__device__ __forceinline__ __nv_bfloat16 bf16_stochastic(float x, uint32_t noise16) {
+    uint32_t u = __float_as_uint(x);
+    if ((u & 0x7f800000u) == 0x7f800000u) return __float2bfloat16_rn(x);
+    u += noise16 & 0xffffu;
+    return __ushort_as_bfloat16(static_cast<unsigned short>(u >> 16));
 }
 
 // Rodrigues rotation of an axis-angle vector. The expression order is the one

@@ -235,7 +235,9 @@ __global__ void samples_kernel(const int* __restrict__ control, float* __restric
 }
 
 // density_controller.cu:168-243 (children) and 245-278 (parent ids, new flags,
-// statistics reset), fused: one thread per source Gaussian.
+// statistics reset), fused: one thread per source Gaussian. kBf16: precision-form
+// layout (the 48 SH rows are bf16 and are copied bit for bit).
+template <bool kBf16>
 __global__ void write_kernel(const float* __restrict__ params, const int4* __restrict__ counts,
                              const int4* __restrict__ offsets, const int* __restrict__ control,
                              const float* __restrict__ samples, float* __restrict__ out,
@@ -286,7 +288,13 @@ __global__ void write_kernel(const float* __restrict__ params, const int4* __res
             atomicExch(const_cast<int*>(control) + 2, 1);
             return;
         }
-        for (int p = 0; p < kParams; ++p) {
+        if constexpr (kBf16) {
+            const auto* in_sh = reinterpret_cast<const __nv_bfloat16*>(params + kGeometryRows * N);
+            auto* out_sh = reinterpret_cast<__nv_bfloat16*>(out + kGeometryRows * static_cast<int64_t>(out_stride));
+            for (int k = 0; k < kShRows; ++k)
+                out_sh[static_cast<int64_t>(k) * out_stride + dst] = in_sh[static_cast<int64_t>(k) * N + id];
+        }
+        for (int p = 0; p < (kBf16 ? kGeometryRows : kParams); ++p) {
             float value = params[static_cast<int64_t>(p) * N + id];
             if (split && p < GSN_POSITION_INDEX + 3) {
                 float delta = 0;
@@ -389,8 +397,14 @@ int launch_density_prepare(const int4* offsets, int* control, int n, int random_
 
 int launch_density_apply(const DensityApplyArgs& a, cudaStream_t s) {
     samples_kernel<<<a.random_blocks, kThreads, 0, s>>>(a.control, a.samples, a.random_blocks, a.seed);
-    write_kernel<<<grid_for(a.n), kThreads, 0, s>>>(a.params, a.counts, a.offsets, a.control, a.samples, a.out,
-                                                   a.history_parents, a.parents, a.new_flags, a.n, a.out_stride);
+    if (a.bf16_sh)
+        write_kernel<true><<<grid_for(a.n), kThreads, 0, s>>>(a.params, a.counts, a.offsets, a.control, a.samples,
+                                                              a.out, a.history_parents, a.parents, a.new_flags, a.n,
+                                                              a.out_stride);
+    else
+        write_kernel<false><<<grid_for(a.n), kThreads, 0, s>>>(a.params, a.counts, a.offsets, a.control, a.samples,
+                                                               a.out, a.history_parents, a.parents, a.new_flags, a.n,
+                                                               a.out_stride);
     finish_kernel<<<grid_for(a.n), kThreads, 0, s>>>(a.sums, a.abs_sums, a.obs, a.control);
     return launched(3);
 }

@@ -56,6 +56,7 @@ struct DensityApplyArgs {
     int out_stride;
     int random_blocks;
     unsigned long long seed;
+    bool bf16_sh;       // precision-form layout (10 fp32 rows + 48 bf16 SH rows)
 };
 
 int launch_density_init(int* control, int count, cudaStream_t s);

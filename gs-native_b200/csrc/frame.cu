@@ -40,6 +40,7 @@ __global__ void __launch_bounds__(32) advance_frame_kernel(StepSchedule s, StepF
         f->position_lr = s.position_lr[step];
         f->c1 = s.c1[step];
         f->c2 = s.c2[step];
+        f->seed = s.seeds[step];
         f->view = view;
         f->step = step;
     }
@@ -48,7 +49,7 @@ __global__ void __launch_bounds__(32) advance_frame_kernel(StepSchedule s, StepF
 }  // namespace
 
 int launch_advance_frame(const StepSchedule& s, StepFrame* frame, cudaStream_t stream) {
-    if (!frame || !s.cameras || !s.targets || !s.views || !s.position_lr || !s.c1 || !s.c2 || !s.cursor ||
+    if (!frame || !s.cameras || !s.targets || !s.views || !s.position_lr || !s.c1 || !s.c2 || !s.seeds || !s.cursor ||
         !s.status || s.steps <= 0 || s.view_count <= 0)
         return GSN_ERR_INVALID_ARGUMENT;
     advance_frame_kernel<<<1, 32, 0, stream>>>(s, frame);

@@ -22,6 +22,7 @@ struct StepFrame {
     const uint8_t* target;
     float position_lr;
     float c1, c2;  // Adam bias corrections of this step
+    uint32_t seed; // stochastic-rounding seed of this step (precision form)
     int view;
     int step;      // index into the schedule
 };
@@ -35,6 +36,7 @@ struct StepSchedule {
     const float* position_lr;   // [steps]
     const float* c1;            // [steps]
     const float* c2;            // [steps]
+    const uint32_t* seeds;      // [steps]
     int* cursor;                // next step; advanced by the frame kernel
     int* status;                // sticky GSN_ERR_CAPACITY: schedule, view index or records ran out
     const int* overflow;        // the renderer's record-overflow flag of the previous step
@@ -55,8 +57,9 @@ struct ProjectOutputs {
     float* radii;            // [N] optional 3-sigma pixel radius (0 = culled), may be null
 };
 // cam_dev (optional): device camera read instead of `cam` (batched form).
+// bf16_sh: precision-form parameter layout (10 fp32 rows + 48 bf16 SH rows).
 int launch_project(const float* params, int n, const gsn_camera& cam, const gsn_camera* cam_dev, int sh_degree,
-                   const ProjectOutputs& out, cudaStream_t stream);
+                   bool bf16_sh, const ProjectOutputs& out, cudaStream_t stream);
 
 // ---------------------------------------------------------------- sorting
 // Stable LSD radix sort of (uint32 key, uint32 value) pairs over key bits
@@ -159,13 +162,15 @@ struct GaussianUpdateArgs {
     float* abs_sums;
     unsigned int* obs_counts;
     float* grads_out;         // optional 58 x n mapped parameter gradients
-    const StepFrame* frame;   // optional: camera, lr[0], c1 and c2 come from the device frame
+    const StepFrame* frame;   // optional: camera, lr[0], c1, c2 and seed come from the device frame
+    bool bf16_sh;             // precision-form layout of params, m and v (10 fp32 + 48 bf16 rows)
+    uint32_t seed;            // stochastic-rounding seed of the step (precision form)
 };
 int launch_gaussian_update(const GaussianUpdateArgs& a, int sh_degree, cudaStream_t stream);
 
 // Adam history gather after densification: row r of the new moments takes the
 // parent's entry, or zero for parent -1 / out of range.
 int launch_remap_moments(const int* parents, const float* prev_m, const float* prev_v, float* m, float* v,
-                         int prev_count, int count, cudaStream_t stream);
+                         int prev_count, int count, bool bf16_sh, cudaStream_t stream);
 
 }  // namespace gsn

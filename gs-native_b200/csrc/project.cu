@@ -41,7 +41,8 @@ __device__ __forceinline__ void sh_basis(float x, float y, float z, float b[16])
     b[15] = -kSh3a * x * (xx - 3.0f * yy);
 }
 
-template <int D>
+// kBf16: precision form (bf16 SH rows; near-singular conics inverted in FP64).
+template <int D, bool kBf16>
 __global__ void __launch_bounds__(256) project_kernel(const float* __restrict__ params,
                                                       gsn_camera cam_arg, const gsn_camera* __restrict__ cam_dev,
                                                       int n, ProjectOutputs out) {
@@ -99,7 +100,20 @@ __global__ void __launch_bounds__(256) project_kernel(const float* __restrict__ 
     float b = JV[0] * J[3] + JV[1] * J[4] + JV[2] * J[5];
     float c = JV[3] * J[3] + JV[4] * J[4] + JV[5] * J[5] + kLowPass;
     float det = a * c - b * b;
-    if (!(det > 0.0f)) return;
+    // precision form: when a*c and b^2 agree in their leading 12 bits the fp32
+    // difference has lost them, so the determinant and the inverse are formed
+    // in FP64 (the only FP64 use of the projection)
+    bool singular64 = false;
+    double det64 = 0.0;
+    if constexpr (kBf16) {
+        if (det < 2.44140625e-4f * (a * c)) {
+            det64 = static_cast<double>(a) * c - static_cast<double>(b) * b;
+            if (!(det64 > 0.0)) return;
+            det = static_cast<float>(det64);
+            singular64 = true;
+        }
+    }
+    if (!(det > 0.0f) && !singular64) return;
     float mid = 0.5f * (a + c);
     float radius = ceilf(3.0f * sqrtf(mid + sqrtf(fmaxf(0.1f, mid * mid - det))));
     float u = cam.fx * px / z + cam.cx;
@@ -117,10 +131,16 @@ __global__ void __launch_bounds__(256) project_kernel(const float* __restrict__ 
     out.rects[i] = rect;
     out.tile_counts[i] = (rect.z - rect.x) * (rect.w - rect.y);
     if (out.radii) out.radii[i] = radius;
-    float det_inv = 1.0f / det;
     float opacity = 1.0f / (1.0f + expf(-__ldg(params + 9 * N + i)));
     out.means[i] = make_float2(u, v);
-    out.conic_opacity[i] = make_float4(c * det_inv, -b * det_inv, a * det_inv, opacity);
+    if (singular64) {
+        const double inv64 = 1.0 / det64;
+        out.conic_opacity[i] = make_float4(static_cast<float>(c * inv64), static_cast<float>(-b * inv64),
+                                           static_cast<float>(a * inv64), opacity);
+    } else {
+        float det_inv = 1.0f / det;
+        out.conic_opacity[i] = make_float4(c * det_inv, -b * det_inv, a * det_inv, opacity);
+    }
 
     // View direction from the camera centre, C = -R^T t.
     float dx = gx + R[0] * t[0] + R[3] * t[1] + R[6] * t[2];
@@ -133,27 +153,34 @@ __global__ void __launch_bounds__(256) project_kernel(const float* __restrict__ 
     float rgb[3];
 #pragma unroll
     for (int ch = 0; ch < 3; ++ch) {
-        const float* sh = params + (GSN_SH_INDEX + ch * kShStride) * N + i;
         float value = 0.0f;
 #pragma unroll
-        for (int k = 0; k < K; ++k) value += basis[k] * __ldg(sh + k * N);
+        for (int k = 0; k < K; ++k) value += basis[k] * load_sh<kBf16>(params, N, ch * kShStride + k, i);
         rgb[ch] = fmaxf(value + 0.5f, 0.0f);
     }
     out.colors[i] = make_float3(rgb[0], rgb[1], rgb[2]);
 }
 
+template <bool kBf16>
+void launch_project_layout(const float* params, int n, const gsn_camera& cam, const gsn_camera* cam_dev, int d,
+                           const ProjectOutputs& out, cudaStream_t stream) {
+    dim3 grid(ceil_div(n, 256));
+    switch (d) {
+        case 0: project_kernel<0, kBf16><<<grid, 256, 0, stream>>>(params, cam, cam_dev, n, out); break;
+        case 1: project_kernel<1, kBf16><<<grid, 256, 0, stream>>>(params, cam, cam_dev, n, out); break;
+        case 2: project_kernel<2, kBf16><<<grid, 256, 0, stream>>>(params, cam, cam_dev, n, out); break;
+        default: project_kernel<3, kBf16><<<grid, 256, 0, stream>>>(params, cam, cam_dev, n, out); break;
+    }
+}
+
 }  // namespace
 
 int launch_project(const float* params, int n, const gsn_camera& cam, const gsn_camera* cam_dev, int sh_degree,
-                   const ProjectOutputs& out, cudaStream_t stream) {
+                   bool bf16_sh, const ProjectOutputs& out, cudaStream_t stream) {
     if (n <= 0) return GSN_OK;
-    dim3 grid(ceil_div(n, 256));
-    switch (sh_degree < 0 ? 0 : (sh_degree > 3 ? 3 : sh_degree)) {
-        case 0: project_kernel<0><<<grid, 256, 0, stream>>>(params, cam, cam_dev, n, out); break;
-        case 1: project_kernel<1><<<grid, 256, 0, stream>>>(params, cam, cam_dev, n, out); break;
-        case 2: project_kernel<2><<<grid, 256, 0, stream>>>(params, cam, cam_dev, n, out); break;
-        default: project_kernel<3><<<grid, 256, 0, stream>>>(params, cam, cam_dev, n, out); break;
-    }
+    const int d = sh_degree < 0 ? 0 : (sh_degree > 3 ? 3 : sh_degree);
+    if (bf16_sh) launch_project_layout<true>(params, n, cam, cam_dev, d, out, stream);
+    else launch_project_layout<false>(params, n, cam, cam_dev, d, out, stream);
     return launched(1);
 }
 

@@ -94,6 +94,8 @@ def lib():
         "gsn_renderer_get_buffers": ([vp, P(RendererBuffers)], i32),
         "gsn_renderer_record_offsets": ([vp, P(vp)], i32),
         "gsn_renderer_set_record_capacity": ([vp, i64], i32),
+        "gsn_renderer_set_bf16_sh": ([vp, i32], i32),
+        "gsn_solver_set_bf16_sh": ([vp, i32], i32),
         "gsn_solver_create": ([P(vp)], i32),
         "gsn_solver_destroy": ([vp], i32),
         "gsn_solver_set_stream": ([vp, vp], i32),
@@ -167,6 +169,9 @@ class Renderer:
 
     def set_record_capacity(self, records):
         return lib().gsn_renderer_set_record_capacity(self.handle, int(records))
+
+    def set_bf16_sh(self, enabled=True):
+        _check(lib().gsn_renderer_set_bf16_sh(self.handle, int(bool(enabled))), "set_bf16_sh")
 
 
 def launch_count():
@@ -264,6 +269,9 @@ class Solver:
     def set_compute_loss(self, enabled=True):
         _check(lib().gsn_solver_set_compute_loss(self.handle, int(bool(enabled))), "set_compute_loss")
 
+    def set_bf16_sh(self, enabled=True):
+        _check(lib().gsn_solver_set_bf16_sh(self.handle, int(bool(enabled))), "set_bf16_sh")
+
     def loss(self):
         out = (ctypes.c_double * 4)()
         _check(lib().gsn_solver_loss(self.handle, out), "loss")
@@ -311,6 +319,7 @@ class Density:
             "gsn_density_reset_opacity": [vp, vp, i32, f32],
             "gsn_density_control": [vp, P(vp), P(i32), f32, f32, f32, f32, f32, ctypes.c_ulonglong, P(i32), f32],
             "gsn_density_buffers": [vp, P(vp), P(vp), P(vp)], "gsn_density_set_max_gaussians": [vp, i32],
+            "gsn_density_set_bf16_sh": [vp, i32],
             "gsn_density_internals": [vp, P(vp), P(vp), P(vp), P(vp)],
         }
         for name, args in sigs.items():
@@ -370,6 +379,9 @@ class Density:
     def set_max_gaussians(self, n):
         _check(lib().gsn_density_set_max_gaussians(self.handle, int(n)), "set_max_gaussians")
 
+    def set_bf16_sh(self, enabled=True):
+        _check(lib().gsn_density_set_bf16_sh(self.handle, int(bool(enabled))), "set_bf16_sh")
+
     def internals(self):
         ps = [ctypes.c_void_p() for _ in range(4)]
         _check(lib().gsn_density_internals(self.handle, *[ctypes.byref(p) for p in ps]), "internals")
@@ -408,6 +420,7 @@ class TrainingOptions(ctypes.Structure):
         ("opacity_reset_interval", ctypes.c_int), ("opacity_reset", ctypes.c_float),
         ("background", ctypes.c_float * 3), ("max_gaussians", ctypes.c_int),
         ("density_seed", ctypes.c_ulonglong), ("initial_opacity", ctypes.c_float),
+        ("precision", ctypes.c_int), ("graph", ctypes.c_int),
     ]
 
     @classmethod
@@ -590,3 +603,22 @@ class Graph:
         out = ctypes.c_int()
         _check(lib().gsn_graph_launches_per_step(self.handle, ctypes.byref(out)), "launches_per_step")
         return out.value
+
+
+def to_precision_layout(params, torch):
+    """58 x N fp32 parameter block (numpy or torch) -> the precision-form device
+    block: 10 fp32 geometry rows, then the 48 SH rows as bf16 (34 float rows)."""
+    p = torch.as_tensor(params).cuda().float()
+    n = p.shape[1]
+    block = torch.empty(34 * n, dtype=torch.float32, device="cuda")
+    block[:10 * n] = p[:10].reshape(-1)
+    block[10 * n:].view(torch.bfloat16)[:] = p[10:].reshape(-1).to(torch.bfloat16)
+    return block
+
+
+def from_precision_layout(block, n, torch):
+    """Inverse of to_precision_layout: a 58 x N fp32 tensor (SH widened)."""
+    out = torch.empty((58, n), dtype=torch.float32, device=block.device)
+    out[:10] = block[:10 * n].reshape(10, n)
+    out[10:] = block[10 * n:34 * n].view(torch.bfloat16).reshape(48, n).float()
+    return out

@@ -166,7 +166,8 @@ bool DensityController::ControlDensity(GaussianBuffers& gaussians, float scene_e
         spare_gaussian_stride_ = 0;
     } else if (!spare_gaussian_parameters_ || next_stride > spare_gaussian_stride_) {
         void* replacement = nullptr;
-        if (DeviceAlloc(&replacement, sizeof(float) * kMaxParamCount * static_cast<size_t>(next_stride)) != cudaSuccess)
+        const size_t rows = bf16_sh_ ? 34 : kMaxParamCount;
+        if (DeviceAlloc(&replacement, sizeof(float) * rows * static_cast<size_t>(next_stride)) != cudaSuccess)
             return false;
         cudaFree(spare_gaussian_parameters_);
         spare_gaussian_parameters_ = static_cast<float*>(replacement);
@@ -204,6 +205,7 @@ bool DensityController::ControlDensity(GaussianBuffers& gaussians, float scene_e
     a.out_stride = spare_gaussian_stride_;
     a.random_blocks = random_blocks_;
     a.seed = seed;
+    a.bf16_sh = bf16_sh_;
     if (gsn::launch_density_apply(a, stream_) != GSN_OK) return false;
     gsn::stage_mark(stream_, gsn::kStageOther);
     parameter_stride_ = next_stride;

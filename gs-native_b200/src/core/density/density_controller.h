@@ -53,6 +53,9 @@ public:
     void SetStream(cudaStream_t stream) { stream_ = stream; }
     // 0 = unlimited (reference behaviour).
     void SetMaxGaussians(int max_gaussians) { max_gaussians_ = max_gaussians < 0 ? 0 : max_gaussians; }
+    // Precision form: parameter blocks in the 10 fp32 + 48 bf16 row layout
+    // (34 float rows of stride N); set before the first ControlDensity.
+    void SetBf16Sh(bool enabled) { bf16_sh_ = enabled; }
     const float* GetNewFlags() const { return new_flags_.get(); }
     float* GetGradientSums() { return gradient_sums_.get(); }
     float* GetAbsoluteGradientSums() { return absolute_gradient_sums_.get(); }
@@ -85,6 +88,7 @@ private:
     int parameter_stride_ = 0;
     int random_blocks_ = 0;
     int max_gaussians_ = 0;
+    bool bf16_sh_ = false;
     unsigned long long seed_ = 0;
 };
 

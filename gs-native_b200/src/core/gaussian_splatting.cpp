@@ -4,6 +4,8 @@
 
 #include <algorithm>
 #include <array>
+#include <climits>
+#include <cstring>
 #include <cmath>
 #include <limits>
 #include <numeric>
@@ -14,10 +16,14 @@
 
 namespace gs_native {
 
-GaussianSplatting::~GaussianSplatting() { cudaFree(gaussians_.gaussians_); }
+GaussianSplatting::~GaussianSplatting() {
+    graph_.Release();
+    cudaFree(gaussians_.gaussians_);
+}
 
 void GaussianSplatting::SetStream(cudaStream_t stream) {
     stream_ = stream;
+    graph_.Release();
     renderer_.SetStream(stream);
     solver_.SetStream(stream);
     density_.SetStream(stream);
@@ -80,6 +86,11 @@ bool GaussianSplatting::Initialize(const TrainingScene& scene, const TrainingOpt
     sh_degree_ = 0;
     solver_.SetLearningRates(options_.lr);
     density_.SetMaxGaussians(options_.max_gaussians);
+    renderer_.SetBf16Sh(options_.bf16_sh);
+    eval_renderer_.SetBf16Sh(options_.bf16_sh);
+    solver_.SetBf16Sh(options_.bf16_sh);
+    density_.SetBf16Sh(options_.bf16_sh);
+    graph_.Release();
     if (!InitializeGaussians(scene.point_positions, scene.point_colors, scene.point_count)) return false;
     return cudaStreamSynchronize(stream_) == cudaSuccess;
 }
@@ -99,31 +110,134 @@ bool GaussianSplatting::InitializeGaussians(const float* positions, const float*
         }
         p[kOpacityIndex * N + i] = logit;
     }
-    void* block = nullptr;
-    if (DeviceAlloc(&block, p.size() * sizeof(float)) != cudaSuccess) return false;
-    if (cudaMemcpy(block, p.data(), p.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess ||
+    return SetParameters(p.data(), count);
+}
+
+namespace {
+
+// bf16 bits of x, round to nearest even (host side of the precision layout).
+uint16_t ToBf16(float x) {
+    uint32_t u;
+    std::memcpy(&u, &x, sizeof(u));
+    if ((u & 0x7f800000u) == 0x7f800000u) return static_cast<uint16_t>(u >> 16 | ((u & 0xffffu) ? 0x40u : 0u));
+    u += 0x7fffu + ((u >> 16) & 1u);
+    return static_cast<uint16_t>(u >> 16);
+}
+
+float FromBf16(uint16_t b) {
+    uint32_t u = static_cast<uint32_t>(b) << 16;
+    float x;
+    std::memcpy(&x, &u, sizeof(x));
+    return x;
+}
+
+constexpr size_t kGeometryRows = kShIndex;  // 10 fp32 rows, then 48 bf16 SH rows
+
+}  // namespace
+
+size_t GaussianSplatting::PhysicalRows() const { return options_.bf16_sh ? kGeometryRows + 24 : kMaxParamCount; }
+
+bool GaussianSplatting::SetParameters(const float* host_params, int count) {
+    const size_t N = static_cast<size_t>(count);
+    std::vector<float> block(PhysicalRows() * N);
+    if (options_.bf16_sh) {
+        std::memcpy(block.data(), host_params, kGeometryRows * N * sizeof(float));
+        auto* sh = reinterpret_cast<uint16_t*>(block.data() + kGeometryRows * N);
+        for (size_t k = 0; k < kMaxParamCount - kGeometryRows; ++k)
+            for (size_t i = 0; i < N; ++i) sh[k * N + i] = ToBf16(host_params[(kGeometryRows + k) * N + i]);
+    } else {
+        std::memcpy(block.data(), host_params, block.size() * sizeof(float));
+    }
+    void* dev = nullptr;
+    if (DeviceAlloc(&dev, block.size() * sizeof(float)) != cudaSuccess) return false;
+    if (cudaMemcpy(dev, block.data(), block.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess ||
         !density_.Initialize(count, count) || !solver_.RemapGaussians(nullptr, count)) {
-        cudaFree(block);
+        cudaFree(dev);
         return false;
     }
+    graph_.Release();
     cudaFree(gaussians_.gaussians_);
-    gaussians_.gaussians_ = static_cast<float*>(block);
+    gaussians_.gaussians_ = static_cast<float*>(dev);
     gaussians_.gaussian_count_ = count;
+    return true;
+}
+
+bool GaussianSplatting::GetParameters(std::vector<float>& out) const {
+    const size_t N = static_cast<size_t>(gaussians_.gaussian_count_);
+    std::vector<float> block(PhysicalRows() * N);
+    if (cudaMemcpy(block.data(), gaussians_.gaussians_, block.size() * sizeof(float), cudaMemcpyDeviceToHost) !=
+        cudaSuccess)
+        return false;
+    if (!options_.bf16_sh) {
+        out = std::move(block);
+        return true;
+    }
+    out.assign(kMaxParamCount * N, 0.0f);
+    std::memcpy(out.data(), block.data(), kGeometryRows * N * sizeof(float));
+    const auto* sh = reinterpret_cast<const uint16_t*>(block.data() + kGeometryRows * N);
+    for (size_t k = 0; k < kMaxParamCount - kGeometryRows; ++k)
+        for (size_t i = 0; i < N; ++i) out[(kGeometryRows + k) * N + i] = FromBf16(sh[k * N + i]);
     return true;
 }
 
 bool GaussianSplatting::Train(int iterations) {
     if (iterations < 0 || !gaussians_.gaussians_ || cameras_.empty()) return false;
-    std::mt19937 generator(0);
+    generator_.seed(0);
     for (int it = 0; it < iterations; ++it) {
         if (gaussians_.gaussian_count_ == 0) return false;
-        if (camera_cursor_ >= static_cast<int>(camera_order_.size())) {
-            std::shuffle(camera_order_.begin(), camera_order_.end(), generator);
-            camera_cursor_ = 0;
+        const int next = completed_ + 1;
+        if (options_.graph && completed_ >= options_.densify_until &&
+            std::min(options_.max_sh_degree, next / options_.sh_degree_interval) == options_.max_sh_degree &&
+            next / options_.sh_degree_interval >= options_.max_sh_degree) {
+            if (!GraphSteps(iterations - it)) return false;
+            break;
         }
+        NextCamera();
         if (!Step()) return false;
     }
     return cudaStreamSynchronize(stream_) == cudaSuccess;
+}
+
+void GaussianSplatting::NextCamera() {
+    if (camera_cursor_ >= static_cast<int>(camera_order_.size())) {
+        std::shuffle(camera_order_.begin(), camera_order_.end(), generator_);
+        camera_cursor_ = 0;
+    }
+}
+
+float GaussianSplatting::PositionLearningRate(int next) const {
+    const float fraction = std::min(1.0f, static_cast<float>(next) / static_cast<float>(options_.position_lr_steps));
+    return scene_extent_ * std::exp(std::log(options_.position_lr_init) * (1.0f - fraction) +
+                                    std::log(options_.position_lr_final) * fraction);
+}
+
+bool GaussianSplatting::GraphSteps(int iterations) {
+    sh_degree_ = options_.max_sh_degree;
+    if (!graph_.Captured()) {
+        // twice the largest record buffer the eager steps needed
+        const int64_t capacity = std::min<int64_t>(std::max<int64_t>(renderer_.GetRecordCapacity(), 1 << 20) * 2,
+                                                   INT_MAX / 2);
+        solver_.SetDensityAccumulators(nullptr, nullptr, nullptr);
+        if (!graph_.Capture(renderer_, solver_, gaussians_, cameras_, targets_.get(), target_stride_,
+                            options_.background, image_.get(), sh_degree_, capacity, stream_))
+            return false;
+    }
+    std::vector<int> views;
+    std::vector<float> lrs;
+    for (int done = 0; done < iterations;) {
+        const int n = std::min(iterations - done, 4096);
+        views.resize(n);
+        lrs.resize(n);
+        for (int k = 0; k < n; ++k) {
+            NextCamera();
+            views[k] = camera_order_[camera_cursor_++];
+            lrs[k] = PositionLearningRate(completed_ + k + 1);
+        }
+        if (!graph_.Run(views.data(), lrs.data(), n)) return false;
+        completed_ += n;
+        done += n;
+    }
+    return graph_.Check() == GSN_OK;
 }
 
 bool GaussianSplatting::Step() {
@@ -131,9 +245,7 @@ bool GaussianSplatting::Step() {
     const CameraParams& camera = cameras_[index];
     const int next = completed_ + 1;
     sh_degree_ = std::min(options_.max_sh_degree, next / options_.sh_degree_interval);
-    const float fraction = std::min(1.0f, static_cast<float>(next) / static_cast<float>(options_.position_lr_steps));
-    const float lr = scene_extent_ * std::exp(std::log(options_.position_lr_init) * (1.0f - fraction) +
-                                              std::log(options_.position_lr_final) * fraction);
+    const float lr = PositionLearningRate(next);
     const uint8_t* target = targets_.get() + static_cast<size_t>(index) * target_stride_;
     if (!renderer_.Render(gaussians_, camera, options_.background, image_.get(), sh_degree_)) return false;
     const bool accumulate = next < options_.densify_until;
@@ -170,7 +282,9 @@ bool GaussianSplatting::ControlDensity() {
 
 bool GaussianSplatting::Render(const CameraParams& camera, float* device_image) {
     if (!gaussians_.gaussians_ || !device_image) return false;
-    return renderer_.Render(gaussians_, camera, options_.background, device_image, sh_degree_);
+    // a renderer of its own: the training renderer's buffers may be bound to a graph
+    eval_renderer_.SetStream(stream_);
+    return eval_renderer_.Render(gaussians_, camera, options_.background, device_image, sh_degree_);
 }
 
 bool GaussianSplatting::Evaluate(const std::vector<CameraParams>& cameras, const std::vector<const uint8_t*>& images,
@@ -205,9 +319,8 @@ bool GaussianSplatting::Evaluate(const std::vector<CameraParams>& cameras, const
 bool GaussianSplatting::Save(const std::string& path) {
     const int count = gaussians_.gaussian_count_;
     if (count <= 0 || !gaussians_.gaussians_) return false;
-    std::vector<float> p(static_cast<size_t>(count) * kMaxParamCount);
-    if (cudaMemcpy(p.data(), gaussians_.gaussians_, p.size() * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
-        return false;
+    std::vector<float> p;
+    if (!GetParameters(p)) return false;
     return WriteGaussiansPly(path, UnpackGaussians(p.data(), count));
 }
 
@@ -215,18 +328,7 @@ bool GaussianSplatting::Load(const std::string& path) {
     std::vector<Gaussian> g;
     if (!ReadGaussiansPly(path, g)) return false;
     std::vector<float> p = PackGaussians(g);
-    const int count = static_cast<int>(g.size());
-    void* block = nullptr;
-    if (DeviceAlloc(&block, p.size() * sizeof(float)) != cudaSuccess) return false;
-    if (cudaMemcpy(block, p.data(), p.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess ||
-        !density_.Initialize(count, count) || !solver_.RemapGaussians(nullptr, count)) {
-        cudaFree(block);
-        return false;
-    }
-    cudaFree(gaussians_.gaussians_);
-    gaussians_.gaussians_ = static_cast<float*>(block);
-    gaussians_.gaussian_count_ = count;
-    return true;
+    return SetParameters(p.data(), static_cast<int>(g.size()));
 }
 
 }  // namespace gs_native

@@ -18,10 +18,12 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <random>
 #include <string>
 #include <vector>
 
 #include "core/density/density_controller.h"
+#include "core/graph/training_graph.h"
 #include "core/render/renderer.h"
 #include "core/solver/solver.h"
 #include "core/types/buffers.h"
@@ -60,6 +62,9 @@ struct TrainingOptions {
     int max_gaussians = 0;  // 0 = unlimited (reference behaviour)
     unsigned long long density_seed = 0;
     float initial_opacity = 0.1f;  // initial opacity logit log(o / (1 - o))
+    // gs-native extensions
+    bool bf16_sh = false;  // precision form: SH rows and their moments in bf16 (34-row block)
+    bool graph = false;    // steady-state iterations (after densify_until) as CUDA-graph replays
 };
 
 class GaussianSplatting {
@@ -94,8 +99,18 @@ public:
 
 private:
     bool InitializeGaussians(const float* positions, const float* colors, int count);
+    // Uploads a host 58 x count fp32 block in the active layout (bf16 SH rows
+    // for the precision form) and resets the optimiser and density state.
+    bool SetParameters(const float* host_params, int count);
+    // The parameters as a host 58 x count fp32 block (bf16 SH rows widened).
+    bool GetParameters(std::vector<float>& out) const;
+    size_t PhysicalRows() const;
     bool ControlDensity();
     bool Step();
+    void NextCamera();
+    // Runs `iterations` steady-state steps as graph replays (after densify_until).
+    bool GraphSteps(int iterations);
+    float PositionLearningRate(int iteration) const;
 
     cudaStream_t stream_ = nullptr;
     TrainingOptions options_;
@@ -104,6 +119,7 @@ private:
     size_t target_stride_ = 0;  // bytes per resident training image
     GaussianBuffers gaussians_;
     Renderer renderer_;
+    Renderer eval_renderer_;  // Render / Evaluate (the training renderer may be bound to a graph)
     Solver solver_;
     DensityController density_;
     DeviceArray<float> image_;
@@ -113,6 +129,8 @@ private:
     int completed_ = 0;
     int sh_degree_ = 0;
     float scene_extent_ = 0.0f;
+    TrainingGraph graph_;
+    std::mt19937 generator_;
 };
 
 }  // namespace gs_native

@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 
 #include "kernels.h"
 #include "profile.h"
@@ -47,7 +48,7 @@ bool TrainingGraph::Capture(Renderer& renderer, Solver& solver, GaussianBuffers&
     view_count_ = static_cast<int>(cameras.size());
     batch_capacity_ = kBatchCapacity;
     if (!cameras_.Reserve(cameras.size()) || !views_.Reserve(batch_capacity_) ||
-        !schedule_.Reserve(3 * static_cast<size_t>(batch_capacity_)) || !control_.Reserve(2) ||
+        !schedule_.Reserve(4 * static_cast<size_t>(batch_capacity_)) || !control_.Reserve(2) ||
         !frame_.Reserve(sizeof(gsn::StepFrame)))
         return false;
     std::vector<gsn_camera> cams(cameras.size());
@@ -56,7 +57,7 @@ bool TrainingGraph::Capture(Renderer& renderer, Solver& solver, GaussianBuffers&
                         stream) != cudaSuccess ||
         cudaMemsetAsync(control_.get(), 0, 2 * sizeof(int), stream) != cudaSuccess ||
         cudaMemsetAsync(views_.get(), 0, batch_capacity_ * sizeof(int), stream) != cudaSuccess ||
-        cudaMemsetAsync(schedule_.get(), 0, 3 * batch_capacity_ * sizeof(float), stream) != cudaSuccess)
+        cudaMemsetAsync(schedule_.get(), 0, 4 * batch_capacity_ * sizeof(float), stream) != cudaSuccess)
         return false;
 
     renderer.SetStream(stream);
@@ -79,6 +80,7 @@ bool TrainingGraph::Capture(Renderer& renderer, Solver& solver, GaussianBuffers&
     s.position_lr = schedule_.get();
     s.c1 = schedule_.get() + batch_capacity_;
     s.c2 = schedule_.get() + 2 * batch_capacity_;
+    s.seeds = reinterpret_cast<const uint32_t*>(schedule_.get() + 3 * batch_capacity_);
     s.cursor = control_.get();
     s.status = control_.get() + 1;
     s.overflow = renderer.GetOverflowFlag();
@@ -133,13 +135,16 @@ bool TrainingGraph::Run(const int* views, const float* position_lrs, int steps) 
         for (int k = 0; k < n; ++k)
             if (views[done + k] < 0 || views[done + k] >= view_count_) return false;
         // c1, c2 exactly as Solver::UpdateGaussians computes them (FP64 on the host)
-        host_schedule_.assign(3 * static_cast<size_t>(n), 0.0f);
+        host_schedule_.assign(4 * static_cast<size_t>(n), 0.0f);
         const uint64_t t0 = solver_->GetIteration();
         for (int k = 0; k < n; ++k) {
             const double t = static_cast<double>(t0 + k + 1);
             host_schedule_[k] = position_lrs[done + k];
             host_schedule_[n + k] = static_cast<float>(1.0 / (1.0 - std::pow(0.9, t)));
             host_schedule_[2 * n + k] = static_cast<float>(1.0 / (1.0 - std::pow(0.999, t)));
+            // the seed is the Adam step number, as in the eager update
+            const uint32_t seed = static_cast<uint32_t>(t0 + k + 1);
+            std::memcpy(&host_schedule_[3 * n + k], &seed, sizeof(seed));
         }
         float* dev = schedule_.get();
         if (cudaMemcpyAsync(views_.get(), views + done, n * sizeof(int), cudaMemcpyHostToDevice, stream_) !=
@@ -149,6 +154,8 @@ bool TrainingGraph::Run(const int* views, const float* position_lrs, int steps) 
             cudaMemcpyAsync(dev + batch_capacity_, host_schedule_.data() + n, n * sizeof(float),
                             cudaMemcpyHostToDevice, stream_) != cudaSuccess ||
             cudaMemcpyAsync(dev + 2 * batch_capacity_, host_schedule_.data() + 2 * n, n * sizeof(float),
+                            cudaMemcpyHostToDevice, stream_) != cudaSuccess ||
+            cudaMemcpyAsync(dev + 3 * batch_capacity_, host_schedule_.data() + 3 * n, n * sizeof(float),
                             cudaMemcpyHostToDevice, stream_) != cudaSuccess ||
             cudaMemsetAsync(control_.get(), 0, sizeof(int), stream_) != cudaSuccess)
             return false;

@@ -71,7 +71,7 @@ private:
     int batch_capacity_ = 0;
     DeviceArray<gsn_camera> cameras_;
     DeviceArray<int> views_;
-    DeviceArray<float> schedule_;    // position lr, c1, c2 planes of batch_capacity_
+    DeviceArray<float> schedule_;    // position lr, c1, c2, seed planes of batch_capacity_
     DeviceArray<int> control_;       // [0] cursor, [1] status
     DeviceArray<unsigned char> frame_;
     std::vector<float> host_schedule_;

@@ -114,7 +114,7 @@ bool Renderer::Render(const GaussianBuffers& gaussians, const CameraParams& came
         gsn::ProjectOutputs po{means_.get(), conic_opacities_.get(), colors_.get(), depths_.get(),
                                rects_.get(), tile_counts_.get(), depth_keys_[0].get(), radii_.get()};
         gsn::stage_mark(s, gsn::kStageProject);
-        if (gsn::launch_project(gaussians.gaussians_, count, cam, device_camera_, sh_degree, po, s) != GSN_OK) return false;
+        if (gsn::launch_project(gaussians.gaussians_, count, cam, device_camera_, sh_degree, bf16_sh_, po, s) != GSN_OK) return false;
         gsn::stage_mark(s, gsn::kStageDepthSort);
         gsn::RadixSortScratch scratch = gsn::radix_sort_scratch(sort_scratch_.get(), sort_max);
         bool in_alt = false;

@@ -56,6 +56,10 @@ public:
     // step frame) instead of the host camera; the host camera still fixes the
     // resolution and tile grid. nullptr restores the host camera.
     void SetDeviceCamera(const gsn_camera* camera) { device_camera_ = camera; }
+    // Precision form: the parameter block holds 10 fp32 geometry rows followed
+    // by the 48 SH rows in bf16 (34 float rows of stride N).
+    void SetBf16Sh(bool enabled) { bf16_sh_ = enabled; }
+    bool GetBf16Sh() const { return bf16_sh_; }
     const int* GetTileCounts() const { return tile_counts_.get(); }
     const int4* GetTileRects() const { return rects_.get(); }
     const float* GetDepths() const { return depths_.get(); }
@@ -78,6 +82,7 @@ private:
     int64_t record_capacity_ = 0;
     bool fixed_capacity_ = false;
     const gsn_camera* device_camera_ = nullptr;
+    bool bf16_sh_ = false;
     int64_t last_records_ = 0;
     int last_count_ = 0;
 

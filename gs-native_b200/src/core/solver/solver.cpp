@@ -12,6 +12,21 @@ namespace gs_native {
 
 Solver::~Solver() = default;
 
+namespace {
+
+size_t PhysicalRows(bool bf16_sh) { return bf16_sh ? 34 : kMaxParamCount; }
+
+}  // namespace
+
+void Solver::SetBf16Sh(bool enabled) {
+    if (enabled == bf16_sh_) return;
+    bf16_sh_ = enabled;
+    m_.Reset();
+    v_.Reset();
+    gaussian_count_ = 0;
+    iteration_ = 0;
+}
+
 bool Solver::Iterate(const CameraParams& camera, const Renderer& renderer, const float* image, const uint8_t* target,
                      GaussianBuffers& gaussians, float position_learning_rate, int sh_degree) {
     if (!ComputeImageGradients(camera, image, target)) return false;
@@ -42,9 +57,9 @@ bool Solver::RemapGaussians(const int* parent_ids, int gaussian_count) {
         per_gaussian_capacity_ = n;
     }
     DeviceArray<float> m, v;
-    if (!m.Reserve(n * kMaxParamCount) || !v.Reserve(n * kMaxParamCount)) return false;
+    if (!m.Reserve(n * PhysicalRows(bf16_sh_)) || !v.Reserve(n * PhysicalRows(bf16_sh_))) return false;
     if (gsn::launch_remap_moments(parent_ids, m_.get(), v_.get(), m.get(), v.get(), m_.get() ? gaussian_count_ : 0,
-                                  gaussian_count, stream_) != GSN_OK)
+                                  gaussian_count, bf16_sh_, stream_) != GSN_OK)
         return false;
     if (cudaStreamSynchronize(stream_) != cudaSuccess) return false;
     m_ = std::move(m);
@@ -139,6 +154,8 @@ bool Solver::UpdateGaussians(const CameraParams& camera, const Renderer& rendere
     }
     a.grads_out = grads_out;
     a.frame = frame_;
+    a.bf16_sh = bf16_sh_;
+    a.seed = static_cast<uint32_t>(iteration);
     gsn::stage_mark(stream_, gsn::kStageGaussianUpdate);
     if (gsn::launch_gaussian_update(a, std::clamp(sh_degree, 0, 3), stream_) != GSN_OK) return false;
     gsn::stage_mark(stream_, gsn::kStageOther);

@@ -82,6 +82,11 @@ public:
     // position learning rate and Adam's bias corrections are read from this
     // device frame (written on the device at the start of each step).
     void SetStepFrame(const gsn::StepFrame* frame) { frame_ = frame; }
+    // Precision form: parameters and moments in the 10 fp32 + 48 bf16 row
+    // layout (34 float rows of stride N); SH updates use stochastic rounding.
+    // Changing the layout drops the Adam history.
+    void SetBf16Sh(bool enabled);
+    bool GetBf16Sh() const { return bf16_sh_; }
     void SetIteration(uint64_t iteration) { iteration_ = iteration; }
 
     // Stage entry points (used by Iterate and by the C ABI).
@@ -111,6 +116,7 @@ private:
     float* acc_abs_ = nullptr;
     unsigned int* acc_count_ = nullptr;
     const gsn::StepFrame* frame_ = nullptr;
+    bool bf16_sh_ = false;
 };
 
 }  // namespace gs_native

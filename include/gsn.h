@@ -156,6 +156,12 @@ int gsn_renderer_record_offsets(gsn_renderer* r, const int** out);
 
 /* Fixed record capacity (0 = grow on demand, the reference behaviour). */
 int gsn_renderer_set_record_capacity(gsn_renderer* r, int64_t records);
+/* Precision form (gs-native extension): `enabled` selects the parameter layout
+ * of 10 fp32 geometry rows followed by the 48 SH rows in bf16 (34 float rows
+ * of stride count). The same switch exists on the solver (parameters and Adam
+ * moments; SH updates use stochastic rounding; switching drops the history)
+ * and on the density controller. */
+int gsn_renderer_set_bf16_sh(gsn_renderer* r, int enabled);
 
 
 /* ------------------------------------------------------------------ solver
@@ -195,6 +201,7 @@ int gsn_solver_set_learning_rates(gsn_solver* s, float scale, float rotation, fl
 /* Enables the FP64 loss reduction; gsn_solver_loss then copies
  * [loss, mean L1, mean SSIM, PSNR dB] of the last iterate to `out` (host). */
 int gsn_solver_set_compute_loss(gsn_solver* s, int enabled);
+int gsn_solver_set_bf16_sh(gsn_solver* s, int enabled);
 int gsn_solver_loss(gsn_solver* s, double* out);
 int gsn_solver_loss_device(gsn_solver* s, const double** out);
 
@@ -253,6 +260,7 @@ int gsn_density_buffers(gsn_density* d, const int** history_parent_ids, const in
 /* Cap on the Gaussian count (0 = unlimited, the reference behaviour): additions
  * beyond the cap are dropped in id order. */
 int gsn_density_set_max_gaussians(gsn_density* d, int max_gaussians);
+int gsn_density_set_bf16_sh(gsn_density* d, int enabled);
 
 /* The normal samples of the last ControlDensity (device float[6 * sampled]) and
  * the accumulated statistics (device float[capacity] x2, uint[capacity]). */
@@ -290,6 +298,9 @@ typedef struct gsn_training_options {
     int max_gaussians;               /* 0 = unlimited */
     unsigned long long density_seed; /* 0 */
     float initial_opacity;           /* 0.1 */
+    /* gs-native extensions (0 = reference behaviour) */
+    int precision;                   /* 1: precision form - SH and its Adam moments stored in bf16 */
+    int graph;                       /* 1: iterations after densify_until run as CUDA-graph replays */
 } gsn_training_options;
 
 int gsn_training_options_default(gsn_training_options* out);

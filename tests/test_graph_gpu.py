@@ -28,6 +28,7 @@ def views_scene(n=20000, views=4):
         assert r.render(hp.data_ptr(), n, c, [0, 0, 0], img.data_ptr(), 3) == 0
         targets[k] = (img * 255.0).round().clamp(0, 255).to(t.uint8)
     sync()
+    views_scene.hidden = hidden
     return cams, model, targets
 
 
@@ -106,3 +107,28 @@ def test_graph_rejects_mixed_resolutions_and_bad_views():
         g.run([0, 2], [1e-4, 1e-4])  # view 2 does not exist
     assert g.check() == 0
     g.close()
+
+
+def test_trainer_graph_steady_state_trains_like_eager():
+    """Iterations after densify_until run as graph replays in the trainer; with
+    the same schedule (camera order, learning rates) the result matches the
+    eager trainer up to the backward's atomic summation order. (Float-atomic
+    reordering makes any two runs drift apart slowly, so the replayed span is
+    kept to 60 steps.)"""
+    cams, _, targets = views_scene(n=20000, views=6)
+    hidden = views_scene.hidden
+    imgs = [targets[k].cpu().numpy() for k in range(6)]
+    points, colors = scenes.initial_points(hidden, 4000, 5)
+    out = {}
+    for graph in (0, 1):
+        opts = gsn.TrainingOptions.defaults(densify_from=100, densify_until=400, densify_interval=100,
+                                            sh_degree_interval=100, opacity_reset_interval=100000, graph=graph)
+        tr = gsn.Trainer()
+        assert tr.initialize(cams, imgs, points, colors, opts) == 0
+        assert tr.train(460) == 0
+        psnr, loss = tr.evaluate(cams, imgs)
+        st = tr.state()
+        out[graph] = (psnr, loss, st["count"], st["completed"])
+        tr.close()
+    assert out[0][2] == out[1][2] and out[0][3] == out[1][3] == 460
+    assert abs(out[0][0] - out[1][0]) < 0.05, out
