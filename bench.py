@@ -13,11 +13,14 @@ means N(0, 3^2)); 200 cameras on a ring of radius 8 at elevation +/-15 deg,
 hidden model and quantised to u8. The model being optimised is a 1.2M-Gaussian
 draw of the same distribution (seed 8).
 
-Two forms of the same iteration are timed: `plain_fp32` (eager launches from
-the host) and `graph_fp32` (the iteration captured once as a CUDA graph over a
-fixed record capacity and replayed from a device schedule of views). `value`
-is the faster form that completed without a record overflow; both are in
-`forms`.
+Four forms of the same iteration are timed, each from the same initial model:
+`plain_fp32` (eager launches from the host, the reference-parity form),
+`graph_fp32` (the iteration captured once as a CUDA graph over a fixed record
+capacity and replayed from a device schedule of views), and `precision_bf16` /
+`precision_bf16_graph` (SH rows and their Adam moments stored in bf16 with
+stochastic rounding; fp32 blending and accumulation). `value` is the fastest
+form that completed without a record overflow; all are in `forms`, with
+`chosen_over_plain` the ratio to the plain form.
 
 Printed JSON line: `value` is iterations/s with targets resident in HBM,
 `e2e` the same through host buffers (pinned H2D target upload and a D2H loss
@@ -247,141 +250,153 @@ def run_gsn(args):
     stream = torch.cuda.current_stream()
     sp = stream.cuda_stream
 
-    renderer = gsn.Renderer()
-    solver = gsn.Solver()
-    renderer.set_stream(sp)
-    solver.set_stream(sp)
     # hidden-model targets, resident in HBM and in pinned host memory
     tm = torch.from_numpy(target_model).cuda()
     img = torch.empty((1064, 1600, 3), device="cuda")
     targets = torch.empty((len(train), 1064, 1600, 3), dtype=torch.uint8, device="cuda")
+    maker = gsn.Renderer()
     for k, cam in enumerate(train):
-        assert renderer.render(tm.data_ptr(), tm.shape[1], cam, [0, 0, 0], img.data_ptr(), SH_DEGREE) == 0
+        assert maker.render(tm.data_ptr(), tm.shape[1], cam, [0, 0, 0], img.data_ptr(), SH_DEGREE) == 0
         targets[k] = (img * 255.0).round().clamp(0, 255).to(torch.uint8)
-    del tm
+    del tm, maker
     host_targets = targets.cpu().pin_memory()
     staging = torch.empty((1064, 1600, 3), dtype=torch.uint8, device="cuda")
-    params = torch.from_numpy(model).cuda()
     lr = position_lr(15000, extent)
     loss_host = torch.zeros(4, dtype=torch.float64).pin_memory()
 
-    def step(k, e2e=False):
+    class Form:
+        """One form of the iteration: its own renderer, solver and parameter block."""
+
+        def __init__(self, bf16):
+            self.renderer, self.solver = gsn.Renderer(), gsn.Solver()
+            self.renderer.set_stream(sp)
+            self.solver.set_stream(sp)
+            if bf16:
+                self.renderer.set_bf16_sh(True)
+                self.solver.set_bf16_sh(True)
+                self.params = gsn.to_precision_layout(model, torch)
+            else:
+                self.params = torch.from_numpy(model).cuda()
+
+    def step(f, k, e2e=False):
         cam = train[k % len(train)]
         if e2e:
             staging.copy_(host_targets[k % len(train)], non_blocking=True)
             tgt = staging
         else:
             tgt = targets[k % len(train)]
-        assert renderer.render(params.data_ptr(), n, cam, [0, 0, 0], img.data_ptr(), SH_DEGREE) == 0
-        assert solver.iterate(cam, renderer, img.data_ptr(), tgt.data_ptr(), params.data_ptr(), n, lr,
-                              SH_DEGREE) == 0
+        assert f.renderer.render(f.params.data_ptr(), n, cam, [0, 0, 0], img.data_ptr(), SH_DEGREE) == 0
+        assert f.solver.iterate(cam, f.renderer, img.data_ptr(), tgt.data_ptr(), f.params.data_ptr(), n, lr,
+                                SH_DEGREE) == 0
         if e2e:
-            gsn.memcpy_async(loss_host.data_ptr(), solver.loss_device(), 32, sp)
+            gsn.memcpy_async(loss_host.data_ptr(), f.solver.loss_device(), 32, sp)
             stream.synchronize()
 
     def barrier():
         if dist is not None:
             dist.barrier()
 
-    def timed(k0, steps, e2e=False):
+    def max_over_ranks(ms):
+        if dist is not None:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    def timed(run, steps):
         barrier()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         launches0 = gsn.launch_count()
         e0.record(stream)
-        for k in range(steps):
-            step(k0 + k, e2e)
+        run(steps)
         e1.record(stream)
         torch.cuda.synchronize()
         launches = gsn.launch_count() - launches0
         barrier()
-        ms = e0.elapsed_time(e1)
-        if dist is not None:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms, launches
+        return max_over_ranks(e0.elapsed_time(e1)), launches
 
-    for k in range(args.warmup):
-        step(k)
-    torch.cuda.synchronize()
+    def eager_steps(f, k0, e2e=False):
+        return lambda steps: [step(f, k0 + k, e2e) for k in range(steps)]
+
+    def profile_stages(f):
+        gsn.profile_enable(True)
+        for k in range(args.steps):
+            step(f, args.warmup + k)
+        st = gsn.profile_collect()
+        gsn.profile_enable(False)
+        return {k: v / args.steps for k, v in st.items() if v > 0}
+
+    def measure(f, with_stages=True):
+        """Eager timing, per-stage profile, end-to-end timing, then the graph form."""
+        for k in range(args.warmup):
+            step(f, k)
+        torch.cuda.synchronize()
+        ms, launches = timed(eager_steps(f, args.warmup), args.steps)
+        stages = profile_stages(f) if with_stages else None
+        f.solver.set_compute_loss(True)
+        for k in range(2):
+            step(f, k, True)
+        ms_e2e, _ = timed(eager_steps(f, args.warmup, True), args.steps)
+        records = int(f.renderer.buffers().record_count_host)
+        # visible Gaussians of the last frame, read while the renderer is alive
+        counts = torch.empty(n, dtype=torch.int32, device="cuda")
+        gsn.memcpy(counts.data_ptr(), f.renderer.buffers().tile_counts, 4 * n)
+        visible_count = int((counts > 0).sum().item())
+        # batched form: the iteration captured once as a CUDA graph over a fixed
+        # record capacity, replayed from a device schedule of views
+        graph = gsn.Graph()
+        capacity = int(records * 1.5) + 65536
+        graph.capture(f.renderer, f.solver, f.params.data_ptr(), n, train, targets.data_ptr(), 1064 * 1600 * 3,
+                      [0, 0, 0], img.data_ptr(), SH_DEGREE, capacity, sp)
+        schedule = [(args.warmup + k) % len(train) for k in range(args.steps)]
+        graph.run(schedule[:max(3, args.warmup)], [lr] * max(3, args.warmup))
+        ms_graph, graph_launches = timed(lambda steps: graph.run(schedule[:steps], [lr] * steps), args.steps)
+        status = graph.check()
+
+        def graph_e2e(steps):
+            # pinned target upload, one replay and the loss read per step
+            for k in range(steps):
+                v = schedule[k]
+                targets[v].copy_(host_targets[v], non_blocking=True)
+                graph.run([v], [lr])
+                gsn.memcpy_async(loss_host.data_ptr(), f.solver.loss_device(), 32, sp)
+                stream.synchronize()
+
+        ms_graph_e2e, _ = timed(graph_e2e, args.steps)
+        status = status or graph.check()
+        per_step = graph.launches_per_step()
+        graph.close()
+        rate = lambda t: world * args.steps / (t / 1000.0)  # noqa: E731
+        eager = {"value": round(rate(ms), 3), "ms_per_step": round(ms / args.steps, 4), "e2e": round(rate(ms_e2e), 3),
+                 "gpu_launches": int(launches), "psnr_db_last_step": round(float(loss_host[3]), 3)}
+        graphed = {"value": round(rate(ms_graph), 3), "ms_per_step": round(ms_graph / args.steps, 4),
+                   "e2e": round(rate(ms_graph_e2e), 3), "gpu_launches": int(graph_launches),
+                   "launches_per_step": per_step, "record_capacity": capacity, "status": status,
+                   "psnr_db_last_step": round(float(loss_host[3]), 3)}
+        return eager, graphed, stages, records, visible_count
+
     if args.profile_only:
-        step(args.warmup)
+        f = Form(False)
+        for k in range(args.warmup + 1):
+            step(f, k)
         torch.cuda.synchronize()
         return
 
     visible = os.environ.get("CUDA_VISIBLE_DEVICES", "")
     smi_index = visible.split(",")[local] if visible else str(local)
     sampler = ClockSampler(smi_index) if rank == 0 else None
-    ms, launches = timed(args.warmup, args.steps)
+    plain = Form(False)
+    plain_eager, plain_graph, stages, records, vis = measure(plain)
+    del plain
+    torch.cuda.empty_cache()
+    prec = Form(True)
+    prec_eager, prec_graph, prec_stages, _, _ = measure(prec)
     clocks = sampler.stop() if sampler else None
-    value = world * args.steps / (ms / 1000.0)
-
-    # per-stage device time (profiled pass of the same steps)
-    gsn.profile_enable(True)
-    for k in range(args.steps):
-        step(args.warmup + k)
-    stages = gsn.profile_collect()
-    gsn.profile_enable(False)
-    stages = {k: v / args.steps for k, v in stages.items() if v > 0}
-
-    # end-to-end through host buffers
-    solver.set_compute_loss(True)
-    for k in range(2):
-        step(k, True)
-    ms_e2e, _ = timed(args.warmup, args.steps, e2e=True)
-    value_e2e = world * args.steps / (ms_e2e / 1000.0)
-    psnr = float(loss_host[3])
-
-    b = renderer.buffers()
-    records = int(b.record_count_host)
-
-    # batched form: the same iteration captured once as a CUDA graph over a
-    # fixed record capacity, replayed from a device schedule of views
-    graph = gsn.Graph()
-    capacity = int(records * 1.5) + 65536
-    graph.capture(renderer, solver, params.data_ptr(), n, train, targets.data_ptr(), 1064 * 1600 * 3,
-                  [0, 0, 0], img.data_ptr(), SH_DEGREE, capacity, sp)
-    schedule = [(args.warmup + k) % len(train) for k in range(args.steps)]
-    graph.run(schedule[:max(3, args.warmup)], [lr] * max(3, args.warmup))
-    barrier()
-    torch.cuda.synchronize()
-    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    launches0 = gsn.launch_count()
-    g0.record(stream)
-    graph.run(schedule, [lr] * args.steps)
-    g1.record(stream)
-    torch.cuda.synchronize()
-    graph_launches = gsn.launch_count() - launches0
-    barrier()
-    ms_graph = g0.elapsed_time(g1)
-    if dist is not None:
-        t = torch.tensor([ms_graph], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_graph = float(t.item())
-    graph_status = graph.check()
-    # end-to-end: pinned target upload, one replay and the loss read per step
-    barrier()
-    torch.cuda.synchronize()
-    g0.record(stream)
-    for k in range(args.steps):
-        v = schedule[k]
-        targets[v].copy_(host_targets[v], non_blocking=True)
-        graph.run([v], [lr])
-        gsn.memcpy_async(loss_host.data_ptr(), solver.loss_device(), 32, sp)
-        stream.synchronize()
-    g1.record(stream)
-    torch.cuda.synchronize()
-    ms_graph_e2e = g0.elapsed_time(g1)
-    if dist is not None:
-        t = torch.tensor([ms_graph_e2e], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_graph_e2e = float(t.item())
-    graph_status = graph_status or graph.check()
-    launches_per_step = graph.launches_per_step()
-    graph.close()
-    value_graph = world * args.steps / (ms_graph / 1000.0)
-    value_graph_e2e = world * args.steps / (ms_graph_e2e / 1000.0)
+    del prec
+    value = plain_eager["value"]
+    ms = plain_eager["ms_per_step"] * args.steps
+    psnr = plain_eager["psnr_db_last_step"]
 
     if rank != 0:
         if dist is not None:
@@ -391,9 +406,6 @@ def run_gsn(args):
     tiles = cam.tile_count_x * cam.tile_count_y
     pixels = cam.width * cam.height
     tile_bits = max(1, (tiles - 1).bit_length())
-    counts = torch.empty(n, dtype=torch.int32, device="cuda")
-    gsn.memcpy(counts.data_ptr(), b.tile_counts, 4 * n)
-    vis = int((counts > 0).sum().item())
     alg = algorithmic_bytes(n, records, tiles, pixels, tile_passes=(tile_bits + 7) // 8, visible=vis)
     peak, peak_kind = load_peaks()
     stage_table = {}
@@ -423,21 +435,16 @@ def run_gsn(args):
         tgt0 = targets[0].cpu().numpy()
         res = cpu_baseline(model, train[0], tgt0, extent, steps=1)
         cpu = {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")}
-    graph_ok = graph_status == 0
-    forms = {
-        "plain_fp32": {"value": round(value, 3), "ms_per_step": round(ms / args.steps, 4),
-                       "e2e": round(value_e2e, 3), "gpu_launches": int(launches)},
-        "graph_fp32": {"value": round(value_graph, 3), "ms_per_step": round(ms_graph / args.steps, 4),
-                       "e2e": round(value_graph_e2e, 3), "gpu_launches": int(graph_launches),
-                       "launches_per_step": launches_per_step, "record_capacity": capacity,
-                       "status": graph_status},
-    }
-    chosen = "graph_fp32" if graph_ok and value_graph > value else "plain_fp32"
+    forms = {"plain_fp32": plain_eager, "graph_fp32": plain_graph, "precision_bf16": prec_eager,
+             "precision_bf16_graph": prec_graph}
+    valid = {k: v for k, v in forms.items() if v.get("status", 0) == 0}
+    chosen = max(valid, key=lambda k: valid[k]["value"])
     out = {
         "metric": METRIC, "value": forms[chosen]["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": forms[chosen]["ms_per_step"], "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": ("FP32 training step (render, L1+SSIM gradient, backward, Adam) at the "
+        "scaling": "weak", "vs_baseline": None, "dtype": "bf16+f32" if chosen.startswith("precision") else "f32",
+        "data": "synthetic",
+        "config": {"workload": ("training step (render, L1+SSIM gradient, backward, Adam) at the "
                                 "1.2M-Gaussian cap, 1600x1064, SH degree 3, one ring view per step"),
                    "form": chosen, "gaussians": n, "width": 1600, "height": 1064,
                    "records_per_step": records, "visible_gaussians": vis, "parallelism": f"replicas{world}",
@@ -446,9 +453,10 @@ def run_gsn(args):
         "forms": forms,
         "chosen_over_plain": round(forms[chosen]["value"] / value, 4),
         "e2e": {"value": forms[chosen]["e2e"], "unit": UNIT, "h2d_bytes_per_step": 1600 * 1064 * 3,
-                "d2h_bytes_per_step": 32, "psnr_db_last_step": round(psnr, 3)},
+                "d2h_bytes_per_step": 32, "psnr_db_last_step": forms[chosen]["psnr_db_last_step"]},
         "roofline": roofline,
         "stages": stage_table,
+        "stages_precision": {k: round(v, 4) for k, v in prec_stages.items()},
         "clocks": clocks,
         "cpu_baseline": cpu,
     }
