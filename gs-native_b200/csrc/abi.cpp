@@ -631,4 +631,19 @@ int gsn_graph_launches_per_step(gsn_graph* g, int* out) {
     return GSN_OK;
 }
 
+// ---------------------------------------------------------------- tensor cores
+int gsn_tc_gemm_selftest(const float* a, const float* b, float* d, void* stream) {
+    int* status = nullptr;
+    if (cudaMalloc(&status, sizeof(int)) != cudaSuccess) return GSN_ERR_OUT_OF_MEMORY;
+    int result = cudaMemsetAsync(status, 0, sizeof(int), AsStream(stream)) == cudaSuccess ? GSN_OK : GSN_ERR_CUDA;
+    if (result == GSN_OK) result = gsn::launch_tc_gemm_selftest(a, b, d, status, AsStream(stream));
+    int host_status = GSN_OK;
+    if (result == GSN_OK &&
+        (cudaMemcpyAsync(&host_status, status, sizeof(int), cudaMemcpyDeviceToHost, AsStream(stream)) != cudaSuccess ||
+         cudaStreamSynchronize(AsStream(stream)) != cudaSuccess))
+        result = GSN_ERR_CUDA;
+    cudaFree(status);
+    return result == GSN_OK ? host_status : result;
+}
+
 }  // extern "C"

@@ -173,4 +173,10 @@ int launch_gaussian_update(const GaussianUpdateArgs& a, int sh_degree, cudaStrea
 int launch_remap_moments(const int* parents, const float* prev_m, const float* prev_v, float* m, float* v,
                          int prev_count, int count, bool bf16_sh, cudaStream_t stream);
 
+// ---------------------------------------------------------------- tcgen05
+// D (128 x 64 fp32, row-major) = A (128 x 128) * B^T (B: 64 x 128), operands
+// fp32 row-major on the device, rounded to bf16 and multiplied on the tensor
+// cores; *status is set to GSN_ERR_TIMEOUT if the MMA never completed.
+int launch_tc_gemm_selftest(const float* a, const float* b, float* d, int* status, cudaStream_t stream);
+
 }  // namespace gsn

@@ -354,6 +354,13 @@ int gsn_graph_run(gsn_graph* g, const int* views, const float* position_lrs, int
 int gsn_graph_check(gsn_graph* g);
 int gsn_graph_launches_per_step(gsn_graph* g, int* out);
 
+/* ------------------------------------------------------------------ tensor cores
+ * Self-test of the tcgen05 path used by the precision form's SSIM filter
+ * (gs-native extension): d (128 x 64 fp32, row-major) = a (128 x 128) * b^T
+ * (b: 64 x 128), all device pointers, operands rounded to bf16, accumulated in
+ * fp32 tensor memory. Synchronises; GSN_ERR_TIMEOUT if the MMA did not finish. */
+int gsn_tc_gemm_selftest(const float* a, const float* b, float* d, void* stream);
+
 /* ------------------------------------------------------------------ PLY
  * WriteGaussiansPly / ReadGaussiansPly (reference src/io/data_io.cpp:420-590)
  * on a host 58 x count SoA block. */
