@@ -65,6 +65,7 @@ def parse():
     p.add_argument("--profile-only", action="store_true",
                    help="warm-up steps plus one step on 3 views, no JSON (for ncu captures)")
     p.add_argument("--views", type=int, default=0, help="number of training views used (0 = all 180)")
+    p.add_argument("--precision", action="store_true", help="with --profile-only: run the precision form")
     return p.parse_args()
 
 
@@ -377,7 +378,7 @@ def run_gsn(args):
         return eager, graphed, stages, records, visible_count
 
     if args.profile_only:
-        f = Form(False)
+        f = Form(args.precision)
         for k in range(args.warmup + 1):
             step(f, k)
         torch.cuda.synchronize()

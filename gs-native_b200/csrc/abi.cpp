@@ -281,6 +281,21 @@ int gsn_solver_set_bf16_sh(gsn_solver* s, int enabled) {
     return GSN_OK;
 }
 
+int gsn_solver_set_tensor_core_loss(gsn_solver* s, int enabled) {
+    if (!s) return GSN_ERR_INVALID_ARGUMENT;
+    s->impl.SetTensorCoreLoss(enabled != 0);
+    return GSN_OK;
+}
+
+int gsn_solver_status(gsn_solver* s, int* status) {
+    if (!s || !status) return GSN_ERR_INVALID_ARGUMENT;
+    *status = GSN_OK;
+    if (!s->impl.GetStatusDevice()) return GSN_OK;
+    return cudaMemcpy(status, s->impl.GetStatusDevice(), sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess
+               ? GSN_OK
+               : GSN_ERR_CUDA;
+}
+
 int gsn_solver_set_compute_loss(gsn_solver* s, int enabled) {
     if (!s) return GSN_ERR_INVALID_ARGUMENT;
     s->impl.SetComputeLoss(enabled != 0);

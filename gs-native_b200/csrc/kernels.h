@@ -127,6 +127,12 @@ int launch_raster_forward(const RasterForwardArgs& a, cudaStream_t stream);
 // frame (optional): the target is frame->target instead of `target`.
 int launch_loss_gradient(const float* image, const uint8_t* target, const StepFrame* frame, float* grad, int width,
                          int height, double* sums, cudaStream_t stream);
+// Precision form of the same gradient: the 11x11 window runs as banded-Toeplitz
+// GEMMs on the tcgen05 tensor cores with a hi/lo bf16 split and fp32
+// accumulation (loss_tc.cu). *status (device) is set to GSN_ERR_TIMEOUT if a
+// tensor-core pass never completed.
+int launch_loss_gradient_tc(const float* image, const uint8_t* target, const StepFrame* frame, float* grad, int width,
+                            int height, double* sums, int* status, cudaStream_t stream);
 // out[0..3] = loss, mean L1, mean SSIM, PSNR (dB) from the sums above.
 int launch_finalize_loss(const double* sums, int width, int height, double* out, cudaStream_t stream);
 

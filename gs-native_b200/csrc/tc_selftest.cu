@@ -47,8 +47,8 @@ __global__ void __launch_bounds__(128) tc_gemm_selftest_kernel(const float* __re
 #pragma unroll 1
         for (int k = 0; k < kK / 16; ++k) {
             // K = 16 step k starts at core-matrix column 2k (256 bytes per step)
-            const uint64_t da = tc::kmajor_desc(base_a + k * 256, 128, kK * 16);
-            const uint64_t db = tc::kmajor_desc(base_b + k * 256, 128, kK * 16);
+            const uint64_t da = tc::smem_desc(base_a + k * 256, 128, kK * 16);
+            const uint64_t db = tc::smem_desc(base_b + k * 256, 128, kK * 16);
             tc::mma_bf16(tmem, da, db, idesc, k > 0);
         }
         tc::commit(&bar);

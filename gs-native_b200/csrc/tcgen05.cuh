@@ -27,9 +27,12 @@ __host__ __device__ constexpr uint32_t kmajor_offset(uint32_t r, uint32_t k, uin
     return ((r >> 3) * (K >> 3) + (k >> 3)) * 128u + (r & 7u) * 16u + (k & 7u) * 2u;
 }
 
-// Shared-memory descriptor: start address, leading (K) and stride (8-row)
-// byte offsets, descriptor version 1 (sm_100), no swizzle.
-__device__ __forceinline__ uint64_t kmajor_desc(uint32_t smem_addr, uint32_t lbo, uint32_t sbo) {
+// Shared-memory descriptor (no swizzle, descriptor version 1 of sm_100):
+// start address and the leading / stride byte offsets. For a K-major operand
+// LBO separates core matrices along K and SBO 8-row groups along M/N; for an
+// MN-major operand (instruction-descriptor major bit set) SBO separates
+// 8-element groups along M/N and LBO 8-row groups along K.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t smem_addr, uint32_t lbo, uint32_t sbo) {
     return static_cast<uint64_t>((smem_addr >> 4) & 0x3FFFu) |
            (static_cast<uint64_t>((lbo >> 4) & 0x3FFFu) << 16) |
            (static_cast<uint64_t>((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);

@@ -96,6 +96,8 @@ def lib():
         "gsn_renderer_set_record_capacity": ([vp, i64], i32),
         "gsn_renderer_set_bf16_sh": ([vp, i32], i32),
         "gsn_solver_set_bf16_sh": ([vp, i32], i32),
+        "gsn_solver_set_tensor_core_loss": ([vp, i32], i32),
+        "gsn_solver_status": ([vp, P(i32)], i32),
         "gsn_solver_create": ([P(vp)], i32),
         "gsn_solver_destroy": ([vp], i32),
         "gsn_solver_set_stream": ([vp, vp], i32),
@@ -271,6 +273,14 @@ class Solver:
 
     def set_bf16_sh(self, enabled=True):
         _check(lib().gsn_solver_set_bf16_sh(self.handle, int(bool(enabled))), "set_bf16_sh")
+
+    def set_tensor_core_loss(self, enabled=True):
+        _check(lib().gsn_solver_set_tensor_core_loss(self.handle, int(bool(enabled))), "set_tensor_core_loss")
+
+    def status(self):
+        out = ctypes.c_int()
+        _check(lib().gsn_solver_status(self.handle, ctypes.byref(out)), "status")
+        return out.value
 
     def loss(self):
         out = (ctypes.c_double * 4)()

@@ -21,6 +21,7 @@ size_t PhysicalRows(bool bf16_sh) { return bf16_sh ? 34 : kMaxParamCount; }
 void Solver::SetBf16Sh(bool enabled) {
     if (enabled == bf16_sh_) return;
     bf16_sh_ = enabled;
+    tensor_core_loss_ = enabled;
     m_.Reset();
     v_.Reset();
     gaussian_count_ = 0;
@@ -81,9 +82,18 @@ bool Solver::ComputeImageGradients(const CameraParams& camera, const float* imag
         sums = loss_.get();
     }
     gsn::stage_mark(stream_, gsn::kStageLossGradient);
-    if (gsn::launch_loss_gradient(image, target, frame_, image_gradients_.get(), camera.width_, camera.height_, sums,
-                                  stream_) != GSN_OK)
+    if (tensor_core_loss_) {
+        if (!status_.get()) {
+            if (!status_.Reserve(1) || cudaMemsetAsync(status_.get(), 0, sizeof(int), stream_) != cudaSuccess)
+                return false;
+        }
+        if (gsn::launch_loss_gradient_tc(image, target, frame_, image_gradients_.get(), camera.width_,
+                                         camera.height_, sums, status_.get(), stream_) != GSN_OK)
+            return false;
+    } else if (gsn::launch_loss_gradient(image, target, frame_, image_gradients_.get(), camera.width_,
+                                         camera.height_, sums, stream_) != GSN_OK) {
         return false;
+    }
     if (sums && gsn::launch_finalize_loss(sums, camera.width_, camera.height_, loss_.get() + 3, stream_) != GSN_OK)
         return false;
     return true;

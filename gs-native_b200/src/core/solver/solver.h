@@ -87,6 +87,13 @@ public:
     // Changing the layout drops the Adam history.
     void SetBf16Sh(bool enabled);
     bool GetBf16Sh() const { return bf16_sh_; }
+    // The L1+SSIM gradient on the tcgen05 tensor cores (banded-Toeplitz filter
+    // GEMMs, hi/lo bf16 split, fp32 accumulation). On by default in the
+    // precision form; can be switched independently.
+    void SetTensorCoreLoss(bool enabled) { tensor_core_loss_ = enabled; }
+    bool GetTensorCoreLoss() const { return tensor_core_loss_; }
+    // Device status word of the tensor-core passes: 0, or GSN_ERR_TIMEOUT.
+    const int* GetStatusDevice() const { return status_.get(); }
     void SetIteration(uint64_t iteration) { iteration_ = iteration; }
 
     // Stage entry points (used by Iterate and by the C ABI).
@@ -117,6 +124,8 @@ private:
     unsigned int* acc_count_ = nullptr;
     const gsn::StepFrame* frame_ = nullptr;
     bool bf16_sh_ = false;
+    bool tensor_core_loss_ = false;
+    DeviceArray<int> status_;
 };
 
 }  // namespace gs_native

@@ -202,6 +202,12 @@ int gsn_solver_set_learning_rates(gsn_solver* s, float scale, float rotation, fl
  * [loss, mean L1, mean SSIM, PSNR dB] of the last iterate to `out` (host). */
 int gsn_solver_set_compute_loss(gsn_solver* s, int enabled);
 int gsn_solver_set_bf16_sh(gsn_solver* s, int enabled);
+/* The L1+SSIM gradient on the tcgen05 tensor cores (banded-Toeplitz GEMMs,
+ * hi/lo bf16 split, fp32 accumulation): on with the precision form, switchable
+ * on its own. gsn_solver_status synchronises and returns GSN_OK or
+ * GSN_ERR_TIMEOUT (a tensor-core pass did not complete). */
+int gsn_solver_set_tensor_core_loss(gsn_solver* s, int enabled);
+int gsn_solver_status(gsn_solver* s, int* status);
 int gsn_solver_loss(gsn_solver* s, double* out);
 int gsn_solver_loss_device(gsn_solver* s, const double** out);
 
