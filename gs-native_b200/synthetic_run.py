@@ -10,6 +10,7 @@ wall and device time, the final Gaussian count and the mean FP64 PSNR of the
 held-out views.
 
     python synthetic_run.py [--iterations 30000] [--cap 1200000] [--width 1600 --height 1064]
+                            [--precision] [--graph]
 """
 import argparse
 import json
@@ -62,6 +63,8 @@ def main():
     p.add_argument("--width", type=int, default=1600)
     p.add_argument("--height", type=int, default=1064)
     p.add_argument("--chunk", type=int, default=1000)
+    p.add_argument("--precision", action="store_true", help="precision form (bf16 SH, tensor-core SSIM)")
+    p.add_argument("--graph", action="store_true", help="steady-state iterations as CUDA-graph replays")
     args = p.parse_args()
     import torch
 
@@ -69,7 +72,8 @@ def main():
     t0 = time.time()
     train, test, train_images, test_images, points, colors = build_scene(args, torch)
     setup_s = time.time() - t0
-    opts = gsn.TrainingOptions.defaults(max_gaussians=args.cap)
+    opts = gsn.TrainingOptions.defaults(max_gaussians=args.cap, precision=int(args.precision),
+                                        graph=int(args.graph))
     trainer = gsn.Trainer()
     assert trainer.initialize(train, train_images, points, colors, opts) == 0
     torch.cuda.synchronize()
@@ -95,7 +99,8 @@ def main():
         "iterations": args.iterations, "wall_s": round(wall, 2), "device_ms": round(device_ms, 1),
         "iters_per_s": round(args.iterations / (device_ms / 1000.0), 2), "gaussians": st["count"],
         "psnr_test_db": round(psnr, 4), "loss_test": round(loss, 6), "psnr_train_subset_db": round(psnr_train, 4),
-        "setup_s": round(setup_s, 1), "resolution": [args.width, args.height], "cap": args.cap, "log": log,
+        "setup_s": round(setup_s, 1), "resolution": [args.width, args.height], "cap": args.cap,
+        "form": ("precision_bf16" if args.precision else "plain_fp32") + ("_graph" if args.graph else ""), "log": log,
     }), flush=True)
 
 
