@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "core/density/density_controller.h"
+#include "core/density/density_mlp.h"
 #include "core/gaussian_splatting.h"
 #include "core/graph/training_graph.h"
 #include "io/ply.h"
@@ -32,6 +33,10 @@ struct gsn_density {
 
 struct gsn_trainer {
     gs_native::GaussianSplatting impl;
+};
+
+struct gsn_mlp {
+    gs_native::DensityMlp impl;
 };
 
 struct gsn_graph {
@@ -463,6 +468,9 @@ int gsn_training_options_default(gsn_training_options* out) {
     out->initial_opacity = o.initial_opacity;
     out->precision = o.bf16_sh ? 1 : 0;
     out->graph = o.graph ? 1 : 0;
+    out->learned_density = o.learned_density ? 1 : 0;
+    out->learned_confidence = o.learned_confidence;
+    out->log_density = o.log_density ? 1 : 0;
     return GSN_OK;
 }
 
@@ -497,6 +505,9 @@ gs_native::TrainingOptions ToOptions(const gsn_training_options& in) {
     o.initial_opacity = in.initial_opacity;
     o.bf16_sh = in.precision != 0;
     o.graph = in.graph != 0;
+    o.learned_density = in.learned_density != 0;
+    o.learned_confidence = in.learned_confidence;
+    o.log_density = in.log_density != 0;
     return o;
 }
 }  // namespace
@@ -659,6 +670,69 @@ int gsn_tc_gemm_selftest(const float* a, const float* b, float* d, void* stream)
         result = GSN_ERR_CUDA;
     cudaFree(status);
     return result == GSN_OK ? host_status : result;
+}
+
+// ---------------------------------------------------------------- learned density
+int gsn_trainer_set_density_mlp(gsn_trainer* t, const float* weights) {
+    if (!t || !weights) return GSN_ERR_INVALID_ARGUMENT;
+    return t->impl.SetDensityMlp(weights) ? GSN_OK : GSN_ERR_CUDA;
+}
+
+int gsn_trainer_density_log(gsn_trainer* t, const float** features, const int8_t** decisions, const int** parents,
+                            int* before, int* after, int* steps, int* iteration) {
+    if (!t) return GSN_ERR_INVALID_ARGUMENT;
+    const gs_native::DensityLog& log = t->impl.GetDensityLog();
+    if (features) *features = log.features;
+    if (decisions) *decisions = log.decisions;
+    if (parents) *parents = log.parents;
+    if (before) *before = log.before;
+    if (after) *after = log.after;
+    if (steps) *steps = log.steps;
+    if (iteration) *iteration = log.iteration;
+    return GSN_OK;
+}
+
+int gsn_mlp_create(gsn_mlp** out) {
+    if (!out) return GSN_ERR_INVALID_ARGUMENT;
+    *out = new (std::nothrow) gsn_mlp();
+    return *out ? GSN_OK : GSN_ERR_OUT_OF_MEMORY;
+}
+
+int gsn_mlp_destroy(gsn_mlp* m) {
+    delete m;
+    return GSN_OK;
+}
+
+int gsn_mlp_initialize(gsn_mlp* m, unsigned long long seed) {
+    if (!m) return GSN_ERR_INVALID_ARGUMENT;
+    return m->impl.Initialize(seed) ? GSN_OK : GSN_ERR_CUDA;
+}
+
+int gsn_mlp_set_weights(gsn_mlp* m, const float* host_weights) {
+    if (!m || !host_weights) return GSN_ERR_INVALID_ARGUMENT;
+    return m->impl.SetWeights(host_weights) ? GSN_OK : GSN_ERR_CUDA;
+}
+
+int gsn_mlp_get_weights(gsn_mlp* m, float* host_weights) {
+    if (!m || !host_weights) return GSN_ERR_INVALID_ARGUMENT;
+    return m->impl.GetWeights(host_weights) ? GSN_OK : GSN_ERR_NOT_READY;
+}
+
+int gsn_mlp_gradients(gsn_mlp* m, const float* features, const int* labels, const float* weights, int n,
+                      float* host_grad, double* loss) {
+    if (!m) return GSN_ERR_INVALID_ARGUMENT;
+    return m->impl.Gradients(features, labels, weights, n, host_grad, loss) ? GSN_OK : GSN_ERR_INVALID_ARGUMENT;
+}
+
+int gsn_mlp_train(gsn_mlp* m, const float* features, const int* labels, const float* weights, int n, int steps,
+                  float lr, double* loss) {
+    if (!m) return GSN_ERR_INVALID_ARGUMENT;
+    return m->impl.Train(features, labels, weights, n, steps, lr, loss) ? GSN_OK : GSN_ERR_INVALID_ARGUMENT;
+}
+
+int gsn_mlp_infer(gsn_mlp* m, const float* features, int n, float confidence, int8_t* actions, float* probs) {
+    if (!m) return GSN_ERR_INVALID_ARGUMENT;
+    return m->impl.Infer(features, n, confidence, actions, probs) ? GSN_OK : GSN_ERR_INVALID_ARGUMENT;
 }
 
 }  // extern "C"

@@ -55,18 +55,11 @@ __global__ void accumulate_observations_kernel(const float* __restrict__ grads, 
     atomicAdd(counts + id, 1u);
 }
 
-__global__ void decide_kernel(const float* __restrict__ params, const float* __restrict__ sums,
-                              const float* __restrict__ abs_sums, const unsigned int* __restrict__ obs,
-                              const int* __restrict__ control, int4* __restrict__ counts, int* __restrict__ additions,
-                              int n, DensityThresholds th) {
-    const int id = blockIdx.x * blockDim.x + threadIdx.x;
-    if (id > n) return;
-    if (id == n || id >= control[0]) {
-        counts[id] = make_int4(0, 0, 0, 0);
-        if (additions && id < n) additions[id] = 0;
-        return;
-    }
-    const int64_t N = n;
+// The plain threshold rule for one Gaussian (density_controller.cu:60-116):
+// (survive, clone, split sampled, split kept).
+__device__ __forceinline__ int4 plain_decision(const float* __restrict__ params, const float* __restrict__ sums,
+                                               const float* __restrict__ abs_sums, const unsigned int* __restrict__ obs,
+                                               int64_t N, int id, const DensityThresholds& th) {
     float opacity = 1.0f / (1.0f + expf(-params[static_cast<int64_t>(GSN_OPACITY_INDEX) * N + id]));
     float gradient = obs[id] ? sums[id] / obs[id] : 0;
     if (isnan(gradient)) gradient = 0;
@@ -90,8 +83,107 @@ __global__ void decide_kernel(const float* __restrict__ params, const float* __r
         if (isnan(x) || isnan(y) || isnan(z)) remaining = nanf("");
     }
     bool remove = opacity < th.min_opacity || (th.prune_large && remaining > th.max_world_size);
-    counts[id] = make_int4(!split && !remove, clone && !remove, split, split && !remove);
-    if (additions) additions[id] = (clone && !remove) || (split && !remove) ? 1 : 0;
+    return make_int4(!split && !remove, clone && !remove, split, split && !remove);
+}
+
+// Decision of an action code (learned policy): 0 keep, 1 clone, 2 split, 3 prune.
+__device__ __forceinline__ int4 action_decision(int action) {
+    switch (action) {
+        case 1: return make_int4(1, 1, 0, 0);
+        case 2: return make_int4(0, 0, 1, 1);
+        case 3: return make_int4(0, 0, 0, 0);
+        default: return make_int4(1, 0, 0, 0);
+    }
+}
+
+__global__ void decide_kernel(const float* __restrict__ params, const float* __restrict__ sums,
+                              const float* __restrict__ abs_sums, const unsigned int* __restrict__ obs,
+                              const int* __restrict__ control, const int8_t* __restrict__ actions,
+                              int4* __restrict__ counts, int* __restrict__ additions, int n, DensityThresholds th) {
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id > n) return;
+    if (id == n || id >= control[0]) {
+        counts[id] = make_int4(0, 0, 0, 0);
+        if (additions && id < n) additions[id] = 0;
+        return;
+    }
+    int4 c = plain_decision(params, sums, abs_sums, obs, n, id, th);
+    // a learned proposal replaces the plain decision where one is given (>= 0)
+    if (actions && actions[id] >= 0) c = action_decision(actions[id]);
+    counts[id] = c;
+    if (additions) additions[id] = c.y || c.w ? 1 : 0;
+}
+
+__global__ void codes_kernel(const int4* __restrict__ counts, int n, int8_t* __restrict__ codes) {
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= n) return;
+    const int4 c = counts[id];
+    codes[id] = c.z ? 2 : (c.y ? 1 : (c.x ? 0 : 3));
+}
+
+// The 16 per-Gaussian statistics of the learned density policy (normalised so
+// that the plain rule's thresholds sit at simple values):
+//  0 mean view-space gradient / gradient threshold   1 mean |gradient| / its threshold
+//  2 log(1 + observations)                            3 opacity
+//  4 opacity logit                                    5 log(max scale / split threshold)
+//  6 log(min scale / split threshold)                 7 mean log-scale - log(split threshold)
+//  8 max scale / prune-large world size               9 |SH DC|
+// 10 RMS of the higher SH coefficients               11 distance from the scene centre / extent
+// 12 log(max / min scale)                            13-15 plain rule: clone, split, prune
+template <bool kBf16>
+__global__ void features_kernel(const float* __restrict__ params, const float* __restrict__ sums,
+                                const float* __restrict__ abs_sums, const unsigned int* __restrict__ obs, int n,
+                                DensityThresholds th, float3 centre, float extent, float* __restrict__ out) {
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= n) return;
+    const int64_t N = n;
+    const int4 c = plain_decision(params, sums, abs_sums, obs, N, id, th);
+    const float logit = params[static_cast<int64_t>(GSN_OPACITY_INDEX) * N + id];
+    float ls[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) ls[a] = params[static_cast<int64_t>(GSN_LOG_SCALE_INDEX + a) * N + id];
+    const float lmax = fmaxf(ls[0], fmaxf(ls[1], ls[2])), lmin = fminf(ls[0], fminf(ls[1], ls[2]));
+    const float lsplit = logf(fmaxf(th.split_threshold, 1e-12f));
+    const float gmean = obs[id] ? sums[id] / obs[id] : 0.0f;
+    const float amean = obs[id] ? abs_sums[id] / obs[id] : 0.0f;
+    const float athr = th.absolute_gradient_threshold > 0.0f ? th.absolute_gradient_threshold : th.gradient_threshold;
+    float dc = 0.0f, rest = 0.0f;
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch) {
+        const float d = load_sh<kBf16>(params, N, ch * kShStride, id);
+        dc += d * d;
+#pragma unroll
+        for (int k = 1; k < kShStride; ++k) {
+            const float v = load_sh<kBf16>(params, N, ch * kShStride + k, id);
+            rest += v * v;
+        }
+    }
+    const float dx = params[id] - centre.x, dy = params[N + id] - centre.y, dz = params[2 * N + id] - centre.z;
+    float f[16];
+    f[0] = fminf(gmean / th.gradient_threshold, 50.0f);
+    f[1] = fminf(amean / athr, 50.0f);
+    f[2] = log1pf(static_cast<float>(obs[id]));
+    f[3] = 1.0f / (1.0f + expf(-logit));
+    f[4] = fminf(fmaxf(logit, -10.0f), 10.0f);
+    f[5] = fminf(fmaxf(lmax - lsplit, -10.0f), 10.0f);
+    f[6] = fminf(fmaxf(lmin - lsplit, -10.0f), 10.0f);
+    f[7] = fminf(fmaxf((ls[0] + ls[1] + ls[2]) * (1.0f / 3.0f) - lsplit, -10.0f), 10.0f);
+    f[8] = fminf(expf(lmax) / fmaxf(th.max_world_size, 1e-12f), 10.0f);
+    f[9] = sqrtf(dc);
+    f[10] = sqrtf(rest * (1.0f / 45.0f));
+    f[11] = fminf(sqrtf(dx * dx + dy * dy + dz * dz) / fmaxf(extent, 1e-12f), 10.0f);
+    f[12] = fminf(lmax - lmin, 20.0f);
+    f[13] = c.y ? 1.0f : 0.0f;
+    f[14] = c.z ? 1.0f : 0.0f;
+    f[15] = !c.x && !c.y && !c.z ? 1.0f : 0.0f;
+#pragma unroll
+    for (int k = 0; k < 16; ++k)
+        if (!isfinite(f[k])) f[k] = 0.0f;
+    float4* o = reinterpret_cast<float4*>(out + static_cast<int64_t>(id) * 16);
+    o[0] = make_float4(f[0], f[1], f[2], f[3]);
+    o[1] = make_float4(f[4], f[5], f[6], f[7]);
+    o[2] = make_float4(f[8], f[9], f[10], f[11]);
+    o[3] = make_float4(f[12], f[13], f[14], f[15]);
 }
 
 // Cap: accept additions (clone or kept split) in id order while the count stays
@@ -368,8 +460,8 @@ size_t density_scan_scratch_bytes(int n) {
 
 int launch_density_decide(const DensityDecideArgs& a, cudaStream_t s) {
     const int n = a.n;
-    decide_kernel<<<grid_for(n + 1), kThreads, 0, s>>>(a.params, a.sums, a.abs_sums, a.obs, a.control, a.counts,
-                                                      a.max_count > 0 ? a.additions : nullptr, n, a.th);
+    decide_kernel<<<grid_for(n + 1), kThreads, 0, s>>>(a.params, a.sums, a.abs_sums, a.obs, a.control, a.actions,
+                                                      a.counts, a.max_count > 0 ? a.additions : nullptr, n, a.th);
     int launches = 1;
     const int blocks = (n + 1 + kScanChunk - 1) / kScanChunk;
     auto scan4 = [&]() {
@@ -388,6 +480,25 @@ int launch_density_decide(const DensityDecideArgs& a, cudaStream_t s) {
     }
     prepare_kernel<<<1, 1, 0, s>>>(a.offsets, a.control, n, a.random_blocks);
     return launched(launches + 1);
+}
+
+int launch_density_codes(const int4* counts, int n, int8_t* codes, cudaStream_t s) {
+    if (n <= 0) return GSN_OK;
+    codes_kernel<<<grid_for(n), kThreads, 0, s>>>(counts, n, codes);
+    return launched(1);
+}
+
+int launch_density_features(const float* params, const float* sums, const float* abs_sums, const unsigned int* obs,
+                            int n, const DensityThresholds& th, float3 centre, float extent, bool bf16_sh,
+                            float* features, cudaStream_t s) {
+    if (n <= 0) return GSN_OK;
+    if (bf16_sh)
+        features_kernel<true><<<grid_for(n), kThreads, 0, s>>>(params, sums, abs_sums, obs, n, th, centre, extent,
+                                                               features);
+    else
+        features_kernel<false><<<grid_for(n), kThreads, 0, s>>>(params, sums, abs_sums, obs, n, th, centre, extent,
+                                                                features);
+    return launched(1);
 }
 
 int launch_density_prepare(const int4* offsets, int* control, int n, int random_blocks, cudaStream_t s) {

@@ -37,6 +37,7 @@ struct DensityDecideArgs {
     int max_count;      // 0 = no cap
     int random_blocks;
     DensityThresholds th;
+    const int8_t* actions;  // optional learned proposals: 0 keep, 1 clone, 2 split, 3 prune, < 0 plain rule
 };
 
 struct DensityApplyArgs {
@@ -68,6 +69,12 @@ size_t density_scan_scratch_bytes(int n);
 int launch_density_decide(const DensityDecideArgs& a, cudaStream_t s);
 int launch_density_prepare(const int4* offsets, int* control, int n, int random_blocks, cudaStream_t s);
 int launch_density_apply(const DensityApplyArgs& a, cudaStream_t s);
+// Decision codes of the last decide (0 keep, 1 clone, 2 split, 3 prune).
+int launch_density_codes(const int4* counts, int n, int8_t* codes, cudaStream_t s);
+// The 16 statistics of the learned density policy, [n][16] floats (density.cu).
+int launch_density_features(const float* params, const float* sums, const float* abs_sums, const unsigned int* obs,
+                            int n, const DensityThresholds& th, float3 centre, float extent, bool bf16_sh,
+                            float* features, cudaStream_t s);
 int launch_density_reset_opacity(const int* control, float* params, int stride, float max_logit, cudaStream_t s);
 
 }  // namespace gsn

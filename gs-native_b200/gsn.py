@@ -431,6 +431,7 @@ class TrainingOptions(ctypes.Structure):
         ("background", ctypes.c_float * 3), ("max_gaussians", ctypes.c_int),
         ("density_seed", ctypes.c_ulonglong), ("initial_opacity", ctypes.c_float),
         ("precision", ctypes.c_int), ("graph", ctypes.c_int),
+        ("learned_density", ctypes.c_int), ("learned_confidence", ctypes.c_float), ("log_density", ctypes.c_int),
     ]
 
     @classmethod
@@ -462,6 +463,8 @@ class Trainer:
             "gsn_trainer_evaluate": [vp, P(Camera), P(vp), i32, P(ctypes.c_double), P(ctypes.c_double)],
             "gsn_trainer_save": [vp, ctypes.c_char_p], "gsn_trainer_load": [vp, ctypes.c_char_p],
             "gsn_trainer_state": [vp, P(vp), P(i32), P(i32), P(i32), P(ctypes.c_float)],
+            "gsn_trainer_set_density_mlp": [vp, P(ctypes.c_float)],
+            "gsn_trainer_density_log": [vp, P(vp), P(vp), P(vp), P(i32), P(i32), P(i32), P(i32)],
         }
         for name, args in sigs.items():
             fn = getattr(L, name)
@@ -632,3 +635,95 @@ def from_precision_layout(block, n, torch):
     out[:10] = block[:10 * n].reshape(10, n)
     out[10:] = block[10 * n:34 * n].view(torch.bfloat16).reshape(48, n).float()
     return out
+
+
+def _trainer_set_density_mlp(self, weights):
+    import numpy as np
+    w = np.ascontiguousarray(weights, dtype=np.float32)
+    assert w.size == MLP_PARAMS
+    _check(lib().gsn_trainer_set_density_mlp(self.handle, w.ctypes.data_as(ctypes.POINTER(ctypes.c_float))),
+           "set_density_mlp")
+
+
+def _trainer_density_log(self):
+    f, d, p = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+    b, a, s, it = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    _check(lib().gsn_trainer_density_log(self.handle, ctypes.byref(f), ctypes.byref(d), ctypes.byref(p),
+                                         ctypes.byref(b), ctypes.byref(a), ctypes.byref(s), ctypes.byref(it)),
+           "density_log")
+    return dict(features=f.value, decisions=d.value, parents=p.value, before=b.value, after=a.value, steps=s.value,
+                iteration=it.value)
+
+
+Trainer.set_density_mlp = _trainer_set_density_mlp
+Trainer.density_log = _trainer_density_log
+
+MLP_PARAMS = 5508
+
+
+class Mlp:
+    """Learned density policy network (include/gsn.h "learned density MLP")."""
+
+    def __init__(self, seed=0):
+        L = lib()
+        vp, i32, P = ctypes.c_void_p, ctypes.c_int, ctypes.POINTER
+        sigs = {
+            "gsn_mlp_create": [P(vp)], "gsn_mlp_destroy": [vp], "gsn_mlp_initialize": [vp, ctypes.c_ulonglong],
+            "gsn_mlp_set_weights": [vp, P(ctypes.c_float)], "gsn_mlp_get_weights": [vp, P(ctypes.c_float)],
+            "gsn_mlp_gradients": [vp, vp, vp, vp, i32, P(ctypes.c_float), P(ctypes.c_double)],
+            "gsn_mlp_train": [vp, vp, vp, vp, i32, i32, ctypes.c_float, P(ctypes.c_double)],
+            "gsn_mlp_infer": [vp, vp, i32, ctypes.c_float, vp, vp],
+        }
+        for name, args in sigs.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = i32
+        h = ctypes.c_void_p()
+        _check(L.gsn_mlp_create(ctypes.byref(h)), "gsn_mlp_create")
+        self.handle = h
+        _check(L.gsn_mlp_initialize(h, seed), "gsn_mlp_initialize")
+
+    def close(self):
+        if self.handle:
+            lib().gsn_mlp_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def weights(self):
+        import numpy as np
+        w = np.zeros(MLP_PARAMS, np.float32)
+        _check(lib().gsn_mlp_get_weights(self.handle, w.ctypes.data_as(ctypes.POINTER(ctypes.c_float))),
+               "get_weights")
+        return w
+
+    def set_weights(self, w):
+        import numpy as np
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        _check(lib().gsn_mlp_set_weights(self.handle, w.ctypes.data_as(ctypes.POINTER(ctypes.c_float))),
+               "set_weights")
+
+    def gradients(self, features_ptr, labels_ptr, weights_ptr, n):
+        import numpy as np
+        g = np.zeros(MLP_PARAMS, np.float32)
+        loss = ctypes.c_double()
+        _check(lib().gsn_mlp_gradients(self.handle, ctypes.c_void_p(features_ptr), ctypes.c_void_p(labels_ptr),
+                                       ctypes.c_void_p(weights_ptr), int(n),
+                                       g.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), ctypes.byref(loss)),
+               "gradients")
+        return g, loss.value
+
+    def train(self, features_ptr, labels_ptr, weights_ptr, n, steps, lr):
+        loss = ctypes.c_double()
+        _check(lib().gsn_mlp_train(self.handle, ctypes.c_void_p(features_ptr), ctypes.c_void_p(labels_ptr),
+                                   ctypes.c_void_p(weights_ptr), int(n), int(steps), float(lr), ctypes.byref(loss)),
+               "train")
+        return loss.value
+
+    def infer(self, features_ptr, n, confidence, actions_ptr, probs_ptr=0):
+        _check(lib().gsn_mlp_infer(self.handle, ctypes.c_void_p(features_ptr), int(n), float(confidence),
+                                   ctypes.c_void_p(actions_ptr), ctypes.c_void_p(probs_ptr or None)), "infer")

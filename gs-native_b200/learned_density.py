@@ -1,0 +1,138 @@
+"""Learned density policy: data collection, GPU training and the plain-rule judge.
+
+1. collect(): a plain training run with the density log on. At every
+   density-control step the trainer keeps each Gaussian's 16 statistics, the
+   threshold rule's decision (keep / clone / split / prune) and the parent map
+   of the step's output. The outcome of a decision is read at the next step:
+   a Gaussian whose result (itself, its clone pair or its split children) is
+   pruned in full by the next step was doomed, so its label becomes prune;
+   every other decision keeps its label. Each step's samples are weighted by
+   the held-out loss improvement that followed it (1 + 10 * relative
+   improvement, clipped to [1, 3]), so decisions of productive steps count more.
+2. fit(): the MLP (16 -> 64 -> 64 -> 4, fp16 weights, fp32 accumulation) is
+   trained on the GPU by the library's fused forward/backward kernels.
+3. judge(): the learned policy (with the threshold rule as fallback below the
+   confidence threshold) and the plain rule train from the same start; the
+   proposal policy is accepted only if its held-out PSNR is within 0.1 dB of
+   the plain rule's.
+"""
+import numpy as np
+
+import gsn
+
+
+class Scene:
+    """Cameras, u8 targets and initial points of one training setup."""
+
+    def __init__(self, train_cams, train_images, test_cams, test_images, points, colors):
+        self.train_cams, self.train_images = train_cams, train_images
+        self.test_cams, self.test_images = test_cams, test_images
+        self.points, self.colors = points, colors
+
+
+def _host(ptr, dtype, count):
+    out = np.zeros(int(count), dtype=dtype)
+    if count:
+        gsn.memcpy(out.ctypes.data, ptr, out.nbytes)
+    return out
+
+
+def collect(scene, options, iterations, chunk=100, samples_per_step=8192, seed=0):
+    """Plain run with the density log; returns (features, labels, weights, info)."""
+    rng = np.random.default_rng(seed)
+    opts = gsn.TrainingOptions.defaults(**options, log_density=1, learned_density=0)
+    tr = gsn.Trainer()
+    assert tr.initialize(scene.train_cams, scene.train_images, scene.points, scene.colors, opts) == 0
+    steps = []
+    last = 0
+    done = 0
+    while done < iterations:
+        k = min(chunk, iterations - done)
+        assert tr.train(k) == 0
+        done += k
+        log = tr.density_log()
+        if log["steps"] == last:
+            continue
+        last = log["steps"]
+        _, loss_after = tr.evaluate(scene.test_cams, scene.test_images)
+        before = log["before"]
+        feats = _host(log["features"], np.float32, before * 16).reshape(before, 16)
+        codes = _host(log["decisions"], np.int8, before)
+        parents = _host(log["parents"], np.int32, log["after"])
+        pick = rng.choice(before, size=min(before, samples_per_step), replace=False)
+        steps.append(dict(features=feats[pick], codes=codes[pick], pick=pick, parents=parents,
+                          all_codes=codes, loss=loss_after, iteration=log["iteration"]))
+    tr.close()
+    feats, labels, weights = [], [], []
+    relabelled = 0
+    for k in range(len(steps) - 1):
+        cur, nxt = steps[k], steps[k + 1]
+        # outputs of step k are the inputs of step k + 1 (same indices)
+        children_pruned = np.ones(len(cur["all_codes"]), bool)
+        has_child = np.zeros(len(cur["all_codes"]), bool)
+        alive = nxt["all_codes"] != 3
+        np.logical_and.at(children_pruned, cur["parents"], ~alive)
+        has_child[cur["parents"]] = True
+        lab = cur["codes"].astype(np.int32).copy()
+        doomed = has_child[cur["pick"]] & children_pruned[cur["pick"]] & (lab != 3)
+        relabelled += int(doomed.sum())
+        lab[doomed] = 3
+        # held-out loss improvement over the interval that followed step k
+        gain = (cur["loss"] - nxt["loss"]) / max(cur["loss"], 1e-12)
+        wt = float(np.clip(1.0 + 10.0 * max(gain, 0.0), 1.0, 3.0))
+        feats.append(cur["features"])
+        labels.append(lab)
+        weights.append(np.full(len(lab), wt, np.float32))
+    info = dict(steps=len(steps), relabelled=relabelled)
+    if not feats:
+        return np.zeros((0, 16), np.float32), np.zeros(0, np.int32), np.zeros(0, np.float32), info
+    return np.concatenate(feats), np.concatenate(labels), np.concatenate(weights), info
+
+
+def fit(features, labels, weights, steps=600, lr=3e-3, seed=0):
+    """Trains the MLP on the GPU; returns (weights, final loss)."""
+    import torch
+    # class balance: the rare actions would otherwise be drowned by keep
+    counts = np.bincount(labels, minlength=4).astype(np.float64)
+    balance = (counts.sum() / np.maximum(counts, 1.0) / 4.0) ** 0.5
+    w = (weights * balance[labels]).astype(np.float32)
+    mlp = gsn.Mlp(seed=seed)
+    fd = torch.from_numpy(np.ascontiguousarray(features)).cuda()
+    ld = torch.from_numpy(np.ascontiguousarray(labels, dtype=np.int32)).cuda()
+    wd = torch.from_numpy(w).cuda()
+    loss = mlp.train(fd.data_ptr(), ld.data_ptr(), wd.data_ptr(), len(labels), steps, lr)
+    out = mlp.weights()
+    mlp.close()
+    return out, loss
+
+
+def train_run(scene, options, iterations, mlp_weights=None, confidence=0.9):
+    """Trains one policy; returns held-out PSNR, final count and the sum of
+    Gaussian counts over the run's chunks (Gaussian-iterations / 100)."""
+    learned = mlp_weights is not None
+    opts = gsn.TrainingOptions.defaults(**options, learned_density=int(learned), learned_confidence=confidence)
+    tr = gsn.Trainer()
+    assert tr.initialize(scene.train_cams, scene.train_images, scene.points, scene.colors, opts) == 0
+    if learned:
+        tr.set_density_mlp(mlp_weights)
+    load = 0
+    done = 0
+    while done < iterations:
+        k = min(100, iterations - done)
+        assert tr.train(k) == 0
+        done += k
+        load += tr.state()["count"] * k
+    psnr, loss = tr.evaluate(scene.test_cams, scene.test_images)
+    count = tr.state()["count"]
+    tr.close()
+    return dict(psnr=psnr, loss=loss, count=count, gaussian_iterations=load)
+
+
+def judge(scene, options, iterations, mlp_weights, confidence=0.9, tolerance_db=0.1):
+    """Plain rule against the learned policy from the same start."""
+    plain = train_run(scene, options, iterations)
+    learned = train_run(scene, options, iterations, mlp_weights, confidence)
+    accepted = learned["psnr"] >= plain["psnr"] - tolerance_db
+    return dict(plain=plain, learned=learned, accepted=bool(accepted),
+                delta_db=learned["psnr"] - plain["psnr"],
+                load_ratio=learned["gaussian_iterations"] / max(plain["gaussian_iterations"], 1))

@@ -56,6 +56,18 @@ public:
     // Precision form: parameter blocks in the 10 fp32 + 48 bf16 row layout
     // (34 float rows of stride N); set before the first ControlDensity.
     void SetBf16Sh(bool enabled) { bf16_sh_ = enabled; }
+    // Learned proposals for the next ControlDensity: per Gaussian 0 keep,
+    // 1 clone, 2 split, 3 prune, or < 0 for the plain threshold rule (device,
+    // count entries; nullptr = plain rule for all).
+    void SetActionOverride(const int8_t* actions) { actions_ = actions; }
+    // Decision codes (0 keep, 1 clone, 2 split, 3 prune) of the last
+    // ControlDensity into a device int8 array of the pre-control count.
+    bool GetDecisionCodes(int8_t* codes, int count) const;
+    // The 16 statistics of the learned policy for the current Gaussians
+    // (device [count][16]); same thresholds as ControlDensity.
+    bool ComputeFeatures(const GaussianBuffers& gaussians, float scene_extent, const float centre[3],
+                         float gradient_threshold, float percent_dense, float min_opacity, float max_screen_size,
+                         float absolute_gradient_threshold, float* features) const;
     const float* GetNewFlags() const { return new_flags_.get(); }
     float* GetGradientSums() { return gradient_sums_.get(); }
     float* GetAbsoluteGradientSums() { return absolute_gradient_sums_.get(); }
@@ -89,6 +101,7 @@ private:
     int random_blocks_ = 0;
     int max_gaussians_ = 0;
     bool bf16_sh_ = false;
+    const int8_t* actions_ = nullptr;
     unsigned long long seed_ = 0;
 };
 

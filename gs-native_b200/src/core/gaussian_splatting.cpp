@@ -60,6 +60,7 @@ bool GaussianSplatting::Initialize(const TrainingScene& scene, const TrainingOpt
         extent = std::max(extent, std::sqrt((c[0] - mean[0]) * (c[0] - mean[0]) + (c[1] - mean[1]) * (c[1] - mean[1]) +
                                             (c[2] - mean[2]) * (c[2] - mean[2])));
     scene_extent_ = static_cast<float>(extent) * 1.1f;
+    for (int a = 0; a < 3; ++a) scene_centre_[a] = static_cast<float>(mean[a]);
     if (scene_extent_ == 0.0f) {
         for (int i = 0; i < scene.point_count; ++i) {
             const float* p = scene.point_positions + 3 * i;
@@ -273,11 +274,47 @@ bool GaussianSplatting::Step() {
 
 bool GaussianSplatting::ControlDensity() {
     int changes[2] = {};
-    if (!density_.ControlDensity(gaussians_, scene_extent_, options_.gradient_threshold, options_.percent_dense,
-                                 options_.min_opacity, completed_ > options_.prune_large_after ? 20.0f : 0.0f,
-                                 options_.density_seed, changes, options_.absolute_gradient_threshold))
-        return false;
+    const float max_screen = completed_ > options_.prune_large_after ? 20.0f : 0.0f;
+    const int before = gaussians_.gaussian_count_;
+    const bool learned = options_.learned_density && mlp_ready_;
+    if (learned || options_.log_density) {
+        if (!density_features_.Reserve(static_cast<size_t>(std::max(before, 1)) * 16) ||
+            !density_.ComputeFeatures(gaussians_, scene_extent_, scene_centre_, options_.gradient_threshold,
+                                      options_.percent_dense, options_.min_opacity, max_screen,
+                                      options_.absolute_gradient_threshold, density_features_.get()))
+            return false;
+    }
+    if (learned) {
+        mlp_.SetStream(stream_);
+        if (!density_actions_.Reserve(static_cast<size_t>(std::max(before, 1))) ||
+            !mlp_.Infer(density_features_.get(), before, options_.learned_confidence, density_actions_.get()))
+            return false;
+        density_.SetActionOverride(density_actions_.get());
+    }
+    const bool ok = density_.ControlDensity(gaussians_, scene_extent_, options_.gradient_threshold,
+                                            options_.percent_dense, options_.min_opacity, max_screen,
+                                            options_.density_seed, changes, options_.absolute_gradient_threshold);
+    density_.SetActionOverride(nullptr);
+    if (!ok) return false;
+    if (options_.log_density) {
+        if (!density_codes_.Reserve(static_cast<size_t>(std::max(before, 1))) ||
+            !density_.GetDecisionCodes(density_codes_.get(), before))
+            return false;
+        density_log_.features = density_features_.get();
+        density_log_.decisions = density_codes_.get();
+        density_log_.parents = density_.GetParentIds();
+        density_log_.before = before;
+        density_log_.after = gaussians_.gaussian_count_;
+        density_log_.iteration = completed_;
+        ++density_log_.steps;
+    }
     return solver_.RemapGaussians(density_.GetHistoryParentIds(), gaussians_.gaussian_count_);
+}
+
+bool GaussianSplatting::SetDensityMlp(const float* weights) {
+    mlp_.SetStream(stream_);
+    mlp_ready_ = weights && mlp_.SetWeights(weights);
+    return mlp_ready_;
 }
 
 bool GaussianSplatting::Render(const CameraParams& camera, float* device_image) {

@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "core/density/density_controller.h"
+#include "core/density/density_mlp.h"
 #include "core/graph/training_graph.h"
 #include "core/render/renderer.h"
 #include "core/solver/solver.h"
@@ -65,6 +66,22 @@ struct TrainingOptions {
     // gs-native extensions
     bool bf16_sh = false;  // precision form: SH rows and their moments in bf16 (34-row block)
     bool graph = false;    // steady-state iterations (after densify_until) as CUDA-graph replays
+    // learned density policy: the MLP's proposals (SetDensityMlp) replace the
+    // threshold rule where its softmax confidence reaches learned_confidence
+    bool learned_density = false;
+    float learned_confidence = 0.9f;
+    bool log_density = false;  // keep the statistics and decisions of the last control step (GetDensityLog)
+};
+
+// Statistics, decisions and parent map of the last density-control step
+// (device pointers, valid until the next step).
+struct DensityLog {
+    const float* features = nullptr;  // [before][16] statistics before the decision
+    const int8_t* decisions = nullptr;  // [before] 0 keep, 1 clone, 2 split, 3 prune
+    const int* parents = nullptr;     // [after] source index of every output Gaussian
+    int before = 0, after = 0;
+    int steps = 0;                    // control steps logged so far
+    int iteration = 0;                // iteration of the last step
 };
 
 class GaussianSplatting {
@@ -96,6 +113,9 @@ public:
     Solver& GetSolver() { return solver_; }
     DensityController& GetDensity() { return density_; }
     const TrainingOptions& GetOptions() const { return options_; }
+    // Weights of the learned density policy (DensityMlp::kParams floats, host).
+    bool SetDensityMlp(const float* weights);
+    const DensityLog& GetDensityLog() const { return density_log_; }
 
 private:
     bool InitializeGaussians(const float* positions, const float* colors, int count);
@@ -131,6 +151,13 @@ private:
     float scene_extent_ = 0.0f;
     TrainingGraph graph_;
     std::mt19937 generator_;
+    float scene_centre_[3] = {0.0f, 0.0f, 0.0f};
+    DensityMlp mlp_;
+    bool mlp_ready_ = false;
+    DeviceArray<float> density_features_;
+    DeviceArray<int8_t> density_actions_;
+    DeviceArray<int8_t> density_codes_;
+    DensityLog density_log_;
 };
 
 }  // namespace gs_native

@@ -307,6 +307,9 @@ typedef struct gsn_training_options {
     /* gs-native extensions (0 = reference behaviour) */
     int precision;                   /* 1: precision form - SH and its Adam moments stored in bf16 */
     int graph;                       /* 1: iterations after densify_until run as CUDA-graph replays */
+    int learned_density;             /* 1: the learned policy (gsn_trainer_set_density_mlp) proposes actions */
+    float learned_confidence;        /* 0.9: softmax probability needed to override the threshold rule */
+    int log_density;                 /* 1: keep the last control step's statistics (gsn_trainer_density_log) */
 } gsn_training_options;
 
 int gsn_training_options_default(gsn_training_options* out);
@@ -366,6 +369,34 @@ int gsn_graph_launches_per_step(gsn_graph* g, int* out);
  * (b: 64 x 128), all device pointers, operands rounded to bf16, accumulated in
  * fp32 tensor memory. Synchronises; GSN_ERR_TIMEOUT if the MMA did not finish. */
 int gsn_tc_gemm_selftest(const float* a, const float* b, float* d, void* stream);
+
+/* Learned density policy of the trainer: MLP weights (host, GSN_MLP_PARAMS
+ * floats; used when options.learned_density is set) and the log of the last
+ * density-control step (device pointers valid until the next step):
+ * features [before][16], decisions [before] (0 keep, 1 clone, 2 split,
+ * 3 prune), parents [after] (source index of each output Gaussian). */
+int gsn_trainer_set_density_mlp(gsn_trainer* t, const float* weights);
+int gsn_trainer_density_log(gsn_trainer* t, const float** features, const int8_t** decisions, const int** parents,
+                            int* before, int* after, int* steps, int* iteration);
+
+/* ------------------------------------------------------------------ learned density MLP
+ * gs-native extension: 16 statistics -> 64 -> 64 -> {keep, clone, split,
+ * prune}, ReLU, fp16 working weights, fp32 arithmetic; trained on the GPU by
+ * the library's own fused forward/backward kernels (full-batch Adam on the
+ * weighted mean cross-entropy). Device arrays: features [n][16] float, labels
+ * [n] int (0..3), sample weights [n] float, actions [n] int8, probs [n][4]. */
+#define GSN_MLP_PARAMS 5508
+typedef struct gsn_mlp gsn_mlp;
+int gsn_mlp_create(gsn_mlp** out);
+int gsn_mlp_destroy(gsn_mlp* m);
+int gsn_mlp_initialize(gsn_mlp* m, unsigned long long seed);
+int gsn_mlp_set_weights(gsn_mlp* m, const float* host_weights);
+int gsn_mlp_get_weights(gsn_mlp* m, float* host_weights);
+int gsn_mlp_gradients(gsn_mlp* m, const float* features, const int* labels, const float* weights, int n,
+                      float* host_grad, double* loss);
+int gsn_mlp_train(gsn_mlp* m, const float* features, const int* labels, const float* weights, int n, int steps,
+                  float lr, double* loss);
+int gsn_mlp_infer(gsn_mlp* m, const float* features, int n, float confidence, int8_t* actions, float* probs);
 
 /* ------------------------------------------------------------------ PLY
  * WriteGaussiansPly / ReadGaussiansPly (reference src/io/data_io.cpp:420-590)

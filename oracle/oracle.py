@@ -254,3 +254,53 @@ def knn3(points):
 
 def set_threads(k):
     return oracle().orc_set_threads(int(k))
+
+
+# ---------------------------------------------------------------- learned density MLP
+MLP_LAYOUT = dict(W1=(0, (64, 16)), b1=(1024, (64,)), W2=(1088, (64, 64)), b2=(5184, (64,)), W3=(5248, (4, 64)),
+                  b3=(5504, (4,)))
+
+
+def mlp_unpack(w):
+    w = np.asarray(w, dtype=np.float64)
+    return {k: w[o:o + int(np.prod(s))].reshape(s) for k, (o, s) in MLP_LAYOUT.items()}
+
+
+def mlp_forward(w, features):
+    """FP64 forward of the 16 -> 64 -> 64 -> 4 ReLU MLP: (z1, h1, z2, h2, logits)."""
+    p = mlp_unpack(w)
+    f = np.asarray(features, dtype=np.float64)
+    z1 = f @ p["W1"].T + p["b1"]
+    h1 = np.maximum(z1, 0.0)
+    z2 = h1 @ p["W2"].T + p["b2"]
+    h2 = np.maximum(z2, 0.0)
+    return z1, h1, z2, h2, h2 @ p["W3"].T + p["b3"]
+
+
+def mlp_loss_gradient(w, features, labels, sample_weights):
+    """FP64 loss and gradient of sum_i (w_i / sum w) * CE(softmax(MLP(f_i)), label_i),
+    the objective the GPU training kernels minimise; gradient in the flat weight
+    layout of MLP_LAYOUT."""
+    p = mlp_unpack(w)
+    f = np.asarray(features, dtype=np.float64)
+    z1, h1, z2, h2, lg = mlp_forward(w, f)
+    lg = lg - lg.max(axis=1, keepdims=True)
+    prob = np.exp(lg)
+    prob /= prob.sum(axis=1, keepdims=True)
+    nw = np.asarray(sample_weights, dtype=np.float64)
+    nw = nw / nw.sum()
+    idx = np.arange(f.shape[0])
+    labels = np.asarray(labels)
+    loss = -np.sum(nw * np.log(prob[idx, labels]))
+    dl = prob.copy()
+    dl[idx, labels] -= 1.0
+    dl *= nw[:, None]
+    g = {"W3": dl.T @ h2, "b3": dl.sum(0)}
+    dz2 = (dl @ p["W3"]) * (z2 > 0)
+    g["W2"], g["b2"] = dz2.T @ h1, dz2.sum(0)
+    dz1 = (dz2 @ p["W2"]) * (z1 > 0)
+    g["W1"], g["b1"] = dz1.T @ f, dz1.sum(0)
+    out = np.zeros(5508)
+    for k, (o, s) in MLP_LAYOUT.items():
+        out[o:o + int(np.prod(s))] = g[k].ravel()
+    return loss, out
