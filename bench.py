@@ -66,6 +66,7 @@ def parse():
                    help="warm-up steps plus one step on 3 views, no JSON (for ncu captures)")
     p.add_argument("--views", type=int, default=0, help="number of training views used (0 = all 180)")
     p.add_argument("--precision", action="store_true", help="with --profile-only: run the precision form")
+    p.add_argument("--no-multiview", action="store_true", help="skip the 32-view multi-view measurement")
     return p.parse_args()
 
 
@@ -202,6 +203,58 @@ def cpu_baseline(model, cam, target_u8, extent, steps=1, threads=None):
                        f"({t1 - t0} of {tiles_x * tiles_y} tiles), scaled by {1 / frac:.1f}; "
                        f"{steps} step(s), {sampled:.1f} s sampled CPU time per step"),
             "seconds_per_step": sec}
+
+
+def measure_multiview(gsn, torch, model, stream, sp, args, world):
+    """32 views of uneven resolution (640x480 ... 2560x1440, sphere of radius 10,
+    seed 23) of the 1.2M model: frames/s of the unbatched single-view path
+    (one Render per view, record count read back per view) against one
+    multi-view render (per-view ordering, one persistent blend launch) in the
+    configuration the autotuner picks on the same views."""
+    import scenes
+    cams = scenes.multiview_cameras(32, seed=23)
+    p = torch.from_numpy(model).cuda()
+    n = p.shape[1]
+    imgs = [torch.empty((c.height, c.width, 3), device="cuda") for c in cams]
+    ptrs = [x.data_ptr() for x in imgs]
+    reps = 3
+    single = gsn.Renderer()
+    single.set_stream(sp)
+
+    def unbatched():
+        for c, x in zip(cams, imgs):
+            assert single.render(p.data_ptr(), n, c, [0, 0, 0], x.data_ptr(), SH_DEGREE) == 0
+
+    mv = gsn.MultiView()
+    mv.set_stream(sp)
+    rows = mv.autotune(p.data_ptr(), n, cams, ptrs, [0, 0, 0], SH_DEGREE, repeats=2)
+
+    def batched():
+        mv.render(p.data_ptr(), n, cams, ptrs, [0, 0, 0], SH_DEGREE)
+
+    def time(fn):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    ms_single = time(unbatched)
+    ms_multi = time(batched)
+    sizes = {}
+    for c in cams:
+        sizes[f"{c.width}x{c.height}"] = sizes.get(f"{c.width}x{c.height}", 0) + 1
+    best = mv.config()
+    return {"views": len(cams), "resolutions": sizes, "gaussians": n,
+            "unbatched_frames_per_s": round(world * 1000.0 * len(cams) / ms_single, 2),
+            "batched_frames_per_s": round(world * 1000.0 * len(cams) / ms_multi, 2),
+            "speedup": round(ms_single / ms_multi, 3),
+            "config": {"tile_w": best[0], "tile_h": best[1], "threads": best[2], "key_bits": best[3]},
+            "autotune_ms": [[r["tile_w"], r["tile_h"], r["threads"], r["key_bits"], round(r["ms"], 3)] for r in rows]}
 
 
 def run_reference(args):
@@ -398,6 +451,7 @@ def run_gsn(args):
     value = plain_eager["value"]
     ms = plain_eager["ms_per_step"] * args.steps
     psnr = plain_eager["psnr_db_last_step"]
+    multiview = None if args.no_multiview else measure_multiview(gsn, torch, model, stream, sp, args, world)
 
     if rank != 0:
         if dist is not None:
@@ -458,6 +512,7 @@ def run_gsn(args):
         "roofline": roofline,
         "stages": stage_table,
         "stages_precision": {k: round(v, 4) for k, v in prec_stages.items()},
+        "multiview": multiview,
         "clocks": clocks,
         "cpu_baseline": cpu,
     }

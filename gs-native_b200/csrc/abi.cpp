@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <new>
 #include <string>
 #include <vector>
@@ -13,6 +14,7 @@
 #include "core/graph/training_graph.h"
 #include "io/ply.h"
 #include "core/knn/knn.h"
+#include "core/render/multiview_renderer.h"
 #include "core/render/renderer.h"
 #include "core/solver/solver.h"
 #include "kernels.h"
@@ -33,6 +35,10 @@ struct gsn_density {
 
 struct gsn_trainer {
     gs_native::GaussianSplatting impl;
+};
+
+struct gsn_multiview {
+    gs_native::MultiViewRenderer impl;
 };
 
 struct gsn_mlp {
@@ -733,6 +739,86 @@ int gsn_mlp_train(gsn_mlp* m, const float* features, const int* labels, const fl
 int gsn_mlp_infer(gsn_mlp* m, const float* features, int n, float confidence, int8_t* actions, float* probs) {
     if (!m) return GSN_ERR_INVALID_ARGUMENT;
     return m->impl.Infer(features, n, confidence, actions, probs) ? GSN_OK : GSN_ERR_INVALID_ARGUMENT;
+}
+
+// ---------------------------------------------------------------- multi-view renderer
+int gsn_multiview_create(gsn_multiview** out) {
+    if (!out) return GSN_ERR_INVALID_ARGUMENT;
+    *out = new (std::nothrow) gsn_multiview();
+    return *out ? GSN_OK : GSN_ERR_OUT_OF_MEMORY;
+}
+
+int gsn_multiview_destroy(gsn_multiview* m) {
+    delete m;
+    return GSN_OK;
+}
+
+int gsn_multiview_set_stream(gsn_multiview* m, void* stream) {
+    if (!m) return GSN_ERR_INVALID_ARGUMENT;
+    m->impl.SetStream(AsStream(stream));
+    return GSN_OK;
+}
+
+int gsn_multiview_set_config(gsn_multiview* m, int tile_w, int tile_h, int threads, int key_bits) {
+    if (!m) return GSN_ERR_INVALID_ARGUMENT;
+    return m->impl.SetConfig({tile_w, tile_h, threads, key_bits}) ? GSN_OK : GSN_ERR_INVALID_ARGUMENT;
+}
+
+int gsn_multiview_get_config(gsn_multiview* m, int* tile_w, int* tile_h, int* threads, int* key_bits) {
+    if (!m || !tile_w || !tile_h || !threads || !key_bits) return GSN_ERR_INVALID_ARGUMENT;
+    const gs_native::MultiViewConfig& c = m->impl.GetConfig();
+    *tile_w = c.tile_w;
+    *tile_h = c.tile_h;
+    *threads = c.threads;
+    *key_bits = c.key_bits;
+    return GSN_OK;
+}
+
+namespace {
+
+bool MultiViewInputs(const gsn_camera* cameras, int views, float* const* images,
+                     std::vector<gs_native::CameraParams>& cams, std::vector<float*>& imgs) {
+    if (!cameras || !images || views <= 0) return false;
+    cams.resize(static_cast<size_t>(views));
+    imgs.resize(static_cast<size_t>(views));
+    for (int k = 0; k < views; ++k) {
+        cams[k] = AsCamera(cameras + k);
+        imgs[k] = images[k];
+    }
+    return true;
+}
+
+}  // namespace
+
+int gsn_multiview_render(gsn_multiview* m, const float* params, int count, const gsn_camera* cameras, int views,
+                         float* const* images, const float* background, int sh_degree) {
+    std::vector<gs_native::CameraParams> cams;
+    std::vector<float*> imgs;
+    if (!m || !background || !MultiViewInputs(cameras, views, images, cams, imgs)) return GSN_ERR_INVALID_ARGUMENT;
+    return m->impl.Render(View(params, count), cams, background, imgs, sh_degree) ? GSN_OK
+                                                                                   : GSN_ERR_INVALID_ARGUMENT;
+}
+
+int gsn_multiview_autotune(gsn_multiview* m, const float* params, int count, const gsn_camera* cameras, int views,
+                           float* const* images, const float* background, int sh_degree, int repeats,
+                           float* results, int max_results, int* result_count) {
+    std::vector<gs_native::CameraParams> cams;
+    std::vector<float*> imgs;
+    if (!m || !background || !MultiViewInputs(cameras, views, images, cams, imgs)) return GSN_ERR_INVALID_ARGUMENT;
+    std::vector<gs_native::MultiViewTiming> timings;
+    if (!m->impl.Autotune(View(params, count), cams, background, imgs, sh_degree, repeats, &timings))
+        return GSN_ERR_CUDA;
+    const int rows = std::min(static_cast<int>(timings.size()), std::max(max_results, 0));
+    for (int k = 0; results && k < rows; ++k) {
+        const gs_native::MultiViewTiming& t = timings[k];
+        results[5 * k + 0] = static_cast<float>(t.config.tile_w);
+        results[5 * k + 1] = static_cast<float>(t.config.tile_h);
+        results[5 * k + 2] = static_cast<float>(t.config.threads);
+        results[5 * k + 3] = static_cast<float>(t.config.key_bits);
+        results[5 * k + 4] = static_cast<float>(t.ms);
+    }
+    if (result_count) *result_count = static_cast<int>(timings.size());
+    return GSN_OK;
 }
 
 }  // extern "C"

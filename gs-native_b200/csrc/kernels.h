@@ -61,6 +61,11 @@ struct ProjectOutputs {
 int launch_project(const float* params, int n, const gsn_camera& cam, const gsn_camera* cam_dev, int sh_degree,
                    bool bf16_sh, const ProjectOutputs& out, cudaStream_t stream);
 
+// Projection with a tile rectangle of tile_w x tile_h pixels (16x16, 16x8 or
+// 8x8; the camera's tile counts must match) - the multi-view renderer's sweep.
+int launch_project_tiled(const float* params, int n, const gsn_camera& cam, int tile_w, int tile_h, int sh_degree,
+                         const ProjectOutputs& out, cudaStream_t stream);
+
 // ---------------------------------------------------------------- sorting
 // Stable LSD radix sort of (uint32 key, uint32 value) pairs over key bits
 // [begin_bit, end_bit). Ping-pongs between (keys, values) and (keys_alt,

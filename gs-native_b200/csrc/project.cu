@@ -42,7 +42,9 @@ __device__ __forceinline__ void sh_basis(float x, float y, float z, float b[16])
 }
 
 // kBf16: precision form (bf16 SH rows; near-singular conics inverted in FP64).
-template <int D, bool kBf16>
+// TW x TH: tile shape of the rectangle (16 x 16, the reference's, everywhere but
+// the multi-view renderer's tile-shape sweep).
+template <int D, bool kBf16, int TW = kTile, int TH = kTile>
 __global__ void __launch_bounds__(256) project_kernel(const float* __restrict__ params,
                                                       gsn_camera cam_arg, const gsn_camera* __restrict__ cam_dev,
                                                       int n, ProjectOutputs out) {
@@ -120,10 +122,10 @@ __global__ void __launch_bounds__(256) project_kernel(const float* __restrict__ 
     float v = cam.fy * py / z + cam.cy;
     if (!isfinite(radius) || !isfinite(u) || !isfinite(v)) return;
     int4 rect;
-    rect.x = static_cast<int>(fminf(cam.tile_count_x, fmaxf(0.0f, (u - radius) / kTile)));
-    rect.y = static_cast<int>(fminf(cam.tile_count_y, fmaxf(0.0f, (v - radius) / kTile)));
-    rect.z = static_cast<int>(fminf(cam.tile_count_x, fmaxf(0.0f, (u + radius + kTile - 1) / kTile)));
-    rect.w = static_cast<int>(fminf(cam.tile_count_y, fmaxf(0.0f, (v + radius + kTile - 1) / kTile)));
+    rect.x = static_cast<int>(fminf(cam.tile_count_x, fmaxf(0.0f, (u - radius) / TW)));
+    rect.y = static_cast<int>(fminf(cam.tile_count_y, fmaxf(0.0f, (v - radius) / TH)));
+    rect.z = static_cast<int>(fminf(cam.tile_count_x, fmaxf(0.0f, (u + radius + TW - 1) / TW)));
+    rect.w = static_cast<int>(fminf(cam.tile_count_y, fmaxf(0.0f, (v + radius + TH - 1) / TH)));
     if (rect.x >= rect.z || rect.y >= rect.w) return;
 
     out.depths[i] = z;
@@ -174,6 +176,29 @@ void launch_project_layout(const float* params, int n, const gsn_camera& cam, co
 }
 
 }  // namespace
+
+template <int TW, int TH>
+static void launch_project_tiles(const float* params, int n, const gsn_camera& cam, int d, const ProjectOutputs& out,
+                          cudaStream_t stream) {
+    dim3 grid(ceil_div(n, 256));
+    switch (d) {
+        case 0: project_kernel<0, false, TW, TH><<<grid, 256, 0, stream>>>(params, cam, nullptr, n, out); break;
+        case 1: project_kernel<1, false, TW, TH><<<grid, 256, 0, stream>>>(params, cam, nullptr, n, out); break;
+        case 2: project_kernel<2, false, TW, TH><<<grid, 256, 0, stream>>>(params, cam, nullptr, n, out); break;
+        default: project_kernel<3, false, TW, TH><<<grid, 256, 0, stream>>>(params, cam, nullptr, n, out); break;
+    }
+}
+
+int launch_project_tiled(const float* params, int n, const gsn_camera& cam, int tile_w, int tile_h, int sh_degree,
+                         const ProjectOutputs& out, cudaStream_t stream) {
+    if (n <= 0) return GSN_OK;
+    const int d = sh_degree < 0 ? 0 : (sh_degree > 3 ? 3 : sh_degree);
+    if (tile_w == 16 && tile_h == 16) launch_project_tiles<16, 16>(params, n, cam, d, out, stream);
+    else if (tile_w == 16 && tile_h == 8) launch_project_tiles<16, 8>(params, n, cam, d, out, stream);
+    else if (tile_w == 8 && tile_h == 8) launch_project_tiles<8, 8>(params, n, cam, d, out, stream);
+    else return GSN_ERR_INVALID_ARGUMENT;
+    return launched(1);
+}
 
 int launch_project(const float* params, int n, const gsn_camera& cam, const gsn_camera* cam_dev, int sh_degree,
                    bool bf16_sh, const ProjectOutputs& out, cudaStream_t stream) {

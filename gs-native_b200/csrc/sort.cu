@@ -327,7 +327,7 @@ __global__ void __launch_bounds__(256) emit_records(const uint32_t* __restrict__
     const int count = record_start[p + 1] - begin;
     if (count <= 0) return;
     if (begin + static_cast<int64_t>(count) > capacity) {
-        if (sub == 0) atomicExch(overflow, 1);
+        if (sub == 0 && overflow) atomicExch(overflow, 1);
         return;
     }
     const uint32_t id = sorted_ids[p];

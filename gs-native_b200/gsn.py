@@ -727,3 +727,70 @@ class Mlp:
     def infer(self, features_ptr, n, confidence, actions_ptr, probs_ptr=0):
         _check(lib().gsn_mlp_infer(self.handle, ctypes.c_void_p(features_ptr), int(n), float(confidence),
                                    ctypes.c_void_p(actions_ptr), ctypes.c_void_p(probs_ptr or None)), "infer")
+
+
+class MultiView:
+    """Multi-view renderer with one persistent blend launch and its autotuner
+    (include/gsn.h "multi-view renderer")."""
+
+    def __init__(self):
+        L = lib()
+        vp, i32, P = ctypes.c_void_p, ctypes.c_int, ctypes.POINTER
+        sigs = {
+            "gsn_multiview_create": [P(vp)], "gsn_multiview_destroy": [vp], "gsn_multiview_set_stream": [vp, vp],
+            "gsn_multiview_set_config": [vp, i32, i32, i32, i32],
+            "gsn_multiview_get_config": [vp, P(i32), P(i32), P(i32), P(i32)],
+            "gsn_multiview_render": [vp, vp, i32, P(Camera), i32, P(vp), c_float_p, i32],
+            "gsn_multiview_autotune": [vp, vp, i32, P(Camera), i32, P(vp), c_float_p, i32, i32, c_float_p, i32,
+                                       P(i32)],
+        }
+        for name, args in sigs.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = i32
+        h = ctypes.c_void_p()
+        _check(L.gsn_multiview_create(ctypes.byref(h)), "gsn_multiview_create")
+        self.handle = h
+
+    def close(self):
+        if self.handle:
+            lib().gsn_multiview_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream):
+        _check(lib().gsn_multiview_set_stream(self.handle, ctypes.c_void_p(stream)), "set_stream")
+
+    def set_config(self, tile_w=16, tile_h=16, threads=64, key_bits=32):
+        _check(lib().gsn_multiview_set_config(self.handle, tile_w, tile_h, threads, key_bits), "set_config")
+
+    def config(self):
+        v = [ctypes.c_int() for _ in range(4)]
+        _check(lib().gsn_multiview_get_config(self.handle, *[ctypes.byref(x) for x in v]), "get_config")
+        return tuple(x.value for x in v)
+
+    @staticmethod
+    def _inputs(cameras, image_ptrs):
+        cams = (Camera * len(cameras))(*cameras)
+        imgs = (ctypes.c_void_p * len(image_ptrs))(*[ctypes.c_void_p(p) for p in image_ptrs])
+        return cams, imgs
+
+    def render(self, params_ptr, count, cameras, image_ptrs, background, sh_degree):
+        cams, imgs = self._inputs(cameras, image_ptrs)
+        _check(lib().gsn_multiview_render(self.handle, ctypes.c_void_p(params_ptr), int(count), cams, len(cameras),
+                                          imgs, floats3(background), int(sh_degree)), "multiview_render")
+
+    def autotune(self, params_ptr, count, cameras, image_ptrs, background, sh_degree, repeats=2):
+        cams, imgs = self._inputs(cameras, image_ptrs)
+        res = (ctypes.c_float * (5 * 64))()
+        n = ctypes.c_int()
+        _check(lib().gsn_multiview_autotune(self.handle, ctypes.c_void_p(params_ptr), int(count), cams, len(cameras),
+                                            imgs, floats3(background), int(sh_degree), int(repeats), res, 64,
+                                            ctypes.byref(n)), "multiview_autotune")
+        return [dict(tile_w=int(res[5 * k]), tile_h=int(res[5 * k + 1]), threads=int(res[5 * k + 2]),
+                     key_bits=int(res[5 * k + 3]), ms=float(res[5 * k + 4])) for k in range(min(n.value, 64))]

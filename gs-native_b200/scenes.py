@@ -131,6 +131,24 @@ def ring_cameras(count, radius, elevation_deg, width, height, fx, fy, seed=None)
     return cams
 
 
+MULTIVIEW_SIZES = ((640, 480), (1280, 720), (1600, 1064), (2048, 1360), (2560, 1440))
+
+
+def multiview_cameras(count=32, seed=23, radius=10.0, sizes=MULTIVIEW_SIZES):
+    """Views of uneven resolution: sizes drawn uniformly from `sizes`, positions
+    uniform on a sphere of `radius` looking at the origin, fx = fy = 0.875 * width
+    (the 1600-pixel ring cameras' 1400 / 1600)."""
+    rng = np.random.default_rng(seed)
+    cams = []
+    for _ in range(count):
+        w, h = sizes[int(rng.integers(0, len(sizes)))]
+        d = rng.normal(size=3)
+        d /= np.linalg.norm(d)
+        R, t = look_at(radius * d)
+        cams.append(pinhole(w, h, 0.875 * w, 0.875 * w, R, t))
+    return cams
+
+
 def training_scene_cameras(count=200, held_out_every=10):
     """Ring of 200 cameras, radius 8, elevation +/-15 deg, 1600x1064, fx=fy=1400;
     every tenth camera is held out (180 train / 20 test)."""

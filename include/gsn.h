@@ -363,6 +363,27 @@ int gsn_graph_run(gsn_graph* g, const int* views, const float* position_lrs, int
 int gsn_graph_check(gsn_graph* g);
 int gsn_graph_launches_per_step(gsn_graph* g, int* out);
 
+/* ------------------------------------------------------------------ multi-view renderer
+ * gs-native extension: `count` cameras of any resolutions rendered into device
+ * fp32 HWC images (images[v] points at width * height * 3 floats) with one
+ * persistent blend launch over all (view, tile) work items. Configuration:
+ * tile 16x16, 16x8 or 8x8; 64, 128 or 256 threads per tile (at least one
+ * pixel row per thread); sort key width 32 (depth pre-sort + tile bits), 48
+ * (tile|depth over 32 + log2 T bits) or 64. gsn_multiview_autotune times every
+ * valid configuration on the given views, keeps the fastest and writes up to
+ * max_results rows of {tile_w, tile_h, threads, key_bits, ms} to results. */
+typedef struct gsn_multiview gsn_multiview;
+int gsn_multiview_create(gsn_multiview** out);
+int gsn_multiview_destroy(gsn_multiview* m);
+int gsn_multiview_set_stream(gsn_multiview* m, void* stream);
+int gsn_multiview_set_config(gsn_multiview* m, int tile_w, int tile_h, int threads, int key_bits);
+int gsn_multiview_get_config(gsn_multiview* m, int* tile_w, int* tile_h, int* threads, int* key_bits);
+int gsn_multiview_render(gsn_multiview* m, const float* params, int count, const gsn_camera* cameras, int views,
+                         float* const* images, const float* background, int sh_degree);
+int gsn_multiview_autotune(gsn_multiview* m, const float* params, int count, const gsn_camera* cameras, int views,
+                           float* const* images, const float* background, int sh_degree, int repeats,
+                           float* results, int max_results, int* result_count);
+
 /* ------------------------------------------------------------------ tensor cores
  * Self-test of the tcgen05 path used by the precision form's SSIM filter
  * (gs-native extension): d (128 x 64 fp32, row-major) = a (128 x 128) * b^T
