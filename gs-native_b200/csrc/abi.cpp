@@ -12,6 +12,8 @@
 #include "core/density/density_mlp.h"
 #include "core/gaussian_splatting.h"
 #include "core/graph/training_graph.h"
+#include "io/colmap.h"
+#include "io/image.h"
 #include "io/ply.h"
 #include "core/knn/knn.h"
 #include "core/render/multiview_renderer.h"
@@ -575,6 +577,18 @@ int gsn_trainer_evaluate(gsn_trainer* t, const gsn_camera* cameras, const uint8_
     return t->impl.Evaluate(cams, imgs, psnr, loss) ? GSN_OK : GSN_ERR_INVALID_ARGUMENT;
 }
 
+int gsn_trainer_evaluate_metrics(gsn_trainer* t, const gsn_camera* cameras, const uint8_t* const* images, int count,
+                                 double* psnr, double* ssim, double* l1, double* loss) {
+    if (!t || !cameras || !images || count <= 0) return GSN_ERR_INVALID_ARGUMENT;
+    std::vector<gs_native::CameraParams> cams;
+    std::vector<const uint8_t*> imgs;
+    for (int k = 0; k < count; ++k) {
+        cams.push_back(AsCamera(cameras + k));
+        imgs.push_back(images[k]);
+    }
+    return t->impl.EvaluateMetrics(cams, imgs, psnr, ssim, l1, loss) ? GSN_OK : GSN_ERR_INVALID_ARGUMENT;
+}
+
 int gsn_trainer_save(gsn_trainer* t, const char* path) {
     if (!t || !path) return GSN_ERR_INVALID_ARGUMENT;
     return t->impl.Save(path) ? GSN_OK : GSN_ERR_IO;
@@ -679,6 +693,16 @@ int gsn_tc_gemm_selftest(const float* a, const float* b, float* d, void* stream)
 }
 
 // ---------------------------------------------------------------- learned density
+int gsn_trainer_save_checkpoint(gsn_trainer* t, const char* path) {
+    if (!t || !path) return GSN_ERR_INVALID_ARGUMENT;
+    return t->impl.SaveCheckpoint(path) ? GSN_OK : GSN_ERR_IO;
+}
+
+int gsn_trainer_load_checkpoint(gsn_trainer* t, const char* path) {
+    if (!t || !path) return GSN_ERR_INVALID_ARGUMENT;
+    return t->impl.LoadCheckpoint(path) ? GSN_OK : GSN_ERR_IO;
+}
+
 int gsn_trainer_set_density_mlp(gsn_trainer* t, const float* weights) {
     if (!t || !weights) return GSN_ERR_INVALID_ARGUMENT;
     return t->impl.SetDensityMlp(weights) ? GSN_OK : GSN_ERR_CUDA;
@@ -819,6 +843,76 @@ int gsn_multiview_autotune(gsn_multiview* m, const float* params, int count, con
     }
     if (result_count) *result_count = static_cast<int>(timings.size());
     return GSN_OK;
+}
+
+struct gsn_scene {
+    gs_native::ColmapScene impl;
+};
+
+int gsn_scene_read_colmap(const char* scene_dir, int downscale, gsn_scene** out) {
+    if (!scene_dir || !out) return GSN_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    gsn_scene* s = new (std::nothrow) gsn_scene;
+    if (!s) return GSN_ERR_OUT_OF_MEMORY;
+    if (!gs_native::ReadColmapScene(scene_dir, downscale, s->impl)) {
+        delete s;
+        return GSN_ERR_IO;
+    }
+    *out = s;
+    return GSN_OK;
+}
+
+int gsn_scene_destroy(gsn_scene* s) {
+    delete s;
+    return GSN_OK;
+}
+
+int gsn_scene_counts(const gsn_scene* s, int* train, int* test, int* points) {
+    if (!s) return GSN_ERR_INVALID_ARGUMENT;
+    if (train) *train = static_cast<int>(s->impl.train_cameras.size());
+    if (test) *test = static_cast<int>(s->impl.test_cameras.size());
+    if (points) *points = static_cast<int>(s->impl.point_positions.size() / 3);
+    return GSN_OK;
+}
+
+int gsn_scene_view(const gsn_scene* s, int split, int index, gsn_camera* camera, const uint8_t** image,
+                   const char** name) {
+    if (!s || (split != 0 && split != 1)) return GSN_ERR_INVALID_ARGUMENT;
+    const auto& cams = split == 0 ? s->impl.train_cameras : s->impl.test_cameras;
+    const auto& imgs = split == 0 ? s->impl.train_images : s->impl.test_images;
+    const auto& names = split == 0 ? s->impl.train_names : s->impl.test_names;
+    if (index < 0 || index >= static_cast<int>(cams.size())) return GSN_ERR_INVALID_ARGUMENT;
+    if (camera) *camera = gs_native::AsGsnCamera(cams[index]);
+    if (image) *image = imgs[index].rgb.data();
+    if (name) *name = names[index].c_str();
+    return GSN_OK;
+}
+
+int gsn_scene_points(const gsn_scene* s, const float** positions, const float** colors) {
+    if (!s) return GSN_ERR_INVALID_ARGUMENT;
+    if (positions) *positions = s->impl.point_positions.data();
+    if (colors) *colors = s->impl.point_colors.data();
+    return GSN_OK;
+}
+
+static bool AsImage(const uint8_t* rgb, int width, int height, gs_native::ImageU8& image) {
+    if (!rgb || width <= 0 || height <= 0) return false;
+    image.width = width;
+    image.height = height;
+    image.rgb.assign(rgb, rgb + static_cast<size_t>(width) * height * 3);
+    return true;
+}
+
+int gsn_image_write_ppm(const char* path, const uint8_t* rgb, int width, int height) {
+    gs_native::ImageU8 image;
+    if (!path || !AsImage(rgb, width, height, image)) return GSN_ERR_INVALID_ARGUMENT;
+    return gs_native::WritePpm(path, image) ? GSN_OK : GSN_ERR_IO;
+}
+
+int gsn_image_write_png(const char* path, const uint8_t* rgb, int width, int height) {
+    gs_native::ImageU8 image;
+    if (!path || !AsImage(rgb, width, height, image)) return GSN_ERR_INVALID_ARGUMENT;
+    return gs_native::WritePng(path, image) ? GSN_OK : GSN_ERR_IO;
 }
 
 }  // extern "C"

@@ -464,6 +464,9 @@ class Trainer:
             "gsn_trainer_save": [vp, ctypes.c_char_p], "gsn_trainer_load": [vp, ctypes.c_char_p],
             "gsn_trainer_state": [vp, P(vp), P(i32), P(i32), P(i32), P(ctypes.c_float)],
             "gsn_trainer_set_density_mlp": [vp, P(ctypes.c_float)],
+            "gsn_trainer_save_checkpoint": [vp, ctypes.c_char_p], "gsn_trainer_load_checkpoint": [vp, ctypes.c_char_p],
+            "gsn_trainer_evaluate_metrics": [vp, P(Camera), P(vp), i32, P(ctypes.c_double), P(ctypes.c_double),
+                                             P(ctypes.c_double), P(ctypes.c_double)],
             "gsn_trainer_density_log": [vp, P(vp), P(vp), P(vp), P(i32), P(i32), P(i32), P(i32)],
         }
         for name, args in sigs.items():
@@ -517,6 +520,14 @@ class Trainer:
         _check(lib().gsn_trainer_evaluate(self.handle, cams, ptrs, len(cameras), ctypes.byref(psnr),
                                           ctypes.byref(loss)), "evaluate")
         return psnr.value, loss.value
+
+    def evaluate_metrics(self, cameras, images):
+        """Mean FP64 PSNR, SSIM, L1 and loss over the views."""
+        cams, ptrs, keep = self._views(cameras, images)
+        out = [ctypes.c_double() for _ in range(4)]
+        _check(lib().gsn_trainer_evaluate_metrics(self.handle, cams, ptrs, len(cameras), *[ctypes.byref(o) for o in out]),
+               "evaluate_metrics")
+        return dict(psnr=out[0].value, ssim=out[1].value, l1=out[2].value, loss=out[3].value)
 
     def save(self, path):
         return lib().gsn_trainer_save(self.handle, str(path).encode())
@@ -656,6 +667,8 @@ def _trainer_density_log(self):
 
 
 Trainer.set_density_mlp = _trainer_set_density_mlp
+Trainer.save_checkpoint = lambda self, path: lib().gsn_trainer_save_checkpoint(self.handle, str(path).encode())
+Trainer.load_checkpoint = lambda self, path: lib().gsn_trainer_load_checkpoint(self.handle, str(path).encode())
 Trainer.density_log = _trainer_density_log
 
 MLP_PARAMS = 5508
@@ -794,3 +807,60 @@ class MultiView:
                                             ctypes.byref(n)), "multiview_autotune")
         return [dict(tile_w=int(res[5 * k]), tile_h=int(res[5 * k + 1]), threads=int(res[5 * k + 2]),
                      key_bits=int(res[5 * k + 3]), ms=float(res[5 * k + 4])) for k in range(min(n.value, 64))]
+
+
+class ColmapScene:
+    """COLMAP scene read without OpenCV (include/gsn.h "COLMAP scene"): train /
+    test cameras (Camera), host u8 HWC images (numpy views copied out), image
+    names and the sparse point cloud."""
+
+    def __init__(self, scene_dir, downscale=1):
+        import numpy as np
+        vp, i32, P = ctypes.c_void_p, ctypes.c_int, ctypes.POINTER
+        read = declare("gsn_scene_read_colmap", [ctypes.c_char_p, i32, P(vp)])
+        counts = declare("gsn_scene_counts", [vp, P(i32), P(i32), P(i32)])
+        view = declare("gsn_scene_view", [vp, i32, i32, P(Camera), P(ctypes.POINTER(ctypes.c_uint8)),
+                                          P(ctypes.c_char_p)])
+        points = declare("gsn_scene_points", [vp, P(c_float_p), P(c_float_p)])
+        destroy = declare("gsn_scene_destroy", [vp])
+        handle = vp()
+        _check(read(str(scene_dir).encode(), int(downscale), ctypes.byref(handle)), "scene_read_colmap")
+        try:
+            n = [ctypes.c_int() for _ in range(3)]
+            _check(counts(handle, *[ctypes.byref(x) for x in n]), "scene_counts")
+            self.train_cameras, self.test_cameras = [], []
+            self.train_images, self.test_images = [], []
+            self.train_names, self.test_names = [], []
+            for split, (cams, imgs, names) in enumerate(
+                    [(self.train_cameras, self.train_images, self.train_names),
+                     (self.test_cameras, self.test_images, self.test_names)]):
+                for k in range(n[split].value):
+                    cam, img, name = Camera(), ctypes.POINTER(ctypes.c_uint8)(), ctypes.c_char_p()
+                    _check(view(handle, split, k, ctypes.byref(cam), ctypes.byref(img), ctypes.byref(name)),
+                           "scene_view")
+                    cams.append(cam)
+                    imgs.append(np.ctypeslib.as_array(img, shape=(cam.height, cam.width, 3)).copy())
+                    names.append(name.value.decode())
+            pos, col = c_float_p(), c_float_p()
+            _check(points(handle, ctypes.byref(pos), ctypes.byref(col)), "scene_points")
+            m = n[2].value
+            self.points = np.ctypeslib.as_array(pos, shape=(m, 3)).copy() if m else np.zeros((0, 3), np.float32)
+            self.colors = np.ctypeslib.as_array(col, shape=(m, 3)).copy() if m else np.zeros((0, 3), np.float32)
+        finally:
+            destroy(handle)
+
+
+def write_png(path, rgb):
+    """8-bit RGB PNG (HWC uint8 array)."""
+    import numpy as np
+    a = np.ascontiguousarray(rgb, dtype=np.uint8)
+    fn = declare("gsn_image_write_png", [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int])
+    return fn(str(path).encode(), ctypes.c_void_p(a.ctypes.data), a.shape[1], a.shape[0])
+
+
+def write_ppm(path, rgb):
+    """Binary PPM (P6) of an HWC uint8 array."""
+    import numpy as np
+    a = np.ascontiguousarray(rgb, dtype=np.uint8)
+    fn = declare("gsn_image_write_ppm", [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int])
+    return fn(str(path).encode(), ctypes.c_void_p(a.ctypes.data), a.shape[1], a.shape[0])

@@ -9,6 +9,7 @@
 #include <cmath>
 #include <limits>
 #include <numeric>
+#include <fstream>
 #include <random>
 
 #include "core/knn/knn.h"
@@ -326,8 +327,15 @@ bool GaussianSplatting::Render(const CameraParams& camera, float* device_image) 
 
 bool GaussianSplatting::Evaluate(const std::vector<CameraParams>& cameras, const std::vector<const uint8_t*>& images,
                                  double* psnr, double* loss) {
-    if (!psnr || cameras.size() != images.size() || cameras.empty() || !gaussians_.gaussians_) return false;
-    double sum_psnr = 0.0, sum_loss = 0.0;
+    if (!psnr) return false;
+    return EvaluateMetrics(cameras, images, psnr, nullptr, nullptr, loss);
+}
+
+bool GaussianSplatting::EvaluateMetrics(const std::vector<CameraParams>& cameras,
+                                        const std::vector<const uint8_t*>& images, double* psnr, double* ssim,
+                                        double* l1, double* loss) {
+    if (cameras.size() != images.size() || cameras.empty() || !gaussians_.gaussians_) return false;
+    double sums[4] = {0.0, 0.0, 0.0, 0.0};  // loss, L1, SSIM, PSNR
     DeviceArray<uint8_t> target;
     DeviceArray<float> image;
     Solver metric;
@@ -345,11 +353,13 @@ bool GaussianSplatting::Evaluate(const std::vector<CameraParams>& cameras, const
                 cudaSuccess ||
             cudaStreamSynchronize(stream_) != cudaSuccess)
             return false;
-        sum_loss += out[0];
-        sum_psnr += out[3];
+        for (int q = 0; q < 4; ++q) sums[q] += out[q];
     }
-    *psnr = sum_psnr / cameras.size();
-    if (loss) *loss = sum_loss / cameras.size();
+    const double n = static_cast<double>(cameras.size());
+    if (loss) *loss = sums[0] / n;
+    if (l1) *l1 = sums[1] / n;
+    if (ssim) *ssim = sums[2] / n;
+    if (psnr) *psnr = sums[3] / n;
     return true;
 }
 
@@ -366,6 +376,121 @@ bool GaussianSplatting::Load(const std::string& path) {
     if (!ReadGaussiansPly(path, g)) return false;
     std::vector<float> p = PackGaussians(g);
     return SetParameters(p.data(), static_cast<int>(g.size()));
+}
+
+namespace {
+
+constexpr char kCheckpointMagic[8] = {'G', 'S', 'N', 'C', 'K', 'P', 'T', '1'};
+constexpr uint32_t kCheckpointVersion = 1;
+
+struct CheckpointHeader {
+    char magic[8];
+    uint32_t version;
+    uint32_t bf16_sh;
+    int32_t count;
+    int32_t rows;
+    int32_t completed;
+    int32_t sh_degree;
+    uint64_t adam_step;
+    int32_t camera_cursor;
+    int32_t camera_count;
+    float scene_extent;
+    float scene_centre[3];
+};
+
+template <typename T>
+bool Download(std::vector<T>& host, const T* device, size_t count) {
+    host.resize(count);
+    return count == 0 || cudaMemcpy(host.data(), device, count * sizeof(T), cudaMemcpyDeviceToHost) == cudaSuccess;
+}
+
+template <typename T>
+bool Upload(T* device, const std::vector<T>& host) {
+    return host.empty() || cudaMemcpy(device, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice) ==
+                               cudaSuccess;
+}
+
+}  // namespace
+
+bool GaussianSplatting::SaveCheckpoint(const std::string& path) {
+    const int count = gaussians_.gaussian_count_;
+    if (!gaussians_.gaussians_ || count <= 0 || cudaStreamSynchronize(stream_) != cudaSuccess) return false;
+    const size_t rows = PhysicalRows(), n = static_cast<size_t>(count);
+    CheckpointHeader h{};
+    std::memcpy(h.magic, kCheckpointMagic, sizeof(h.magic));
+    h.version = kCheckpointVersion;
+    h.bf16_sh = options_.bf16_sh ? 1u : 0u;
+    h.count = count;
+    h.rows = static_cast<int32_t>(rows);
+    h.completed = completed_;
+    h.sh_degree = sh_degree_;
+    h.adam_step = solver_.GetIteration();
+    h.camera_cursor = camera_cursor_;
+    h.camera_count = static_cast<int32_t>(camera_order_.size());
+    h.scene_extent = scene_extent_;
+    for (int a = 0; a < 3; ++a) h.scene_centre[a] = scene_centre_[a];
+    std::vector<float> block, m, v, sums, abs_sums;
+    std::vector<unsigned int> obs;
+    if (!Download(block, gaussians_.gaussians_, rows * n) || !Download(m, solver_.GetFirstMoments(), rows * n) ||
+        !Download(v, solver_.GetSecondMoments(), rows * n) ||
+        !Download(sums, static_cast<const float*>(density_.GetGradientSums()), n) ||
+        !Download(abs_sums, static_cast<const float*>(density_.GetAbsoluteGradientSums()), n) ||
+        !Download(obs, static_cast<const unsigned int*>(density_.GetObservationCounts()), n))
+        return false;
+    std::ofstream out(path, std::ios::binary);
+    if (!out) return false;
+    out.write(reinterpret_cast<const char*>(&h), sizeof(h));
+    out.write(reinterpret_cast<const char*>(camera_order_.data()), camera_order_.size() * sizeof(int));
+    for (const std::vector<float>* a : {&block, &m, &v, &sums, &abs_sums})
+        out.write(reinterpret_cast<const char*>(a->data()), a->size() * sizeof(float));
+    out.write(reinterpret_cast<const char*>(obs.data()), obs.size() * sizeof(unsigned int));
+    return static_cast<bool>(out);
+}
+
+bool GaussianSplatting::LoadCheckpoint(const std::string& path) {
+    if (cameras_.empty()) return false;
+    std::ifstream in(path, std::ios::binary);
+    CheckpointHeader h{};
+    if (!in || !in.read(reinterpret_cast<char*>(&h), sizeof(h)) ||
+        std::memcmp(h.magic, kCheckpointMagic, sizeof(h.magic)) != 0 || h.version != kCheckpointVersion ||
+        h.bf16_sh != (options_.bf16_sh ? 1u : 0u) || h.count <= 0 || h.rows != static_cast<int32_t>(PhysicalRows()) ||
+        h.camera_count != static_cast<int32_t>(cameras_.size()) || h.camera_cursor < 0 ||
+        h.camera_cursor > h.camera_count)
+        return false;
+    const size_t rows = PhysicalRows(), n = static_cast<size_t>(h.count);
+    std::vector<int> order(static_cast<size_t>(h.camera_count));
+    std::vector<float> block(rows * n), m(rows * n), v(rows * n), sums(n), abs_sums(n);
+    std::vector<unsigned int> obs(n);
+    in.read(reinterpret_cast<char*>(order.data()), order.size() * sizeof(int));
+    for (std::vector<float>* a : {&block, &m, &v, &sums, &abs_sums})
+        in.read(reinterpret_cast<char*>(a->data()), a->size() * sizeof(float));
+    in.read(reinterpret_cast<char*>(obs.data()), obs.size() * sizeof(unsigned int));
+    if (!in) return false;
+    for (int k : order)
+        if (k < 0 || k >= h.camera_count) return false;
+    void* dev = nullptr;
+    if (DeviceAlloc(&dev, block.size() * sizeof(float)) != cudaSuccess) return false;
+    if (!Upload(static_cast<float*>(dev), block) || !density_.Initialize(h.count, h.count) ||
+        !solver_.RemapGaussians(nullptr, h.count)) {
+        cudaFree(dev);
+        return false;
+    }
+    graph_.Release();
+    cudaFree(gaussians_.gaussians_);
+    gaussians_.gaussians_ = static_cast<float*>(dev);
+    gaussians_.gaussian_count_ = h.count;
+    if (!Upload(solver_.GetFirstMoments(), m) || !Upload(solver_.GetSecondMoments(), v) ||
+        !Upload(density_.GetGradientSums(), sums) || !Upload(density_.GetAbsoluteGradientSums(), abs_sums) ||
+        !Upload(density_.GetObservationCounts(), obs))
+        return false;
+    solver_.SetIteration(h.adam_step);
+    completed_ = h.completed;
+    sh_degree_ = h.sh_degree;
+    camera_order_ = order;
+    camera_cursor_ = h.camera_cursor;
+    scene_extent_ = h.scene_extent;
+    for (int a = 0; a < 3; ++a) scene_centre_[a] = h.scene_centre[a];
+    return cudaDeviceSynchronize() == cudaSuccess;
 }
 
 }  // namespace gs_native

@@ -103,6 +103,10 @@ public:
     // (host u8 HWC images).
     bool Evaluate(const std::vector<CameraParams>& cameras, const std::vector<const uint8_t*>& images, double* psnr,
                   double* loss = nullptr);
+    // Mean FP64 PSNR (dB), SSIM (11x11 Gaussian window, as the loss), L1 and
+    // loss over the views; any output may be null.
+    bool EvaluateMetrics(const std::vector<CameraParams>& cameras, const std::vector<const uint8_t*>& images,
+                         double* psnr, double* ssim, double* l1, double* loss);
 
     void SetStream(cudaStream_t stream);
     const GaussianBuffers& GetGaussians() const { return gaussians_; }
@@ -113,6 +117,12 @@ public:
     Solver& GetSolver() { return solver_; }
     DensityController& GetDensity() { return density_; }
     const TrainingOptions& GetOptions() const { return options_; }
+    // Resumable checkpoint: parameters in their stored layout, Adam moments and
+    // step, the round's density statistics, iteration, camera order and cursor
+    // (the reference has none). Load requires Initialize() with the same scene
+    // first (the targets are not stored) and the same layout option.
+    bool SaveCheckpoint(const std::string& path);
+    bool LoadCheckpoint(const std::string& path);
     // Weights of the learned density policy (DensityMlp::kParams floats, host).
     bool SetDensityMlp(const float* weights);
     const DensityLog& GetDensityLog() const { return density_log_; }

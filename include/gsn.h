@@ -330,6 +330,10 @@ int gsn_trainer_render(gsn_trainer* t, const gsn_camera* camera, float* image);
 /* Mean PSNR / loss over views with host u8 HWC images (FP64 reductions). */
 int gsn_trainer_evaluate(gsn_trainer* t, const gsn_camera* cameras, const uint8_t* const* images, int count,
                          double* psnr, double* loss);
+/* Mean FP64 PSNR (dB), SSIM (11x11 window), L1 and loss over held-out views
+ * (host u8 HWC images); outputs may be null. gs-native extension. */
+int gsn_trainer_evaluate_metrics(gsn_trainer* t, const gsn_camera* cameras, const uint8_t* const* images, int count,
+                                 double* psnr, double* ssim, double* l1, double* loss);
 /* Save to / load from a Gaussian PLY (gaussian_splatting.cpp:234-260). */
 int gsn_trainer_save(gsn_trainer* t, const char* path);
 int gsn_trainer_load(gsn_trainer* t, const char* path);
@@ -391,6 +395,12 @@ int gsn_multiview_autotune(gsn_multiview* m, const float* params, int count, con
  * fp32 tensor memory. Synchronises; GSN_ERR_TIMEOUT if the MMA did not finish. */
 int gsn_tc_gemm_selftest(const float* a, const float* b, float* d, void* stream);
 
+/* Resumable checkpoint (gs-native extension): parameters in their stored
+ * layout, Adam moments and step, density statistics, iteration, camera order
+ * and cursor. Load after gsn_trainer_initialize with the same scene/options. */
+int gsn_trainer_save_checkpoint(gsn_trainer* t, const char* path);
+int gsn_trainer_load_checkpoint(gsn_trainer* t, const char* path);
+
 /* Learned density policy of the trainer: MLP weights (host, GSN_MLP_PARAMS
  * floats; used when options.learned_density is set) and the log of the last
  * density-control step (device pointers valid until the next step):
@@ -425,6 +435,25 @@ int gsn_mlp_infer(gsn_mlp* m, const float* features, int n, float confidence, in
 int gsn_ply_write(const char* path, const float* params, int count);
 int gsn_ply_read_count(const char* path, int* count);
 int gsn_ply_read(const char* path, float* params, int count);
+
+/* ------------------------------------------------------------------ COLMAP scene
+ * ReadColmapScene (reference src/io/data_io.cpp:328-418) without OpenCV:
+ * sparse/0/{cameras,images,points3D}.bin (one PINHOLE camera), images
+ * pre-decoded to binary PPM (P6) under images/ (images/<name> when it is a PPM,
+ * else images/<name without extension>.ppm), integer downscale by block
+ * averaging. Images sorted by name; every 8th is a test view. Cameras carry
+ * near 0.2, far FLT_MAX and 16x16 tiles. split: 0 train, 1 test. Image
+ * pointers are host u8 HWC and live as long as the scene. */
+typedef struct gsn_scene gsn_scene;
+int gsn_scene_read_colmap(const char* scene_dir, int downscale, gsn_scene** out);
+int gsn_scene_destroy(gsn_scene* s);
+int gsn_scene_counts(const gsn_scene* s, int* train, int* test, int* points);
+int gsn_scene_view(const gsn_scene* s, int split, int index, gsn_camera* camera, const uint8_t** image,
+                   const char** name);
+int gsn_scene_points(const gsn_scene* s, const float** positions, const float** colors);
+/* Binary PPM (P6, maxval 255) and PNG (8-bit RGB, uncompressed deflate) writers. */
+int gsn_image_write_ppm(const char* path, const uint8_t* rgb, int width, int height);
+int gsn_image_write_png(const char* path, const uint8_t* rgb, int width, int height);
 
 #ifdef __cplusplus
 }

@@ -86,3 +86,54 @@ def test_evaluate_reports_fp64_psnr():
     mse = np.mean((img - image / 255.0) ** 2)
     assert abs(psnr - (-10 * np.log10(mse))) < 1e-4
     assert abs(loss - oracle.loss(img, image)) < 1e-6
+
+
+def ring_scene(views=10, n=15000):
+    cams = scenes.ring_cameras(views, 6.0, 15.0, 200, 140, 180.0, 180.0)
+    hidden = scenes.random_gaussians(n, 31, mean_sigma=1.2)
+    t = torch()
+    r = gsn.Renderer()
+    hp = dev(hidden)
+    img = empty((140, 200, 3), t.float32)
+    images = []
+    for c in cams:
+        assert r.render(hp.data_ptr(), n, c, [0, 0, 0], img.data_ptr(), 3) == 0
+        images.append((img * 255).round().clamp(0, 255).to(t.uint8).cpu().numpy())
+    points, colors = scenes.initial_points(hidden, 3000, 4)
+    return cams, images, points, colors
+
+
+def test_checkpoint_resumes_training(tmp_path):
+    cams, images, points, colors = ring_scene()
+    opts = gsn.TrainingOptions.defaults(densify_from=100, densify_until=900, densify_interval=100)
+    a = gsn.Trainer()
+    assert a.initialize(cams, images, points, colors, opts) == 0
+    assert a.train(700) == 0
+    ck = tmp_path / "state.ckpt"
+    assert a.save_checkpoint(ck) == 0
+    saved = a.state()
+    t = torch()
+    before = t.empty(58 * saved["count"], dtype=t.float32, device="cuda")
+    gsn.memcpy(before.data_ptr(), saved["params"], 4 * 58 * saved["count"])
+    assert a.train(300) == 0
+    b = gsn.Trainer()
+    assert b.initialize(cams, images, points, colors, opts) == 0
+    assert b.load_checkpoint(ck) == 0
+    sb = b.state()
+    assert sb["count"] == saved["count"] and sb["completed"] == 700 and sb["sh_degree"] == saved["sh_degree"]
+    loaded = t.empty(58 * sb["count"], dtype=t.float32, device="cuda")
+    gsn.memcpy(loaded.data_ptr(), sb["params"], 4 * 58 * sb["count"])
+    assert t.equal(before, loaded)
+    assert b.train(300) == 0
+    ma, mb = a.evaluate_metrics(cams, images), b.evaluate_metrics(cams, images)
+    # the same schedule from the same state; the float-atomic order of the
+    # gradient statistics differs, so threshold decisions may flip for a few
+    assert b.state()["completed"] == 1000
+    assert abs(a.state()["count"] - b.state()["count"]) <= 0.005 * a.state()["count"]
+    assert abs(ma["psnr"] - mb["psnr"]) < 0.05
+    assert 0 < mb["ssim"] <= 1 and mb["l1"] > 0
+    # a checkpoint of another layout is refused
+    opts_p = gsn.TrainingOptions.defaults(densify_from=100, densify_until=900, densify_interval=100, precision=1)
+    c = gsn.Trainer()
+    assert c.initialize(cams, images, points, colors, opts_p) == 0
+    assert c.load_checkpoint(ck) != 0
