@@ -589,6 +589,20 @@ int gsn_trainer_evaluate_metrics(gsn_trainer* t, const gsn_camera* cameras, cons
     return t->impl.EvaluateMetrics(cams, imgs, psnr, ssim, l1, loss) ? GSN_OK : GSN_ERR_INVALID_ARGUMENT;
 }
 
+int gsn_eval_metrics(const float* image, const uint8_t* target, int width, int height, double* out, void* stream) {
+    if (!image || !target || !out || width <= 0 || height <= 0) return GSN_ERR_INVALID_ARGUMENT;
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    gs_native::DeviceArray<double> workspace, metrics;
+    if (!workspace.Reserve(gsn::eval_metrics_workspace(width, height) / sizeof(double)) || !metrics.Reserve(4))
+        return GSN_ERR_OUT_OF_MEMORY;
+    const int st = gsn::launch_eval_metrics(image, target, width, height, workspace.get(), metrics.get(), s);
+    if (st != GSN_OK) return st;
+    if (cudaMemcpyAsync(out, metrics.get(), 4 * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return GSN_ERR_CUDA;
+    return GSN_OK;
+}
+
 int gsn_trainer_save(gsn_trainer* t, const char* path) {
     if (!t || !path) return GSN_ERR_INVALID_ARGUMENT;
     return t->impl.Save(path) ? GSN_OK : GSN_ERR_IO;

@@ -138,6 +138,12 @@ int launch_loss_gradient(const float* image, const uint8_t* target, const StepFr
 // tensor-core pass never completed.
 int launch_loss_gradient_tc(const float* image, const uint8_t* target, const StepFrame* frame, float* grad, int width,
                             int height, double* sums, int* status, cudaStream_t stream);
+// FP64 held-out-view metrics (eval.cu): image clamped to [0, 1]; out (device,
+// 4 doubles) = PSNR (dB), mean SSIM (11x11 Gaussian window, sigma 1.5, zero
+// padding), mean L1, MSE. workspace: eval_metrics_workspace(width, height) bytes.
+size_t eval_metrics_workspace(int width, int height);
+int launch_eval_metrics(const float* image, const uint8_t* target, int width, int height, double* workspace,
+                        double* out, cudaStream_t stream);
 // out[0..3] = loss, mean L1, mean SSIM, PSNR (dB) from the sums above.
 int launch_finalize_loss(const double* sums, int width, int height, double* out, cudaStream_t stream);
 

@@ -522,7 +522,8 @@ class Trainer:
         return psnr.value, loss.value
 
     def evaluate_metrics(self, cameras, images):
-        """Mean FP64 PSNR, SSIM, L1 and loss over the views."""
+        """Mean FP64 PSNR, SSIM and L1 of the clamped renders and the mean
+        training loss over the views."""
         cams, ptrs, keep = self._views(cameras, images)
         out = [ctypes.c_double() for _ in range(4)]
         _check(lib().gsn_trainer_evaluate_metrics(self.handle, cams, ptrs, len(cameras), *[ctypes.byref(o) for o in out]),
@@ -864,3 +865,15 @@ def write_ppm(path, rgb):
     a = np.ascontiguousarray(rgb, dtype=np.uint8)
     fn = declare("gsn_image_write_ppm", [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int])
     return fn(str(path).encode(), ctypes.c_void_p(a.ctypes.data), a.shape[1], a.shape[0])
+
+
+def eval_metrics(image_ptr, target_ptr, width, height, stream=0):
+    """FP64 held-out-view metrics of one device fp32 HWC render against a device
+    u8 HWC target: dict(psnr, ssim, l1, mse) with the render clamped to [0, 1]."""
+    fn = declare("gsn_eval_metrics", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                      ctypes.POINTER(ctypes.c_double), ctypes.c_void_p])
+    out = (ctypes.c_double * 4)()
+    _check(fn(ctypes.c_void_p(image_ptr), ctypes.c_void_p(target_ptr), int(width), int(height), out,
+              ctypes.c_void_p(stream)), "eval_metrics")
+    return dict(psnr=out[0], ssim=out[1], l1=out[2], mse=out[3])
+

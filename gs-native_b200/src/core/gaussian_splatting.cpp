@@ -14,6 +14,7 @@
 
 #include "core/knn/knn.h"
 #include "io/ply.h"
+#include "kernels.h"
 
 namespace gs_native {
 
@@ -335,31 +336,44 @@ bool GaussianSplatting::EvaluateMetrics(const std::vector<CameraParams>& cameras
                                         const std::vector<const uint8_t*>& images, double* psnr, double* ssim,
                                         double* l1, double* loss) {
     if (cameras.size() != images.size() || cameras.empty() || !gaussians_.gaussians_) return false;
-    double sums[4] = {0.0, 0.0, 0.0, 0.0};  // loss, L1, SSIM, PSNR
+    double sums[4] = {0.0, 0.0, 0.0, 0.0};  // PSNR, SSIM, L1 (clamped image), loss
     DeviceArray<uint8_t> target;
     DeviceArray<float> image;
-    Solver metric;
-    metric.SetStream(stream_);
-    metric.SetComputeLoss(true);
+    DeviceArray<double> workspace, metrics;
+    Solver objective;
+    objective.SetStream(stream_);
+    objective.SetComputeLoss(true);
+    if (!metrics.Reserve(4)) return false;
     for (size_t k = 0; k < cameras.size(); ++k) {
         const CameraParams& c = cameras[k];
         const size_t px = static_cast<size_t>(c.width_) * c.height_;
-        if (!images[k] || !target.Reserve(px * 3) || !image.Reserve(px * 3)) return false;
+        if (!images[k] || !target.Reserve(px * 3) || !image.Reserve(px * 3) ||
+            !workspace.Reserve(gsn::eval_metrics_workspace(c.width_, c.height_) / sizeof(double)))
+            return false;
         if (cudaMemcpyAsync(target.get(), images[k], px * 3, cudaMemcpyHostToDevice, stream_) != cudaSuccess)
             return false;
-        if (!Render(c, image.get()) || !metric.ComputeImageGradients(c, image.get(), target.get())) return false;
-        double out[4];
-        if (cudaMemcpyAsync(out, metric.GetLossDevice(), sizeof(out), cudaMemcpyDeviceToHost, stream_) !=
-                cudaSuccess ||
+        if (!Render(c, image.get()) ||
+            gsn::launch_eval_metrics(image.get(), target.get(), c.width_, c.height_, workspace.get(), metrics.get(),
+                                     stream_) != GSN_OK)
+            return false;
+        // the training objective (unclamped image), reduced in FP64 as well
+        if (loss && !objective.ComputeImageGradients(c, image.get(), target.get())) return false;
+        double m[4], objective_out[4] = {0.0, 0.0, 0.0, 0.0};
+        if (cudaMemcpyAsync(m, metrics.get(), sizeof(m), cudaMemcpyDeviceToHost, stream_) != cudaSuccess ||
+            (loss && cudaMemcpyAsync(objective_out, objective.GetLossDevice(), sizeof(objective_out),
+                                     cudaMemcpyDeviceToHost, stream_) != cudaSuccess) ||
             cudaStreamSynchronize(stream_) != cudaSuccess)
             return false;
-        for (int q = 0; q < 4; ++q) sums[q] += out[q];
+        sums[0] += m[0];
+        sums[1] += m[1];
+        sums[2] += m[2];
+        sums[3] += objective_out[0];
     }
     const double n = static_cast<double>(cameras.size());
-    if (loss) *loss = sums[0] / n;
-    if (l1) *l1 = sums[1] / n;
-    if (ssim) *ssim = sums[2] / n;
-    if (psnr) *psnr = sums[3] / n;
+    if (psnr) *psnr = sums[0] / n;
+    if (ssim) *ssim = sums[1] / n;
+    if (l1) *l1 = sums[2] / n;
+    if (loss) *loss = sums[3] / n;
     return true;
 }
 

@@ -99,12 +99,14 @@ public:
     bool Save(const std::string& path);
     // Replaces the model by a PLY file (Adam history and statistics reset).
     bool Load(const std::string& path);
-    // Mean PSNR (dB, FP64 reduction) of the current model over the given views
-    // (host u8 HWC images).
+    // Mean PSNR (dB) of the current model over the given views (host u8 HWC
+    // images) and the mean training loss; see EvaluateMetrics.
     bool Evaluate(const std::vector<CameraParams>& cameras, const std::vector<const uint8_t*>& images, double* psnr,
                   double* loss = nullptr);
-    // Mean FP64 PSNR (dB), SSIM (11x11 Gaussian window, as the loss), L1 and
-    // loss over the views; any output may be null.
+    // Held-out-view metrics averaged over the views, in FP64 on the GPU: PSNR
+    // (dB) of the RGB MSE, SSIM (11x11 Gaussian window, sigma 1.5) and L1, all of
+    // the render clamped to [0, 1], plus the training loss of the unclamped
+    // render. Any output may be null.
     bool EvaluateMetrics(const std::vector<CameraParams>& cameras, const std::vector<const uint8_t*>& images,
                          double* psnr, double* ssim, double* l1, double* loss);
 

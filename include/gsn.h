@@ -334,6 +334,11 @@ int gsn_trainer_evaluate(gsn_trainer* t, const gsn_camera* cameras, const uint8_
  * (host u8 HWC images); outputs may be null. gs-native extension. */
 int gsn_trainer_evaluate_metrics(gsn_trainer* t, const gsn_camera* cameras, const uint8_t* const* images, int count,
                                  double* psnr, double* ssim, double* l1, double* loss);
+/* FP64 held-out-view metrics of one rendered view on the GPU (gs-native
+ * extension): image (device fp32 HWC) clamped to [0, 1] against the device u8
+ * HWC target; out (host, 4 doubles) = PSNR (dB), mean SSIM (11x11 Gaussian
+ * window, sigma 1.5, zero padding), mean L1, MSE. Synchronises the stream. */
+int gsn_eval_metrics(const float* image, const uint8_t* target, int width, int height, double* out, void* stream);
 /* Save to / load from a Gaussian PLY (gaussian_splatting.cpp:234-260). */
 int gsn_trainer_save(gsn_trainer* t, const char* path);
 int gsn_trainer_load(gsn_trainer* t, const char* path);

@@ -405,6 +405,52 @@ double orc_loss(const double* image, const uint8_t* target, int width, int heigh
     return 0.8 * l1 / count + 0.2 * (1 - ssim / count);
 }
 
+/* Evaluation metrics of held-out views, as the reference documents them
+ * (README.md "Metrics are averaged over the held-out views..."): RGB clamped to
+ * [0, 1], PSNR of the RGB mean squared error, SSIM with the 11 x 11 Gaussian
+ * window (sigma 1.5) and the loss's zero padding and constants, mean L1.
+ * out[0..3] = PSNR (dB), mean SSIM, mean L1, MSE. FP64 throughout. */
+void orc_eval_metrics(const double* image, const uint8_t* target, int width, int height, double* out) {
+    double w[11];
+    gaussian_window(w);
+    int64_t P = (int64_t)width * height;
+    double* buf = (double*)malloc(sizeof(double) * P * 4);
+    double* f = (double*)malloc(sizeof(double) * P * 5);
+    double *a = buf, *b = buf + P, *prod = buf + 2 * P, *tmp = buf + 3 * P;
+    double l1 = 0, sq = 0, ssim = 0;
+    for (int c = 0; c < 3; ++c) {
+        for (int64_t i = 0; i < P; ++i) {
+            double v = image[i * 3 + c];
+            a[i] = v < 0 ? 0 : (v > 1 ? 1 : v);
+            b[i] = target[i * 3 + c] / 255.0;
+            l1 += fabs(a[i] - b[i]);
+            sq += (a[i] - b[i]) * (a[i] - b[i]);
+        }
+        double* src[5] = {a, b, NULL, NULL, NULL};
+        for (int k = 0; k < 5; ++k) {
+            if (k >= 2) {
+                for (int64_t i = 0; i < P; ++i)
+                    prod[i] = k == 2 ? a[i] * a[i] : (k == 3 ? b[i] * b[i] : a[i] * b[i]);
+                src[k] = prod;
+            }
+            filter_band(src[k], f + k * P, tmp, width, height, 0, height, w);
+        }
+        for (int64_t i = 0; i < P; ++i) {
+            double ma = f[i], mb = f[P + i];
+            double va = f[2 * P + i] - ma * ma, vb = f[3 * P + i] - mb * mb, cov = f[4 * P + i] - ma * mb;
+            ssim += (2 * ma * mb + 0.0001) * (2 * cov + 0.0009) / ((ma * ma + mb * mb + 0.0001) * (va + vb + 0.0009));
+        }
+    }
+    free(f);
+    free(buf);
+    double count = 3.0 * (double)P;
+    double mse = sq / count;
+    out[0] = mse > 0 ? -10.0 * log10(mse) : INFINITY;
+    out[1] = ssim / count;
+    out[2] = l1 / count;
+    out[3] = mse;
+}
+
 /* Analytic gradient of orc_loss: L1 sign term plus the SSIM chain through the
  * two separable filter passes, the quantity solver.cu:26-168 evaluates in FP32.
  * Output rows [row_begin, row_end) (all rows when row_end <= 0). */

@@ -74,6 +74,10 @@ void orc_render(const orc_proj* p, const gsn_camera* cam, const int64_t* offsets
  * contribute to the sums when row_end > 0 (normalised by the full image). */
 double orc_loss(const double* image, const uint8_t* target, int width, int height);
 
+/* Held-out-view metrics: image clamped to [0, 1]; out = PSNR (dB), mean SSIM
+ * (11x11, sigma 1.5, zero padding), mean L1, MSE. FP64. */
+void orc_eval_metrics(const double* image, const uint8_t* target, int width, int height, double* out);
+
 /* Analytic dLoss/dimage of orc_loss (the quantity of solver.cu:26-168), FP64. */
 void orc_loss_gradient(const double* image, const uint8_t* target, int width, int height, double* gradient,
                        int row_begin, int row_end);

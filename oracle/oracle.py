@@ -60,6 +60,7 @@ def oracle():
             "orc_free": [cp],
             "orc_render": [cp, cp, cp, cp, cp, cp, cp, cp, _i32, _i32],
             "orc_loss": [cp, cp, _i32, _i32],
+            "orc_eval_metrics": [cp, cp, _i32, _i32, cp],
             "orc_loss_gradient": [cp, cp, _i32, _i32, cp, _i32, _i32],
             "orc_backward": [cp, _i32, cp, cp, cp, cp, cp, cp, cp, _i32, _i32],
             "orc_projection_statistics": [cp, _i32, cp, cp, cp, cp, cp],
@@ -170,6 +171,16 @@ def loss(image, target):
     target = np.ascontiguousarray(target, dtype=np.uint8)
     h, w = target.shape[:2]
     return oracle().orc_loss(ptr(image), ptr(target), w, h)
+
+
+def eval_metrics(image, target):
+    """(psnr_db, ssim, l1, mse) of one view with the image clamped to [0, 1]."""
+    image = np.ascontiguousarray(image, dtype=np.float64)
+    target = np.ascontiguousarray(target, dtype=np.uint8)
+    h, w = target.shape[:2]
+    out = np.zeros(4, dtype=np.float64)
+    oracle().orc_eval_metrics(ptr(image), ptr(target), w, h, ptr(out))
+    return tuple(float(x) for x in out)
 
 
 def loss_gradient(image, target, rows=(0, 0)):

@@ -12,6 +12,7 @@ import pytest
 
 import colmap_writer as cw
 import gsn
+import oracle
 import scenes
 
 pytestmark = pytest.mark.gpu
@@ -77,6 +78,9 @@ def test_train_and_render_demo(tmp_path):
     assert len(psnr) == 2 and float(rows[-1].split(",")[1]) == pytest.approx(np.mean(psnr), abs=1e-8)
     assert min(psnr) > 15.0  # held-out views of a 14-view ring after 1,200 updates
 
+    metrics = (dest / "metrics.csv").read_text().strip().split("\n")
+    assert metrics[0] == "image,psnr_db,ssim,l1" and len(metrics) == 4
+
     # recompute from the PLY through the library renderer
     import torch
     st, params = gsn.ply_read(ply)
@@ -89,6 +93,9 @@ def test_train_and_render_demo(tmp_path):
         u8 = np.rint(np.clip(img.cpu().numpy(), 0, 1) * np.float32(255)).astype(np.uint8)
         mse = np.mean((u8.astype(np.float64) - target) ** 2) / 255.0 ** 2
         assert -10 * np.log10(mse) == pytest.approx(psnr[k], abs=1e-6)
+        fp64 = [float(x) for x in metrics[1 + k].split(",")[1:]]
+        want = oracle.eval_metrics(img.cpu().numpy().astype(np.float64), target)
+        assert np.allclose(fp64, want[:3], rtol=1e-9, atol=1e-10)
         name = f"{k:05d}.png"
         assert np.array_equal(cw.decode_png(dest / "renders" / name), u8)
         assert np.array_equal(cw.decode_png(dest / "gt" / name), target)
