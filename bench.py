@@ -13,14 +13,17 @@ means N(0, 3^2)); 200 cameras on a ring of radius 8 at elevation +/-15 deg,
 hidden model and quantised to u8. The model being optimised is a 1.2M-Gaussian
 draw of the same distribution (seed 8).
 
-Four forms of the same iteration are timed, each from the same initial model:
+Six forms of the same iteration are timed, each from the same initial model:
 `plain_fp32` (eager launches from the host, the reference-parity form),
 `graph_fp32` (the iteration captured once as a CUDA graph over a fixed record
-capacity and replayed from a device schedule of views), and `precision_bf16` /
-`precision_bf16_graph` (SH rows and their Adam moments stored in bf16 with
-stochastic rounding; fp32 blending and accumulation). `value` is the fastest
-form that completed without a record overflow; all are in `forms`, with
-`chosen_over_plain` the ratio to the plain form.
+capacity and replayed from a device schedule of views), `culled_fp32` /
+`culled_graph_fp32` (exact tile culling: only records whose tile the alpha
+>= 1/255 ellipse reaches are emitted and sorted; images and gradients are
+unchanged) and `precision_bf16_culled` / `precision_bf16_culled_graph` (culling
+plus SH rows and their Adam moments stored in bf16 with stochastic rounding;
+fp32 blending and accumulation). `value` is the fastest form that completed
+without a record overflow; all are in `forms`, with `chosen_over_plain` the
+ratio to the plain form.
 
 Printed JSON line: `value` is iterations/s with targets resident in HBM,
 `e2e` the same through host buffers (pinned H2D target upload and a D2H loss
@@ -66,6 +69,7 @@ def parse():
                    help="warm-up steps plus one step on 3 views, no JSON (for ncu captures)")
     p.add_argument("--views", type=int, default=0, help="number of training views used (0 = all 180)")
     p.add_argument("--precision", action="store_true", help="with --profile-only: run the precision form")
+    p.add_argument("--culled", action="store_true", help="with --profile-only: exact tile culling on")
     p.add_argument("--no-multiview", action="store_true", help="skip the 32-view multi-view measurement")
     return p.parse_args()
 
@@ -321,10 +325,11 @@ def run_gsn(args):
     class Form:
         """One form of the iteration: its own renderer, solver and parameter block."""
 
-        def __init__(self, bf16):
+        def __init__(self, bf16, culled=False):
             self.renderer, self.solver = gsn.Renderer(), gsn.Solver()
             self.renderer.set_stream(sp)
             self.solver.set_stream(sp)
+            self.renderer.set_exact_culling(culled)
             if bf16:
                 self.renderer.set_bf16_sh(True)
                 self.solver.set_bf16_sh(True)
@@ -431,7 +436,7 @@ def run_gsn(args):
         return eager, graphed, stages, records, visible_count
 
     if args.profile_only:
-        f = Form(args.precision)
+        f = Form(args.precision, args.culled)
         for k in range(args.warmup + 1):
             step(f, k)
         torch.cuda.synchronize()
@@ -444,7 +449,11 @@ def run_gsn(args):
     plain_eager, plain_graph, stages, records, vis = measure(plain)
     del plain
     torch.cuda.empty_cache()
-    prec = Form(True)
+    culled = Form(False, True)
+    culled_eager, culled_graph, culled_stages, culled_records, _ = measure(culled)
+    del culled
+    torch.cuda.empty_cache()
+    prec = Form(True, True)
     prec_eager, prec_graph, prec_stages, _, _ = measure(prec)
     clocks = sampler.stop() if sampler else None
     del prec
@@ -490,8 +499,9 @@ def run_gsn(args):
         tgt0 = targets[0].cpu().numpy()
         res = cpu_baseline(model, train[0], tgt0, extent, steps=1)
         cpu = {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")}
-    forms = {"plain_fp32": plain_eager, "graph_fp32": plain_graph, "precision_bf16": prec_eager,
-             "precision_bf16_graph": prec_graph}
+    forms = {"plain_fp32": plain_eager, "graph_fp32": plain_graph, "culled_fp32": culled_eager,
+             "culled_graph_fp32": culled_graph, "precision_bf16_culled": prec_eager,
+             "precision_bf16_culled_graph": prec_graph}
     valid = {k: v for k, v in forms.items() if v.get("status", 0) == 0}
     chosen = max(valid, key=lambda k: valid[k]["value"])
     out = {
@@ -511,7 +521,9 @@ def run_gsn(args):
                 "d2h_bytes_per_step": 32, "psnr_db_last_step": forms[chosen]["psnr_db_last_step"]},
         "roofline": roofline,
         "stages": stage_table,
+        "stages_culled": {k: round(v, 4) for k, v in culled_stages.items()},
         "stages_precision": {k: round(v, 4) for k, v in prec_stages.items()},
+        "records": {"plain": records, "culled": culled_records},
         "multiview": multiview,
         "clocks": clocks,
         "cpu_baseline": cpu,

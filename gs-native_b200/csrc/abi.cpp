@@ -227,6 +227,12 @@ int gsn_renderer_set_bf16_sh(gsn_renderer* r, int enabled) {
     return GSN_OK;
 }
 
+int gsn_renderer_set_exact_culling(gsn_renderer* r, int enabled) {
+    if (!r) return GSN_ERR_INVALID_ARGUMENT;
+    r->impl.SetExactCulling(enabled != 0);
+    return GSN_OK;
+}
+
 int gsn_renderer_set_record_capacity(gsn_renderer* r, int64_t records) {
     if (!r) return GSN_ERR_INVALID_ARGUMENT;
     return r->impl.SetRecordCapacity(records) ? GSN_OK : GSN_ERR_INVALID_ARGUMENT;
@@ -479,6 +485,7 @@ int gsn_training_options_default(gsn_training_options* out) {
     out->learned_density = o.learned_density ? 1 : 0;
     out->learned_confidence = o.learned_confidence;
     out->log_density = o.log_density ? 1 : 0;
+    out->exact_culling = o.exact_culling ? 1 : 0;
     return GSN_OK;
 }
 
@@ -516,6 +523,7 @@ gs_native::TrainingOptions ToOptions(const gsn_training_options& in) {
     o.learned_density = in.learned_density != 0;
     o.learned_confidence = in.learned_confidence;
     o.log_density = in.log_density != 0;
+    o.exact_culling = in.exact_culling != 0;
     return o;
 }
 }  // namespace

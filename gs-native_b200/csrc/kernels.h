@@ -55,6 +55,7 @@ struct ProjectOutputs {
     int* tile_counts;        // [N] tiles touched (0 = culled)
     uint32_t* depth_keys;    // [N] float bits of z, 0xFFFFFFFF when culled
     float* radii;            // [N] optional 3-sigma pixel radius (0 = culled), may be null
+    int* cull_counts;        // [N] optional exact-culling record counts (16 x 16 tiles only), may be null
 };
 // cam_dev (optional): device camera read instead of `cam` (batched form).
 // bf16_sh: precision-form parameter layout (10 fp32 rows + 48 bf16 SH rows).
@@ -105,6 +106,17 @@ int launch_exclusive_scan(const int* in, const uint32_t* gather, int* out, int n
 int launch_emit_records(const uint32_t* sorted_ids, const int* record_start, const int4* rects,
                         int n, int tile_count_x, uint32_t* tile_keys, uint32_t* record_ids,
                         int64_t capacity, int* overflow, cudaStream_t stream);
+
+// Exact tile culling (project.cu): with ProjectOutputs::cull_counts set, the
+// projection also counts, per Gaussian, the tiles of its rect whose pixel
+// centres the widened alpha >= 1/255 ellipse reaches; launch_emit_records_culled
+// emits exactly those records in depth order. Dropped records are ones the blend
+// kernels skip at every pixel, so images and gradients are unchanged. A count
+// the emitter cannot reproduce sets *overflow to 2 (never expected).
+int launch_emit_records_culled(const uint32_t* sorted_ids, const int* record_start, const int4* rects,
+                               const float2* means, const float4* conic_opacity, int n, int tile_count_x,
+                               uint32_t* tile_keys, uint32_t* record_ids, int64_t capacity, int* overflow,
+                               cudaStream_t stream);
 
 // Per-tile [begin, end) offsets of sorted tile keys (empty tiles included).
 int launch_tile_ranges(const uint32_t* sorted_tiles, const int* record_count_device, int max_records,

@@ -41,6 +41,123 @@ __device__ __forceinline__ void sh_basis(float x, float y, float z, float b[16])
     b[15] = -kSh3a * x * (xx - 3.0f * yy);
 }
 
+// ---------------------------------------------------------------- exact tile culling
+// A record (tile, Gaussian) can only change a pixel of its tile where
+// alpha = o * exp(-q/2) >= 1/255, i.e. inside the ellipse q(d) <= 2 ln(255 o)
+// (q(d) = A dx^2 + 2 B dx dy + C dy^2, conic (A, B, C), d = pixel - mean). The
+// reference emits every tile of the 3-sigma rectangle; the culled form emits only
+// the tiles whose pixel-centre rectangle meets that ellipse, widened as the blend
+// kernels' alpha box is (2 % + 0.05 on Q plus a condition-number term, and a
+// pixel pad), so a dropped record is one the per-pixel test rejects at every
+// pixel of its tile: images, transmittance and gradients are unchanged.
+//
+// Per tile row the reachable columns form one interval: the ellipse's x-extent
+// inside the band of the row's pixel centres, found at the band edge nearest to
+// the ellipse's leftmost / rightmost point. Both functions are kept out of line
+// so that the counting (projection) and the emitting kernel run one and the same
+// instruction sequence on the same stored values and agree on every count.
+struct CullShape {
+    float mx, my;      // mean
+    float B, inv_a;    // conic B, 1 / A
+    float det, qa;     // A C - B^2, A * Q
+    float hy, ys;      // y half-extent (padded), y of the rightmost point (negated)
+    float pad_x;
+    int mode;          // 0: reaches no pixel, 1: keep whole rows, 2: ellipse spans
+};
+
+__device__ __noinline__ CullShape cull_shape(float2 mean, float4 q) {
+    CullShape s;
+    s.mode = 0;
+    s.mx = mean.x;
+    s.my = mean.y;
+    s.B = q.y;
+    const float lo = 255.0f * q.w;
+    if (!(lo > 1.0f)) return s;  // alpha can never reach 1/255
+    s.mode = 1;
+    const float det = q.x * q.z - q.y * q.y;
+    const float tr = 0.5f * (q.x + q.z);
+    const float disc = sqrtf(fmaxf(tr * tr - det, 0.0f));
+    const float kappa = (tr + disc) / fmaxf(tr - disc, 1e-30f);
+    if (!(det > 0.0f) || !(kappa < 1e5f) || !isfinite(mean.x) || !isfinite(mean.y) || !isfinite(lo)) return s;
+    const float Q = 2.0f * __logf(lo) * (1.02f + 1e-6f * kappa) + 0.05f;
+    const float hx = sqrtf(Q * q.z / det), hy = sqrtf(Q * q.x / det);
+    if (!isfinite(hx) || !isfinite(hy)) return s;
+    s.mode = 2;
+    s.inv_a = 1.0f / q.x;
+    s.det = det;
+    s.qa = q.x * Q;
+    s.hy = hy + 0.05f + 1e-3f * hy + 2e-5f * fabsf(mean.y);
+    s.ys = q.y * hx / q.z;
+    s.pad_x = 0.05f + 1e-3f * hx + 2e-5f * fabsf(mean.x);
+    return s;
+}
+
+// Columns [x, y) of tile row ty (inside rect) that the record can reach.
+__device__ __noinline__ int2 cull_row_span(CullShape s, int4 rect, int ty) {
+    if (s.mode == 0) return make_int2(rect.x, rect.x);
+    if (s.mode == 1) return make_int2(rect.x, rect.z);
+    const float y0 = static_cast<float>(ty * kTile) - s.my, y1 = y0 + (kTile - 1);
+    if (y0 > s.hy || y1 < -s.hy) return make_int2(rect.x, rect.x);
+    const float yr = fminf(fmaxf(-s.ys, y0), y1), yl = fminf(fmaxf(s.ys, y0), y1);
+    const float xr = (-s.B * yr + sqrtf(fmaxf(s.qa - s.det * yr * yr, 0.0f))) * s.inv_a;
+    const float xl = (-s.B * yl - sqrtf(fmaxf(s.qa - s.det * yl * yl, 0.0f))) * s.inv_a;
+    // tile tx holds pixel centres [16 tx, 16 tx + 15]
+    const float c0 = floorf((s.mx + xl - s.pad_x) * (1.0f / kTile));
+    const float c1 = floorf((s.mx + xr + s.pad_x) * (1.0f / kTile)) + 1.0f;
+    const int a = static_cast<int>(fminf(fmaxf(c0, static_cast<float>(rect.x)), static_cast<float>(rect.z)));
+    const int b = static_cast<int>(fminf(fmaxf(c1, static_cast<float>(rect.x)), static_cast<float>(rect.z)));
+    return make_int2(a, max(a, b));
+}
+
+__device__ __forceinline__ int cull_count(float2 mean, float4 q, int4 rect) {
+    const CullShape s = cull_shape(mean, q);
+    if (s.mode == 0) return 0;
+    if (s.mode == 1) return (rect.z - rect.x) * (rect.w - rect.y);
+    int total = 0;
+    for (int ty = rect.y; ty < rect.w; ++ty) {
+        const int2 span = cull_row_span(s, rect, ty);
+        total += span.y - span.x;
+    }
+    return total;
+}
+
+// Records of the culled counts in depth order: the four lanes of a Gaussian
+// walk its rows, each row's column interval split across the lanes.
+__global__ void __launch_bounds__(256) emit_records_culled(const uint32_t* __restrict__ sorted_ids,
+                                                           const int* __restrict__ record_start,
+                                                           const int4* __restrict__ rects,
+                                                           const float2* __restrict__ means,
+                                                           const float4* __restrict__ conic_opacity, int n,
+                                                           int tile_count_x, uint32_t* __restrict__ tile_keys,
+                                                           uint32_t* __restrict__ record_ids, int64_t capacity,
+                                                           int* overflow) {
+    const int64_t gidx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int64_t p = gidx >> 2;
+    const int sub = static_cast<int>(gidx & 3);
+    if (p >= n) return;
+    const int begin = record_start[p];
+    const int count = record_start[p + 1] - begin;
+    if (count <= 0) return;
+    if (begin + static_cast<int64_t>(count) > capacity) {
+        if (sub == 0 && overflow) atomicExch(overflow, 1);
+        return;
+    }
+    const uint32_t id = sorted_ids[p];
+    const int4 r = rects[id];
+    const CullShape s = cull_shape(means[id], conic_opacity[id]);
+    int k = 0;
+    for (int ty = r.y; ty < r.w && k < count; ++ty) {
+        const int2 span = cull_row_span(s, r, ty);
+        const int w = span.y - span.x;
+        for (int j = sub; j < w && k + j < count; j += 4) {
+            tile_keys[begin + k + j] = static_cast<uint32_t>(ty * tile_count_x + span.x + j);
+            record_ids[begin + k + j] = id;
+        }
+        k += w;
+    }
+    if (k != count && sub == 0 && overflow) atomicExch(overflow, 2);
+}
+
 // kBf16: precision form (bf16 SH rows; near-singular conics inverted in FP64).
 // TW x TH: tile shape of the rectangle (16 x 16, the reference's, everywhere but
 // the multi-view renderer's tile-shape sweep).
@@ -53,6 +170,7 @@ __global__ void __launch_bounds__(256) project_kernel(const float* __restrict__ 
     const gsn_camera cam = cam_dev ? *cam_dev : cam_arg;
     const int64_t N = n;
     out.tile_counts[i] = 0;
+    if (out.cull_counts) out.cull_counts[i] = 0;
     out.depth_keys[i] = 0xFFFFFFFFu;
     if (out.radii) out.radii[i] = 0.0f;
 
@@ -135,13 +253,18 @@ __global__ void __launch_bounds__(256) project_kernel(const float* __restrict__ 
     if (out.radii) out.radii[i] = radius;
     float opacity = 1.0f / (1.0f + expf(-__ldg(params + 9 * N + i)));
     out.means[i] = make_float2(u, v);
+    float4 conic;
     if (singular64) {
         const double inv64 = 1.0 / det64;
-        out.conic_opacity[i] = make_float4(static_cast<float>(c * inv64), static_cast<float>(-b * inv64),
-                                           static_cast<float>(a * inv64), opacity);
+        conic = make_float4(static_cast<float>(c * inv64), static_cast<float>(-b * inv64),
+                            static_cast<float>(a * inv64), opacity);
     } else {
         float det_inv = 1.0f / det;
-        out.conic_opacity[i] = make_float4(c * det_inv, -b * det_inv, a * det_inv, opacity);
+        conic = make_float4(c * det_inv, -b * det_inv, a * det_inv, opacity);
+    }
+    out.conic_opacity[i] = conic;
+    if constexpr (TW == kTile && TH == kTile) {
+        if (out.cull_counts) out.cull_counts[i] = cull_count(make_float2(u, v), conic, rect);
     }
 
     // View direction from the camera centre, C = -R^T t.
@@ -197,6 +320,17 @@ int launch_project_tiled(const float* params, int n, const gsn_camera& cam, int 
     else if (tile_w == 16 && tile_h == 8) launch_project_tiles<16, 8>(params, n, cam, d, out, stream);
     else if (tile_w == 8 && tile_h == 8) launch_project_tiles<8, 8>(params, n, cam, d, out, stream);
     else return GSN_ERR_INVALID_ARGUMENT;
+    return launched(1);
+}
+
+int launch_emit_records_culled(const uint32_t* sorted_ids, const int* record_start, const int4* rects,
+                               const float2* means, const float4* conic_opacity, int n, int tile_count_x,
+                               uint32_t* tile_keys, uint32_t* record_ids, int64_t capacity, int* overflow,
+                               cudaStream_t stream) {
+    if (n <= 0) return GSN_OK;
+    emit_records_culled<<<ceil_div(4ll * n, 256), 256, 0, stream>>>(sorted_ids, record_start, rects, means,
+                                                                    conic_opacity, n, tile_count_x, tile_keys,
+                                                                    record_ids, capacity, overflow);
     return launched(1);
 }
 

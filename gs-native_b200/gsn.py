@@ -95,6 +95,7 @@ def lib():
         "gsn_renderer_record_offsets": ([vp, P(vp)], i32),
         "gsn_renderer_set_record_capacity": ([vp, i64], i32),
         "gsn_renderer_set_bf16_sh": ([vp, i32], i32),
+        "gsn_renderer_set_exact_culling": ([vp, i32], i32),
         "gsn_solver_set_bf16_sh": ([vp, i32], i32),
         "gsn_solver_set_tensor_core_loss": ([vp, i32], i32),
         "gsn_solver_status": ([vp, P(i32)], i32),
@@ -174,6 +175,9 @@ class Renderer:
 
     def set_bf16_sh(self, enabled=True):
         _check(lib().gsn_renderer_set_bf16_sh(self.handle, int(bool(enabled))), "set_bf16_sh")
+
+    def set_exact_culling(self, enabled=True):
+        _check(lib().gsn_renderer_set_exact_culling(self.handle, int(bool(enabled))), "set_exact_culling")
 
 
 def launch_count():
@@ -432,6 +436,7 @@ class TrainingOptions(ctypes.Structure):
         ("density_seed", ctypes.c_ulonglong), ("initial_opacity", ctypes.c_float),
         ("precision", ctypes.c_int), ("graph", ctypes.c_int),
         ("learned_density", ctypes.c_int), ("learned_confidence", ctypes.c_float), ("log_density", ctypes.c_int),
+        ("exact_culling", ctypes.c_int),
     ]
 
     @classmethod

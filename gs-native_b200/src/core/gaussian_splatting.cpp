@@ -90,6 +90,7 @@ bool GaussianSplatting::Initialize(const TrainingScene& scene, const TrainingOpt
     solver_.SetLearningRates(options_.lr);
     density_.SetMaxGaussians(options_.max_gaussians);
     renderer_.SetBf16Sh(options_.bf16_sh);
+    renderer_.SetExactCulling(options_.exact_culling);
     eval_renderer_.SetBf16Sh(options_.bf16_sh);
     solver_.SetBf16Sh(options_.bf16_sh);
     density_.SetBf16Sh(options_.bf16_sh);

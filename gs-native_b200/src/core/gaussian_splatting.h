@@ -71,6 +71,7 @@ struct TrainingOptions {
     bool learned_density = false;
     float learned_confidence = 0.9f;
     bool log_density = false;  // keep the statistics and decisions of the last control step (GetDensityLog)
+    bool exact_culling = false;  // training renderer emits only records that can contribute (Renderer::SetExactCulling)
 };
 
 // Statistics, decisions and parent map of the last density-control step

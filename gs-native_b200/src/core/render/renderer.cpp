@@ -43,7 +43,8 @@ bool Renderer::ReserveGaussians(int count) {
     size_t grow = std::max(n, gaussian_capacity_ + gaussian_capacity_ / 4);
     bool ok = means_.Reserve(grow) && conic_opacities_.Reserve(grow) && colors_.Reserve(grow) &&
               depths_.Reserve(grow) && radii_.Reserve(grow) && rects_.Reserve(grow) &&
-              tile_counts_.Reserve(grow) && depth_keys_[0].Reserve(grow) && depth_keys_[1].Reserve(grow) &&
+              tile_counts_.Reserve(grow) && cull_counts_.Reserve(grow) && depth_keys_[0].Reserve(grow) &&
+              depth_keys_[1].Reserve(grow) &&
               depth_ids_[0].Reserve(grow) && depth_ids_[1].Reserve(grow) && record_start_.Reserve(grow + 1) &&
               counters_.Reserve(2);
     if (!ok) return false;
@@ -112,7 +113,8 @@ bool Renderer::Render(const GaussianBuffers& gaussians, const CameraParams& came
     int64_t records = 0;
     if (count > 0) {
         gsn::ProjectOutputs po{means_.get(), conic_opacities_.get(), colors_.get(), depths_.get(),
-                               rects_.get(), tile_counts_.get(), depth_keys_[0].get(), radii_.get()};
+                               rects_.get(), tile_counts_.get(), depth_keys_[0].get(), radii_.get(),
+                               exact_culling_ ? cull_counts_.get() : nullptr};
         gsn::stage_mark(s, gsn::kStageProject);
         if (gsn::launch_project(gaussians.gaussians_, count, cam, device_camera_, sh_degree, bf16_sh_, po, s) != GSN_OK) return false;
         gsn::stage_mark(s, gsn::kStageDepthSort);
@@ -124,8 +126,8 @@ bool Renderer::Render(const GaussianBuffers& gaussians, const CameraParams& came
             return false;
         const uint32_t* by_depth = depth_ids_[in_alt ? 1 : 0].get();
         gsn::stage_mark(s, gsn::kStageRecordScan);
-        if (gsn::launch_exclusive_scan(tile_counts_.get(), by_depth, record_start_.get(), count,
-                                       scan_scratch_.get(), s) != GSN_OK)
+        if (gsn::launch_exclusive_scan(exact_culling_ ? cull_counts_.get() : tile_counts_.get(), by_depth,
+                                       record_start_.get(), count, scan_scratch_.get(), s) != GSN_OK)
             return false;
         if (cudaMemcpyAsync(record_count, record_start_.get() + count, sizeof(int), cudaMemcpyDeviceToDevice,
                             s) != cudaSuccess)
@@ -146,10 +148,16 @@ bool Renderer::Render(const GaussianBuffers& gaussians, const CameraParams& came
             last_records_ = records;
         }
         gsn::stage_mark(s, gsn::kStageEmitRecords);
-        if (gsn::launch_emit_records(by_depth, record_start_.get(), rects_.get(), count, camera.tile_count_x_,
-                                     tile_keys_[0].get(), record_ids_[0].get(), record_capacity_, overflow,
-                                     s) != GSN_OK)
-            return false;
+        const int emitted =
+            exact_culling_
+                ? gsn::launch_emit_records_culled(by_depth, record_start_.get(), rects_.get(), means_.get(),
+                                                  conic_opacities_.get(), count, camera.tile_count_x_,
+                                                  tile_keys_[0].get(), record_ids_[0].get(), record_capacity_,
+                                                  overflow, s)
+                : gsn::launch_emit_records(by_depth, record_start_.get(), rects_.get(), count, camera.tile_count_x_,
+                                           tile_keys_[0].get(), record_ids_[0].get(), record_capacity_, overflow,
+                                           s);
+        if (emitted != GSN_OK) return false;
         const int max_records = fixed_capacity_ ? static_cast<int>(record_capacity_) : static_cast<int>(records);
         scratch = gsn::radix_sort_scratch(sort_scratch_.get(), static_cast<int>(sort_scratch_count_));
         in_alt = false;

@@ -59,6 +59,13 @@ public:
     // Precision form: the parameter block holds 10 fp32 geometry rows followed
     // by the 48 SH rows in bf16 (34 float rows of stride N).
     void SetBf16Sh(bool enabled) { bf16_sh_ = enabled; }
+    // Exact tile culling: emit only the records whose tile the widened
+    // alpha >= 1/255 ellipse reaches (the reference emits the whole 3-sigma
+    // rectangle). Images and gradients are unchanged; the tile lists are the
+    // reference's lists minus records that never contribute. GetTileCounts and
+    // GetRecordOffsets keep the rectangle counts (the visibility statistic).
+    void SetExactCulling(bool enabled) { exact_culling_ = enabled; }
+    bool GetExactCulling() const { return exact_culling_; }
     bool GetBf16Sh() const { return bf16_sh_; }
     const int* GetTileCounts() const { return tile_counts_.get(); }
     const int4* GetTileRects() const { return rects_.get(); }
@@ -83,6 +90,7 @@ private:
     bool fixed_capacity_ = false;
     const gsn_camera* device_camera_ = nullptr;
     bool bf16_sh_ = false;
+    bool exact_culling_ = false;
     int64_t last_records_ = 0;
     int last_count_ = 0;
 
@@ -93,6 +101,7 @@ private:
     DeviceArray<float> radii_;
     DeviceArray<int4> rects_;
     DeviceArray<int> tile_counts_;
+    DeviceArray<int> cull_counts_;  // exact-culling record counts per Gaussian
     DeviceArray<uint32_t> depth_keys_[2];
     DeviceArray<uint32_t> depth_ids_[2];
     DeviceArray<int> record_start_;

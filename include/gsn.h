@@ -162,6 +162,13 @@ int gsn_renderer_set_record_capacity(gsn_renderer* r, int64_t records);
  * moments; SH updates use stochastic rounding; switching drops the history)
  * and on the density controller. */
 int gsn_renderer_set_bf16_sh(gsn_renderer* r, int enabled);
+/* Exact tile culling (gs-native extension): emit only the records whose tile
+ * the (widened) alpha >= 1/255 ellipse of the Gaussian reaches, instead of
+ * every tile of its 3-sigma rectangle (renderer.cu:223-245). Images and
+ * gradients are unchanged; per-tile lists are the reference's minus records
+ * that never contribute. Tile counts / record offsets keep the rectangle
+ * counts (the solver's visibility statistic, solver.cu:484). */
+int gsn_renderer_set_exact_culling(gsn_renderer* r, int enabled);
 
 
 /* ------------------------------------------------------------------ solver
@@ -310,6 +317,7 @@ typedef struct gsn_training_options {
     int learned_density;             /* 1: the learned policy (gsn_trainer_set_density_mlp) proposes actions */
     float learned_confidence;        /* 0.9: softmax probability needed to override the threshold rule */
     int log_density;                 /* 1: keep the last control step's statistics (gsn_trainer_density_log) */
+    int exact_culling;               /* 1: exact tile culling in the training renderer (gsn_renderer_set_exact_culling) */
 } gsn_training_options;
 
 int gsn_training_options_default(gsn_training_options* out);

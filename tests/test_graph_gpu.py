@@ -109,26 +109,35 @@ def test_graph_rejects_mixed_resolutions_and_bad_views():
     g.close()
 
 
-def test_trainer_graph_steady_state_trains_like_eager():
-    """Iterations after densify_until run as graph replays in the trainer; with
-    the same schedule (camera order, learning rates) the result matches the
-    eager trainer up to the backward's atomic summation order. (Float-atomic
-    reordering makes any two runs drift apart slowly, so the replayed span is
-    kept to 60 steps.)"""
+def _graph_vs_eager(densify_from, densify_until, iterations):
     cams, _, targets = views_scene(n=20000, views=6)
     hidden = views_scene.hidden
     imgs = [targets[k].cpu().numpy() for k in range(6)]
     points, colors = scenes.initial_points(hidden, 4000, 5)
     out = {}
     for graph in (0, 1):
-        opts = gsn.TrainingOptions.defaults(densify_from=100, densify_until=400, densify_interval=100,
-                                            sh_degree_interval=100, opacity_reset_interval=100000, graph=graph)
+        opts = gsn.TrainingOptions.defaults(densify_from=densify_from, densify_until=densify_until,
+                                            densify_interval=100, sh_degree_interval=100,
+                                            opacity_reset_interval=100000, graph=graph)
         tr = gsn.Trainer()
         assert tr.initialize(cams, imgs, points, colors, opts) == 0
-        assert tr.train(460) == 0
+        assert tr.train(iterations) == 0
         psnr, loss = tr.evaluate(cams, imgs)
         st = tr.state()
         out[graph] = (psnr, loss, st["count"], st["completed"])
         tr.close()
-    assert out[0][2] == out[1][2] and out[0][3] == out[1][3] == 460
-    assert abs(out[0][0] - out[1][0]) < 0.05, out
+    assert out[0][3] == out[1][3] == iterations
+    return out
+
+
+def test_trainer_graph_steady_state_trains_like_eager():
+    """Iterations after densify_until run as graph replays in the trainer; with
+    the same schedule (camera order, learning rates) the result matches the
+    eager trainer up to the backward's atomic summation order. Without density
+    control (360 replayed steps, SH ramp included) that is the only difference;
+    with it, threshold decisions amplify the float-atomic noise chaotically, so
+    that run only checks the counts and a loose PSNR bound."""
+    out = _graph_vs_eager(100000, 100, 460)
+    assert out[0][2] == out[1][2] and abs(out[0][0] - out[1][0]) < 0.03, out
+    out = _graph_vs_eager(100, 400, 460)
+    assert abs(out[0][2] - out[1][2]) <= 0.01 * out[0][2] and abs(out[0][0] - out[1][0]) < 0.3, out
