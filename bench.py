@@ -13,17 +13,21 @@ means N(0, 3^2)); 200 cameras on a ring of radius 8 at elevation +/-15 deg,
 hidden model and quantised to u8. The model being optimised is a 1.2M-Gaussian
 draw of the same distribution (seed 8).
 
-Six forms of the same iteration are timed, each from the same initial model:
+Eight forms of the same iteration are timed, each from the same initial model:
 `plain_fp32` (eager launches from the host, the reference-parity form),
 `graph_fp32` (the iteration captured once as a CUDA graph over a fixed record
 capacity and replayed from a device schedule of views), `culled_fp32` /
 `culled_graph_fp32` (exact tile culling: only records whose tile the alpha
 >= 1/255 ellipse reaches are emitted and sorted; images and gradients are
-unchanged) and `precision_bf16_culled` / `precision_bf16_culled_graph` (culling
-plus SH rows and their Adam moments stored in bf16 with stochastic rounding;
-fp32 blending and accumulation). `value` is the fastest form that completed
-without a record overflow; all are in `forms`, with `chosen_over_plain` the
-ratio to the plain form.
+unchanged), `culled_sparse_fp32` / `culled_sparse_graph_fp32` (culling plus the
+visibility-masked Adam step on the Morton-ordered model the trainer's spatial
+order keeps; Gaussians outside the view keep p, m, v) and
+`precision_bf16_culled_sparse` / `..._graph` (all of that plus SH rows and their
+Adam moments stored in bf16 with stochastic rounding; fp32 blending and
+accumulation). `value` is the fastest form that completed without a record
+overflow; all are in `forms`, with `chosen_over_plain` the ratio to the plain
+form. The held-out PSNR of each form's full training run is measured by
+synthetic_run.py (the metric's 0.1 dB condition).
 
 Printed JSON line: `value` is iterations/s with targets resident in HBM,
 `e2e` the same through host buffers (pinned H2D target upload and a D2H loss
@@ -70,6 +74,7 @@ def parse():
     p.add_argument("--views", type=int, default=0, help="number of training views used (0 = all 180)")
     p.add_argument("--precision", action="store_true", help="with --profile-only: run the precision form")
     p.add_argument("--culled", action="store_true", help="with --profile-only: exact tile culling on")
+    p.add_argument("--sparse", action="store_true", help="with --profile-only: sparse Adam on the Morton-ordered model")
     p.add_argument("--no-multiview", action="store_true", help="skip the 32-view multi-view measurement")
     return p.parse_args()
 
@@ -325,17 +330,27 @@ def run_gsn(args):
     class Form:
         """One form of the iteration: its own renderer, solver and parameter block."""
 
-        def __init__(self, bf16, culled=False):
+        def __init__(self, bf16, culled=False, sparse=False):
             self.renderer, self.solver = gsn.Renderer(), gsn.Solver()
             self.renderer.set_stream(sp)
             self.solver.set_stream(sp)
             self.renderer.set_exact_culling(culled)
+            self.solver.set_sparse_adam(sparse)
+            block = model
+            if sparse:
+                # the trainer's spatial order (Morton order of the means after every
+                # density step) - the order of the steady-state model it trains
+                dev_model = torch.from_numpy(model).cuda()
+                perm = torch.empty(n, dtype=torch.int32, device="cuda")
+                gsn.spatial_permutation(dev_model.data_ptr(), n, perm.data_ptr(), sp)
+                block = dev_model[:, perm.long()].cpu().numpy()
+                del dev_model, perm
             if bf16:
                 self.renderer.set_bf16_sh(True)
                 self.solver.set_bf16_sh(True)
-                self.params = gsn.to_precision_layout(model, torch)
+                self.params = gsn.to_precision_layout(block, torch)
             else:
-                self.params = torch.from_numpy(model).cuda()
+                self.params = torch.from_numpy(np.ascontiguousarray(block)).cuda()
 
     def step(f, k, e2e=False):
         cam = train[k % len(train)]
@@ -436,7 +451,7 @@ def run_gsn(args):
         return eager, graphed, stages, records, visible_count
 
     if args.profile_only:
-        f = Form(args.precision, args.culled)
+        f = Form(args.precision, args.culled, args.sparse)
         for k in range(args.warmup + 1):
             step(f, k)
         torch.cuda.synchronize()
@@ -453,7 +468,11 @@ def run_gsn(args):
     culled_eager, culled_graph, culled_stages, culled_records, _ = measure(culled)
     del culled
     torch.cuda.empty_cache()
-    prec = Form(True, True)
+    sparse = Form(False, True, True)
+    sparse_eager, sparse_graph, sparse_stages, _, _ = measure(sparse)
+    del sparse
+    torch.cuda.empty_cache()
+    prec = Form(True, True, True)
     prec_eager, prec_graph, prec_stages, _, _ = measure(prec)
     clocks = sampler.stop() if sampler else None
     del prec
@@ -500,8 +519,9 @@ def run_gsn(args):
         res = cpu_baseline(model, train[0], tgt0, extent, steps=1)
         cpu = {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")}
     forms = {"plain_fp32": plain_eager, "graph_fp32": plain_graph, "culled_fp32": culled_eager,
-             "culled_graph_fp32": culled_graph, "precision_bf16_culled": prec_eager,
-             "precision_bf16_culled_graph": prec_graph}
+             "culled_graph_fp32": culled_graph, "culled_sparse_fp32": sparse_eager,
+             "culled_sparse_graph_fp32": sparse_graph, "precision_bf16_culled_sparse": prec_eager,
+             "precision_bf16_culled_sparse_graph": prec_graph}
     valid = {k: v for k, v in forms.items() if v.get("status", 0) == 0}
     chosen = max(valid, key=lambda k: valid[k]["value"])
     out = {
@@ -522,6 +542,7 @@ def run_gsn(args):
         "roofline": roofline,
         "stages": stage_table,
         "stages_culled": {k: round(v, 4) for k, v in culled_stages.items()},
+        "stages_culled_sparse": {k: round(v, 4) for k, v in sparse_stages.items()},
         "stages_precision": {k: round(v, 4) for k, v in prec_stages.items()},
         "records": {"plain": records, "culled": culled_records},
         "multiview": multiview,

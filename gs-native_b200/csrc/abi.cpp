@@ -19,6 +19,7 @@
 #include "core/render/multiview_renderer.h"
 #include "core/render/renderer.h"
 #include "core/solver/solver.h"
+#include "core/spatial/spatial_order.h"
 #include "kernels.h"
 #include "knn_kernels.h"
 #include "profile.h"
@@ -306,6 +307,12 @@ int gsn_solver_set_tensor_core_loss(gsn_solver* s, int enabled) {
     return GSN_OK;
 }
 
+int gsn_solver_set_sparse_adam(gsn_solver* s, int enabled) {
+    if (!s) return GSN_ERR_INVALID_ARGUMENT;
+    s->impl.SetSparseAdam(enabled != 0);
+    return GSN_OK;
+}
+
 int gsn_solver_status(gsn_solver* s, int* status) {
     if (!s || !status) return GSN_ERR_INVALID_ARGUMENT;
     *status = GSN_OK;
@@ -486,6 +493,8 @@ int gsn_training_options_default(gsn_training_options* out) {
     out->learned_confidence = o.learned_confidence;
     out->log_density = o.log_density ? 1 : 0;
     out->exact_culling = o.exact_culling ? 1 : 0;
+    out->sparse_adam = o.sparse_adam ? 1 : 0;
+    out->spatial_order = o.spatial_order ? 1 : 0;
     return GSN_OK;
 }
 
@@ -524,6 +533,8 @@ gs_native::TrainingOptions ToOptions(const gsn_training_options& in) {
     o.learned_confidence = in.learned_confidence;
     o.log_density = in.log_density != 0;
     o.exact_culling = in.exact_culling != 0;
+    o.sparse_adam = in.sparse_adam != 0;
+    o.spatial_order = in.spatial_order != 0;
     return o;
 }
 }  // namespace
@@ -595,6 +606,23 @@ int gsn_trainer_evaluate_metrics(gsn_trainer* t, const gsn_camera* cameras, cons
         imgs.push_back(images[k]);
     }
     return t->impl.EvaluateMetrics(cams, imgs, psnr, ssim, l1, loss) ? GSN_OK : GSN_ERR_INVALID_ARGUMENT;
+}
+
+int gsn_spatial_permutation(const float* params, int count, uint32_t* perm, void* stream) {
+    if (!params || !perm || count <= 0) return GSN_ERR_INVALID_ARGUMENT;
+    gs_native::SpatialOrder order;
+    order.SetStream(static_cast<cudaStream_t>(stream));
+    if (!order.Compute(params, count)) return GSN_ERR_CUDA;
+    if (cudaMemcpyAsync(perm, order.GetPermutation(), sizeof(uint32_t) * count, cudaMemcpyDeviceToDevice,
+                        static_cast<cudaStream_t>(stream)) != cudaSuccess ||
+        cudaStreamSynchronize(static_cast<cudaStream_t>(stream)) != cudaSuccess)
+        return GSN_ERR_CUDA;
+    return GSN_OK;
+}
+
+int gsn_gather_gaussians(const float* src, float* dst, const uint32_t* perm, int count, int bf16_sh, void* stream) {
+    if (!src || !dst || !perm || count <= 0 || src == dst) return GSN_ERR_INVALID_ARGUMENT;
+    return gsn::launch_gather_gaussians(src, dst, perm, count, bf16_sh != 0, static_cast<cudaStream_t>(stream));
 }
 
 int gsn_eval_metrics(const float* image, const uint8_t* target, int width, int height, double* out, void* stream) {

@@ -363,7 +363,9 @@ __global__ void __launch_bounds__(256, 2) gaussian_update_kernel(GaussianUpdateA
             for (int k = 0; k < kShStride; ++k)
                 a.grads_out[(GSN_SH_INDEX + c * kShStride + k) * N + i] = k < K ? ch.grgb[c] * ch.basis[k] : 0.0f;
     }
-    if (!a.m) return;
+    // visibility-masked (sparse) Adam: a Gaussian outside the view keeps its
+    // parameters and moments (no momentum step, no moment decay)
+    if (!a.m || (a.sparse && !visible)) return;
     float* __restrict__ P = a.params;
     float* __restrict__ M = a.m;
     float* __restrict__ V = a.v;

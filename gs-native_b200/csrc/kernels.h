@@ -194,6 +194,7 @@ struct GaussianUpdateArgs {
     const StepFrame* frame;   // optional: camera, lr[0], c1, c2 and seed come from the device frame
     bool bf16_sh;             // precision-form layout of params, m and v (10 fp32 + 48 bf16 rows)
     uint32_t seed;            // stochastic-rounding seed of the step (precision form)
+    bool sparse;              // visibility-masked Adam: Gaussians with tile_counts == 0 keep p, m, v
 };
 int launch_gaussian_update(const GaussianUpdateArgs& a, int sh_degree, cudaStream_t stream);
 
@@ -201,6 +202,17 @@ int launch_gaussian_update(const GaussianUpdateArgs& a, int sh_degree, cudaStrea
 // parent's entry, or zero for parent -1 / out of range.
 int launch_remap_moments(const int* parents, const float* prev_m, const float* prev_v, float* m, float* v,
                          int prev_count, int count, bool bf16_sh, cudaStream_t stream);
+
+// ---------------------------------------------------------------- spatial order
+// Morton keys (30 bits, 10 per axis inside the bounding box of the finite
+// means; bounds: 6 ints of device scratch) for a spatial permutation of the
+// Gaussians (spatial.cu); the row gather dst[r][i] = src[r][perm[i]] of a
+// parameter or moment block in either layout; and parents'[i] = parents[perm[i]]
+// (perm[i] itself when parents is null).
+int launch_morton_keys(const float* params, int n, int* bounds, uint32_t* keys, cudaStream_t stream);
+int launch_gather_gaussians(const float* src, float* dst, const uint32_t* perm, int n, bool bf16_sh,
+                            cudaStream_t stream);
+int launch_compose_parents(const int* parents, const uint32_t* perm, int n, int* out, cudaStream_t stream);
 
 // ---------------------------------------------------------------- tcgen05
 // D (128 x 64 fp32, row-major) = A (128 x 128) * B^T (B: 64 x 128), operands

@@ -278,6 +278,10 @@ class Solver:
     def set_bf16_sh(self, enabled=True):
         _check(lib().gsn_solver_set_bf16_sh(self.handle, int(bool(enabled))), "set_bf16_sh")
 
+    def set_sparse_adam(self, enabled=True):
+        fn = declare("gsn_solver_set_sparse_adam", [ctypes.c_void_p, ctypes.c_int])
+        _check(fn(self.handle, int(bool(enabled))), "set_sparse_adam")
+
     def set_tensor_core_loss(self, enabled=True):
         _check(lib().gsn_solver_set_tensor_core_loss(self.handle, int(bool(enabled))), "set_tensor_core_loss")
 
@@ -436,7 +440,7 @@ class TrainingOptions(ctypes.Structure):
         ("density_seed", ctypes.c_ulonglong), ("initial_opacity", ctypes.c_float),
         ("precision", ctypes.c_int), ("graph", ctypes.c_int),
         ("learned_density", ctypes.c_int), ("learned_confidence", ctypes.c_float), ("log_density", ctypes.c_int),
-        ("exact_culling", ctypes.c_int),
+        ("exact_culling", ctypes.c_int), ("sparse_adam", ctypes.c_int), ("spatial_order", ctypes.c_int),
     ]
 
     @classmethod
@@ -881,4 +885,19 @@ def eval_metrics(image_ptr, target_ptr, width, height, stream=0):
     _check(fn(ctypes.c_void_p(image_ptr), ctypes.c_void_p(target_ptr), int(width), int(height), out,
               ctypes.c_void_p(stream)), "eval_metrics")
     return dict(psnr=out[0], ssim=out[1], l1=out[2], mse=out[3])
+
+
+def spatial_permutation(params_ptr, count, perm_ptr, stream=0):
+    """Morton-order permutation of a device parameter block into perm (device uint32[count])."""
+    fn = declare("gsn_spatial_permutation", [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p])
+    _check(fn(ctypes.c_void_p(params_ptr), int(count), ctypes.c_void_p(perm_ptr), ctypes.c_void_p(stream)),
+           "spatial_permutation")
+
+
+def gather_gaussians(src_ptr, dst_ptr, perm_ptr, count, bf16_sh=False, stream=0):
+    """dst[r][i] = src[r][perm[i]] over a device parameter / moment block."""
+    fn = declare("gsn_gather_gaussians", [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                          ctypes.c_int, ctypes.c_void_p])
+    _check(fn(ctypes.c_void_p(src_ptr), ctypes.c_void_p(dst_ptr), ctypes.c_void_p(perm_ptr), int(count),
+              int(bool(bf16_sh)), ctypes.c_void_p(stream)), "gather_gaussians")
 

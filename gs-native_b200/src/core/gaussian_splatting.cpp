@@ -94,8 +94,14 @@ bool GaussianSplatting::Initialize(const TrainingScene& scene, const TrainingOpt
     eval_renderer_.SetBf16Sh(options_.bf16_sh);
     solver_.SetBf16Sh(options_.bf16_sh);
     density_.SetBf16Sh(options_.bf16_sh);
+    solver_.SetSparseAdam(options_.sparse_adam);
+    spatial_.SetStream(stream_);
     graph_.Release();
     if (!InitializeGaussians(scene.point_positions, scene.point_colors, scene.point_count)) return false;
+    if (options_.spatial_order && gaussians_.gaussian_count_ > 0 &&
+        (!spatial_.Compute(gaussians_.gaussians_, gaussians_.gaussian_count_) ||
+         !spatial_.Apply(gaussians_.gaussians_, gaussians_.gaussian_count_, options_.bf16_sh, nullptr)))
+        return false;
     return cudaStreamSynchronize(stream_) == cudaSuccess;
 }
 
@@ -305,13 +311,29 @@ bool GaussianSplatting::ControlDensity() {
             return false;
         density_log_.features = density_features_.get();
         density_log_.decisions = density_codes_.get();
-        density_log_.parents = density_.GetParentIds();
+        density_log_.parents = density_.GetParentIds();  // composed with the spatial order below
         density_log_.before = before;
         density_log_.after = gaussians_.gaussian_count_;
         density_log_.iteration = completed_;
         ++density_log_.steps;
     }
-    return solver_.RemapGaussians(density_.GetHistoryParentIds(), gaussians_.gaussian_count_);
+    const int* history = density_.GetHistoryParentIds();
+    const int after = gaussians_.gaussian_count_;
+    if (options_.spatial_order && after > 0) {
+        // the density step's statistics are zero again, so only the parameters,
+        // the Adam history map and the logged parent map follow the permutation
+        if (!spatial_.Compute(gaussians_.gaussians_, after) ||
+            !spatial_.Apply(gaussians_.gaussians_, after, options_.bf16_sh, history))
+            return false;
+        if (options_.log_density) {
+            if (!log_parents_.Reserve(static_cast<size_t>(after)) ||
+                !spatial_.Compose(density_log_.parents, log_parents_.get()))
+                return false;
+            density_log_.parents = log_parents_.get();
+        }
+        history = spatial_.GetParents();
+    }
+    return solver_.RemapGaussians(history, after);
 }
 
 bool GaussianSplatting::SetDensityMlp(const float* weights) {

@@ -27,6 +27,7 @@
 #include "core/graph/training_graph.h"
 #include "core/render/renderer.h"
 #include "core/solver/solver.h"
+#include "core/spatial/spatial_order.h"
 #include "core/types/buffers.h"
 #include "util/device_array.h"
 
@@ -72,6 +73,11 @@ struct TrainingOptions {
     float learned_confidence = 0.9f;
     bool log_density = false;  // keep the statistics and decisions of the last control step (GetDensityLog)
     bool exact_culling = false;  // training renderer emits only records that can contribute (Renderer::SetExactCulling)
+    // visibility-masked Adam (Solver::SetSparseAdam): Gaussians outside the view keep p, m, v
+    bool sparse_adam = false;
+    // Morton order of the Gaussians after initialisation and every density step
+    // (SpatialOrder): no value changes, the sparse update skips whole sectors
+    bool spatial_order = false;
 };
 
 // Statistics, decisions and parent map of the last density-control step
@@ -152,6 +158,8 @@ private:
     size_t target_stride_ = 0;  // bytes per resident training image
     GaussianBuffers gaussians_;
     Renderer renderer_;
+    SpatialOrder spatial_;
+    DeviceArray<int> log_parents_;  // density-log parent map composed with the spatial order
     Renderer eval_renderer_;  // Render / Evaluate (the training renderer may be bound to a graph)
     Solver solver_;
     DensityController density_;

@@ -165,6 +165,7 @@ bool Solver::UpdateGaussians(const CameraParams& camera, const Renderer& rendere
     a.grads_out = grads_out;
     a.frame = frame_;
     a.bf16_sh = bf16_sh_;
+    a.sparse = sparse_adam_;
     a.seed = static_cast<uint32_t>(iteration);
     gsn::stage_mark(stream_, gsn::kStageGaussianUpdate);
     if (gsn::launch_gaussian_update(a, std::clamp(sh_degree, 0, 3), stream_) != GSN_OK) return false;

@@ -91,6 +91,11 @@ public:
     // GEMMs, hi/lo bf16 split, fp32 accumulation). On by default in the
     // precision form; can be switched independently.
     void SetTensorCoreLoss(bool enabled) { tensor_core_loss_ = enabled; }
+    // Visibility-masked (sparse) Adam: Gaussians without a tile in the frame
+    // (the renderer's rectangle count is 0) keep their parameters and moments;
+    // the reference updates all of them every iteration (solver.cu:912-915).
+    void SetSparseAdam(bool enabled) { sparse_adam_ = enabled; }
+    bool GetSparseAdam() const { return sparse_adam_; }
     bool GetTensorCoreLoss() const { return tensor_core_loss_; }
     // Device status word of the tensor-core passes: 0, or GSN_ERR_TIMEOUT.
     const int* GetStatusDevice() const { return status_.get(); }
@@ -125,6 +130,7 @@ private:
     const gsn::StepFrame* frame_ = nullptr;
     bool bf16_sh_ = false;
     bool tensor_core_loss_ = false;
+    bool sparse_adam_ = false;
     DeviceArray<int> status_;
 };
 

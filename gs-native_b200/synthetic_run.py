@@ -10,7 +10,7 @@ wall and device time, the final Gaussian count and the mean FP64 PSNR of the
 held-out views.
 
     python synthetic_run.py [--iterations 30000] [--cap 1200000] [--width 1600 --height 1064]
-                            [--precision] [--graph]
+                            [--precision] [--graph] [--culled] [--sparse]
 """
 import argparse
 import json
@@ -65,6 +65,8 @@ def main():
     p.add_argument("--chunk", type=int, default=1000)
     p.add_argument("--precision", action="store_true", help="precision form (bf16 SH, tensor-core SSIM)")
     p.add_argument("--graph", action="store_true", help="steady-state iterations as CUDA-graph replays")
+    p.add_argument("--culled", action="store_true", help="exact tile culling in the training renderer")
+    p.add_argument("--sparse", action="store_true", help="visibility-masked Adam on the Morton-ordered model")
     args = p.parse_args()
     import torch
 
@@ -73,7 +75,8 @@ def main():
     train, test, train_images, test_images, points, colors = build_scene(args, torch)
     setup_s = time.time() - t0
     opts = gsn.TrainingOptions.defaults(max_gaussians=args.cap, precision=int(args.precision),
-                                        graph=int(args.graph))
+                                        graph=int(args.graph), exact_culling=int(args.culled),
+                                        sparse_adam=int(args.sparse), spatial_order=int(args.sparse))
     trainer = gsn.Trainer()
     assert trainer.initialize(train, train_images, points, colors, opts) == 0
     torch.cuda.synchronize()
@@ -100,7 +103,8 @@ def main():
         "iters_per_s": round(args.iterations / (device_ms / 1000.0), 2), "gaussians": st["count"],
         "psnr_test_db": round(psnr, 4), "loss_test": round(loss, 6), "psnr_train_subset_db": round(psnr_train, 4),
         "setup_s": round(setup_s, 1), "resolution": [args.width, args.height], "cap": args.cap,
-        "form": ("precision_bf16" if args.precision else "plain_fp32") + ("_graph" if args.graph else ""), "log": log,
+        "form": ("precision_bf16" if args.precision else "plain_fp32") + ("_culled" if args.culled else "") +
+                ("_sparse" if args.sparse else "") + ("_graph" if args.graph else ""), "log": log,
     }), flush=True)
 
 

@@ -218,6 +218,10 @@ int gsn_solver_status(gsn_solver* s, int* status);
 int gsn_solver_loss(gsn_solver* s, double* out);
 int gsn_solver_loss_device(gsn_solver* s, const double** out);
 
+/* Visibility-masked (sparse) Adam (gs-native extension): Gaussians with no tile
+ * in the frame keep parameters and moments; the reference updates all
+ * 58 x N every iteration (solver.cu:912-915). */
+int gsn_solver_set_sparse_adam(gsn_solver* s, int enabled);
 /* Stage entry points of Iterate for parity tests and partial pipelines:
  * dL/dimage into the solver's buffer (device float[pixels * 3] via *out);
  * screen-space gradients ([count][12] floats via *out); mapped parameter
@@ -318,6 +322,8 @@ typedef struct gsn_training_options {
     float learned_confidence;        /* 0.9: softmax probability needed to override the threshold rule */
     int log_density;                 /* 1: keep the last control step's statistics (gsn_trainer_density_log) */
     int exact_culling;               /* 1: exact tile culling in the training renderer (gsn_renderer_set_exact_culling) */
+    int sparse_adam;                 /* 1: visibility-masked Adam (gsn_solver_set_sparse_adam) */
+    int spatial_order;               /* 1: Morton order of the Gaussians after init and every density step */
 } gsn_training_options;
 
 int gsn_training_options_default(gsn_training_options* out);
@@ -448,6 +454,16 @@ int gsn_mlp_infer(gsn_mlp* m, const float* features, int n, float confidence, in
 int gsn_ply_write(const char* path, const float* params, int count);
 int gsn_ply_read_count(const char* path, int* count);
 int gsn_ply_read(const char* path, float* params, int count);
+
+/* ------------------------------------------------------------------ spatial order
+ * gs-native extension: a Morton-order permutation of the Gaussians (30-bit keys
+ * of the means inside their bounding box; ties keep id order) and the row
+ * gather that applies it to a parameter or Adam-moment block (dst[r][i] =
+ * src[r][perm[i]], 58 fp32 rows, or the precision layout when bf16_sh). No
+ * rendered or trained value depends on the order; locality does. Device
+ * pointers; perm holds count uint32. */
+int gsn_spatial_permutation(const float* params, int count, uint32_t* perm, void* stream);
+int gsn_gather_gaussians(const float* src, float* dst, const uint32_t* perm, int count, int bf16_sh, void* stream);
 
 /* ------------------------------------------------------------------ COLMAP scene
  * ReadColmapScene (reference src/io/data_io.cpp:328-418) without OpenCV:
