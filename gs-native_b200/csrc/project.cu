@@ -121,8 +121,12 @@ __device__ __forceinline__ int cull_count(float2 mean, float4 q, int4 rect) {
     return total;
 }
 
-// Records of the culled counts in depth order: the four lanes of a Gaussian
-// walk its rows, each row's column interval split across the lanes.
+// Records of the culled counts in depth order. Four lanes serve a Gaussian and
+// take its rows four at a time, one row each: a lane finds its row's column
+// interval, the group's exclusive prefix of the interval widths (shuffles
+// within the four lanes) places the row, and the lane writes the row's records.
+// The loop runs the warp's largest number of row groups so every shuffle sees
+// all 32 lanes.
 __global__ void __launch_bounds__(256) emit_records_culled(const uint32_t* __restrict__ sorted_ids,
                                                            const int* __restrict__ record_start,
                                                            const int4* __restrict__ rects,
@@ -134,28 +138,49 @@ __global__ void __launch_bounds__(256) emit_records_culled(const uint32_t* __res
     const int64_t gidx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     const int64_t p = gidx >> 2;
     const int sub = static_cast<int>(gidx & 3);
-    if (p >= n) return;
-    const int begin = record_start[p];
-    const int count = record_start[p + 1] - begin;
-    if (count <= 0) return;
-    if (begin + static_cast<int64_t>(count) > capacity) {
-        if (sub == 0 && overflow) atomicExch(overflow, 1);
-        return;
-    }
-    const uint32_t id = sorted_ids[p];
-    const int4 r = rects[id];
-    const CullShape s = cull_shape(means[id], conic_opacity[id]);
-    int k = 0;
-    for (int ty = r.y; ty < r.w && k < count; ++ty) {
-        const int2 span = cull_row_span(s, r, ty);
-        const int w = span.y - span.x;
-        for (int j = sub; j < w && k + j < count; j += 4) {
-            tile_keys[begin + k + j] = static_cast<uint32_t>(ty * tile_count_x + span.x + j);
-            record_ids[begin + k + j] = id;
+    bool active = p < n;
+    int begin = 0, count = 0;
+    if (active) {
+        begin = record_start[p];
+        count = record_start[p + 1] - begin;
+        active = count > 0;
+        if (active && begin + static_cast<int64_t>(count) > capacity) {
+            if (sub == 0 && overflow) atomicExch(overflow, 1);
+            active = false;
         }
-        k += w;
     }
-    if (k != count && sub == 0 && overflow) atomicExch(overflow, 2);
+    uint32_t id = 0;
+    int4 r = make_int4(0, 0, 0, 0);
+    CullShape s{};
+    if (active) {
+        id = sorted_ids[p];
+        r = rects[id];
+        s = cull_shape(means[id], conic_opacity[id]);
+    }
+    const int groups = active ? (r.w - r.y + 3) / 4 : 0;
+    const int rounds = __reduce_max_sync(0xffffffffu, groups);
+    int k = 0;
+    for (int g = 0; g < rounds; ++g) {
+        const int ty = r.y + 4 * g + sub;
+        int2 span = make_int2(0, 0);
+        if (g < groups && ty < r.w) span = cull_row_span(s, r, ty);
+        const int w = span.y - span.x;
+        // exclusive prefix of the widths over the four lanes of this Gaussian
+        int incl = w;
+#pragma unroll
+        for (int o = 1; o < 4; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o, 4);
+            if (sub >= o) incl += y;
+        }
+        const int group_total = __shfl_sync(0xffffffffu, incl, 3, 4);
+        const int at = k + incl - w;
+        for (int j = 0; j < w && at + j < count; ++j) {
+            tile_keys[begin + at + j] = static_cast<uint32_t>(ty * tile_count_x + span.x + j);
+            record_ids[begin + at + j] = id;
+        }
+        k += group_total;
+    }
+    if (active && k != count && sub == 0 && overflow) atomicExch(overflow, 2);
 }
 
 // kBf16: precision form (bf16 SH rows; near-singular conics inverted in FP64).

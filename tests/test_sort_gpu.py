@@ -50,3 +50,34 @@ def test_sort_pairs_rejects_bad_arguments():
     assert st != 0
     st, _ = gsn.sort_pairs(0, 0, 0, 0, 10, 0, 33, 0, 0)
     assert st != 0
+
+
+@pytest.mark.parametrize("case", ["constant", "skewed_top_byte", "few_distinct"])
+def test_sort_pairs_skewed_digits(case):
+    """Digit distributions the histogram and the look-back must survive: one
+    bucket holding every key, depth-like keys whose exponent byte barely varies,
+    and a handful of distinct keys over 3M pairs (1,500 chunks of look-back)."""
+    rng = np.random.default_rng(7)
+    n = 3_000_000
+    if case == "constant":
+        keys = np.full(n, 0x40A00000, dtype=np.uint32)
+    elif case == "skewed_top_byte":
+        keys = rng.uniform(2.0, 30.0, n).astype(np.float32).view(np.uint32)
+        keys[::97] = 0xFFFFFFFF  # culled entries sort last, as in the renderer
+    else:
+        keys = rng.integers(0, 5, n).astype(np.uint32) * 0x01010101
+    values = np.arange(n, dtype=np.uint32)
+    k, v = run_sort(keys, values, 0, 32)
+    ek, ev = expected(keys, values, 0, 32)
+    assert np.array_equal(k, ek) and np.array_equal(v, ev)
+
+
+def test_sort_pairs_many_chunks_tile_bits():
+    """8M records on 13 tile bits (two passes, 3,900 chunks per pass)."""
+    rng = np.random.default_rng(11)
+    n = 8_000_000
+    keys = rng.integers(0, 6700, n).astype(np.uint32)
+    values = rng.integers(0, 2 ** 31, n).astype(np.uint32)
+    k, v = run_sort(keys, values, 0, 13)
+    ek, ev = expected(keys, values, 0, 13)
+    assert np.array_equal(k, ek) and np.array_equal(v, ev)
