@@ -75,6 +75,7 @@ def parse():
     p.add_argument("--precision", action="store_true", help="with --profile-only: run the precision form")
     p.add_argument("--culled", action="store_true", help="with --profile-only: exact tile culling on")
     p.add_argument("--sparse", action="store_true", help="with --profile-only: sparse Adam on the Morton-ordered model")
+    p.add_argument("--multiview", action="store_true", help="with --profile-only: the 32-view multi-view render")
     p.add_argument("--no-multiview", action="store_true", help="skip the 32-view multi-view measurement")
     return p.parse_args()
 
@@ -451,6 +452,18 @@ def run_gsn(args):
         return eager, graphed, stages, records, visible_count
 
     if args.profile_only:
+        if args.multiview:
+            # the 32-view persistent render in the default configuration, warmup + 1 times
+            import scenes
+            cams = scenes.multiview_cameras(32, seed=23)
+            p = torch.from_numpy(model).cuda()
+            imgs = [torch.empty((c.height, c.width, 3), device="cuda") for c in cams]
+            mv = gsn.MultiView()
+            mv.set_stream(sp)
+            for _ in range(args.warmup + 1):
+                mv.render(p.data_ptr(), n, cams, [x.data_ptr() for x in imgs], [0, 0, 0], SH_DEGREE)
+            torch.cuda.synchronize()
+            return
         f = Form(args.precision, args.culled, args.sparse)
         for k in range(args.warmup + 1):
             step(f, k)
