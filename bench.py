@@ -57,8 +57,14 @@ TARGET_GAUSSIANS = 1_500_000
 MODEL_GAUSSIANS = 1_200_000
 # DRAM bytes (read + write) of one gaussian_update launch on this workload, from
 # the ncu capture summarised in profiles/gaussian_update_plain_1.2M.md.
-NCU_TRAFFIC = {"gaussian_update": 900_431_104 + 801_656_576}
-NCU_TRAFFIC_SOURCE = "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/gaussian_update_plain_1.2M.md"
+# DRAM bytes (read + write) of one gaussian_update launch on this workload, per
+# update form, from the ncu captures summarised in profiles/.
+NCU_TRAFFIC = {
+    "dense": (900_431_104 + 801_656_576,
+              "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/gaussian_update_plain_1.2M.md"),
+    "sparse": (604_525_312 + 483_656_704,
+               "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/gaussian_update_sparse_1.2M.md"),
+}
 
 
 def parse():
@@ -144,20 +150,27 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
-def algorithmic_bytes(n, records, tiles, pixels, s=16, tile_passes=2, visible=None):
-    """Compulsory HBM bytes per launch of each stage (formulas in DESIGN.md)."""
+def algorithmic_bytes(n, records, tiles, pixels, s=16, tile_passes=2, visible=None, culled=False, sparse=False,
+                      bf16=False):
+    """Compulsory HBM bytes per launch of each stage (formulas in DESIGN.md) for
+    a form: culled records are emitted with their conic (36 B per visible
+    Gaussian), the sparse update moves only visible Gaussians' rows, the
+    precision layout stores the 48 SH rows in 2 bytes."""
     vis = n if visible is None else visible
+    sh_bytes = 2 if bf16 else 4
+    row_bytes = 10 * 4 + 3 * s * sh_bytes              # one Gaussian's parameter rows
+    updated = vis if sparse else n
     return {
-        "project": n * (4 * (10 + 3 * s) + 68),
+        "project": n * (row_bytes + 68),
         "depth_sort": 4 * n * 20,
         "record_scan": n * 20,
-        "emit_records": records * 8 + vis * 24,
+        "emit_records": records * 8 + vis * (36 if culled else 24),
         "tile_sort": tile_passes * records * 20,
         "tile_ranges": records * 4 + (tiles + 1) * 8,
         "raster_forward": records * 40 + pixels * 16,
         "loss_gradient": pixels * 3 * 9,
         "raster_backward": records * 40 + pixels * 28 + vis * 48,
-        "gaussian_update": n * (58 * 4 * 6 + 48 + 4 + 16),
+        "gaussian_update": updated * row_bytes * 6 + n * (48 + 4 + 16),
     }
 
 
@@ -502,7 +515,8 @@ def run_gsn(args):
     tiles = cam.tile_count_x * cam.tile_count_y
     pixels = cam.width * cam.height
     tile_bits = max(1, (tiles - 1).bit_length())
-    alg = algorithmic_bytes(n, records, tiles, pixels, tile_passes=(tile_bits + 7) // 8, visible=vis)
+    passes = (tile_bits + 7) // 8
+    alg = algorithmic_bytes(n, records, tiles, pixels, tile_passes=passes, visible=vis)
     peak, peak_kind = load_peaks()
     stage_table = {}
     for name, t in stages.items():
@@ -511,32 +525,43 @@ def run_gsn(args):
             gbs = alg[name] / (t / 1000.0) / 1e9
             entry.update(bytes=int(alg[name]), gbs=round(gbs, 1), hbm_frac=round(gbs / peak, 4))
         stage_table[name] = entry
-    kernel_stages = {k: v for k, v in stages.items() if k in alg}
-    dominant = max(kernel_stages, key=kernel_stages.get)
-    hbm_stages = {k: v for k, v in kernel_stages.items() if k in ("gaussian_update", "project", "depth_sort",
-                                                                     "tile_sort", "emit_records", "loss_gradient")}
-    top_hbm = max(hbm_stages, key=hbm_stages.get)
-    achieved = alg[top_hbm] / (stages[top_hbm] / 1000.0) / 1e9
-    roofline = {"bound": "hbm", "kernel": top_hbm, "achieved": round(achieved, 1), "peak": peak,
-                "unit": "GB/s", "frac": round(achieved / peak, 4),
-                "traffic": NCU_TRAFFIC.get(top_hbm) if n == MODEL_GAUSSIANS else None,
-                "traffic_source": NCU_TRAFFIC_SOURCE if top_hbm in NCU_TRAFFIC else None,
-                "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured" else
-                "fallback 6650 GB/s",
-                "dominant_kernel": dominant,
-                "dominant_note": ("the per-tile blend kernels are bound by the FP32/MUFU issue rate and the "
-                                  "atomics of the backward, not by HBM; their HBM fractions are in `stages`")}
-    cpu = None
-    if not args.no_cpu_baseline and world == 1:
-        tgt0 = targets[0].cpu().numpy()
-        res = cpu_baseline(model, train[0], tgt0, extent, steps=1)
-        cpu = {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")}
     forms = {"plain_fp32": plain_eager, "graph_fp32": plain_graph, "culled_fp32": culled_eager,
              "culled_graph_fp32": culled_graph, "culled_sparse_fp32": sparse_eager,
              "culled_sparse_graph_fp32": sparse_graph, "precision_bf16_culled_sparse": prec_eager,
              "precision_bf16_culled_sparse_graph": prec_graph}
     valid = {k: v for k, v in forms.items() if v.get("status", 0) == 0}
     chosen = max(valid, key=lambda k: valid[k]["value"])
+
+    def roofline_of(form):
+        """Roofline of the largest HBM-bound stage of a form, from its live stage times."""
+        culled_f, sparse_f, bf16_f = "culled" in form, "sparse" in form, form.startswith("precision")
+        st = prec_stages if bf16_f else sparse_stages if sparse_f else culled_stages if culled_f else stages
+        rec = culled_records if culled_f else records
+        ab = algorithmic_bytes(n, rec, tiles, pixels, tile_passes=passes, visible=vis, culled=culled_f,
+                               sparse=sparse_f, bf16=bf16_f)
+        kernel_stages = {k: v for k, v in st.items() if k in ab}
+        hbm = {k: v for k, v in kernel_stages.items() if k in ("gaussian_update", "project", "depth_sort",
+                                                                "tile_sort", "emit_records", "loss_gradient")}
+        top = max(hbm, key=hbm.get)
+        achieved = ab[top] / (st[top] / 1000.0) / 1e9
+        traffic = None
+        if top == "gaussian_update" and n == MODEL_GAUSSIANS and not bf16_f:
+            traffic = NCU_TRAFFIC["sparse" if sparse_f else "dense"]
+        return {"bound": "hbm", "kernel": top, "form": form, "achieved": round(achieved, 1), "peak": peak,
+                "unit": "GB/s", "frac": round(achieved / peak, 4), "algorithmic_bytes": int(ab[top]),
+                "traffic": traffic[0] if traffic else None, "traffic_source": traffic[1] if traffic else None,
+                "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured" else
+                "fallback 6650 GB/s",
+                "dominant_kernel": max(kernel_stages, key=kernel_stages.get),
+                "dominant_note": ("the per-tile blend kernels are bound by the FP32/MUFU issue rate and the "
+                                  "atomics of the backward, not by HBM; their HBM fractions are in `stages`")}
+
+    roofline = roofline_of(chosen)
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        tgt0 = targets[0].cpu().numpy()
+        res = cpu_baseline(model, train[0], tgt0, extent, steps=1)
+        cpu = {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")}
     out = {
         "metric": METRIC, "value": forms[chosen]["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": forms[chosen]["ms_per_step"], "higher_is_better": True,
@@ -553,6 +578,9 @@ def run_gsn(args):
         "e2e": {"value": forms[chosen]["e2e"], "unit": UNIT, "h2d_bytes_per_step": 1600 * 1064 * 3,
                 "d2h_bytes_per_step": 32, "psnr_db_last_step": forms[chosen]["psnr_db_last_step"]},
         "roofline": roofline,
+        "roofline_plain": roofline_of("plain_fp32"),
+        "psnr_note": ("psnr_db_last_step is the training view's PSNR after this run's ~1,000 steps from the random "
+                      "model; the 0.1 dB condition is on held-out PSNR of full training runs (synthetic_run.py)"),
         "stages": stage_table,
         "stages_culled": {k: round(v, 4) for k, v in culled_stages.items()},
         "stages_culled_sparse": {k: round(v, 4) for k, v in sparse_stages.items()},
