@@ -12,9 +12,9 @@
 2. fit(): the MLP (16 -> 64 -> 64 -> 4, fp16 weights, fp32 accumulation) is
    trained on the GPU by the library's fused forward/backward kernels.
 3. judge(): the learned policy (with the threshold rule as fallback below the
-   confidence threshold) and the plain rule train from the same start; the
-   proposal policy is accepted only if its held-out PSNR is within 0.1 dB of
-   the plain rule's.
+   confidence threshold) and the plain rule train from the same start over
+   paired runs with several density seeds; the proposal policy is accepted
+   only if its mean held-out PSNR is within 0.1 dB of the plain rule's.
 """
 import numpy as np
 
@@ -128,11 +128,25 @@ def train_run(scene, options, iterations, mlp_weights=None, confidence=0.9):
     return dict(psnr=psnr, loss=loss, count=count, gaussian_iterations=load)
 
 
-def judge(scene, options, iterations, mlp_weights, confidence=0.9, tolerance_db=0.1):
-    """Plain rule against the learned policy from the same start."""
-    plain = train_run(scene, options, iterations)
-    learned = train_run(scene, options, iterations, mlp_weights, confidence)
-    accepted = learned["psnr"] >= plain["psnr"] - tolerance_db
-    return dict(plain=plain, learned=learned, accepted=bool(accepted),
-                delta_db=learned["psnr"] - plain["psnr"],
-                load_ratio=learned["gaussian_iterations"] / max(plain["gaussian_iterations"], 1))
+def judge(scene, options, iterations, mlp_weights, confidence=0.9, tolerance_db=0.1, repeats=3):
+    """Plain rule against the learned policy from the same start, over `repeats`
+    paired runs (density seeds 0, 1, ...). Runs with density control diverge
+    chaotically from float-atomic noise (single-run held-out PSNR spreads by
+    ~0.3 dB on small scenes), so the verdict uses the mean of the paired PSNR
+    differences: accepted when it is at least -tolerance_db."""
+    plain, learned = [], []
+    for r in range(repeats):
+        opts = dict(options, density_seed=r)
+        plain.append(train_run(scene, opts, iterations))
+        learned.append(train_run(scene, opts, iterations, mlp_weights, confidence))
+    diffs = np.array([b["psnr"] - a["psnr"] for a, b in zip(plain, learned)])
+    delta = float(diffs.mean())
+    mean = lambda runs, key: float(np.mean([x[key] for x in runs]))  # noqa: E731
+    return dict(plain=dict(psnr=mean(plain, "psnr"), count=mean(plain, "count"),
+                           gaussian_iterations=mean(plain, "gaussian_iterations")),
+                learned=dict(psnr=mean(learned, "psnr"), count=mean(learned, "count"),
+                             gaussian_iterations=mean(learned, "gaussian_iterations")),
+                runs=dict(plain=[x["psnr"] for x in plain], learned=[x["psnr"] for x in learned]),
+                accepted=bool(delta >= -tolerance_db), delta_db=delta,
+                delta_std_db=float(diffs.std(ddof=1)) if repeats > 1 else 0.0,
+                load_ratio=mean(learned, "gaussian_iterations") / max(mean(plain, "gaussian_iterations"), 1.0))

@@ -74,12 +74,18 @@ def test_render_matches_plain_form_on_bf16_rounded_sh():
     assert np.mean(np.abs(a - b) <= 1e-6) > 0.99
 
 
-def run_steps(params, cam, target, bf16, steps=1, lr=1e-4):
+def run_steps(params, cam, target, bf16, steps=1, lr=1e-4, tensor_core_loss=False):
+    """Steps of either layout. The precision layout switches the solver to the
+    tensor-core SSIM; these storage tests keep the fp32 loss kernel so that both
+    forms run the same arithmetic and only the bf16 storage differs (the
+    tensor-core loss is pinned in test_loss_tc_gpu.py and
+    test_precision_error_gpu.py)."""
     t = torch()
     n = params.shape[1]
     r, s = gsn.Renderer(), gsn.Solver()
     r.set_bf16_sh(bf16)
     s.set_bf16_sh(bf16)
+    s.set_tensor_core_loss(tensor_core_loss)
     p = gsn.to_precision_layout(params, t) if bf16 else dev(params)
     img = empty((cam.height, cam.width, 3), t.float32)
     for _ in range(steps):
