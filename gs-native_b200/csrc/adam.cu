@@ -354,6 +354,23 @@ __global__ void __launch_bounds__(256, 2) gaussian_update_kernel(GaussianUpdateA
         ch.grgb[0] = ch.grgb[1] = ch.grgb[2] = 0.0f;
     }
     constexpr int K = (D + 1) * (D + 1);
+    if (a.max_radius && visible) {
+        // learned-policy statistics of the round (visible Gaussians only)
+        const float depth = a.depths[i];
+        a.max_radius[i] = fmaxf(a.max_radius[i], a.radii[i]);
+        a.depth_sum[i] += depth;
+        a.depth_sq[i] += depth * depth;
+        float gm = 0.0f, gs = 0.0f, basis2 = 0.0f, rgb2 = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            gm += ch.g[k] * ch.g[k];
+            gs += ch.g[3 + k] * ch.g[3 + k];
+            rgb2 += ch.grgb[k] * ch.grgb[k];
+        }
+#pragma unroll
+        for (int k = 0; k < K; ++k) basis2 += ch.basis[k] * ch.basis[k];
+        a.last_grad[i] = make_float4(sqrtf(gm), sqrtf(gs), fabsf(ch.g[9]), sqrtf(rgb2 * basis2));
+    }
     if (a.grads_out) {
 #pragma unroll
         for (int r = 0; r < 10; ++r) a.grads_out[r * N + i] = ch.g[r];

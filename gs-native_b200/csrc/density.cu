@@ -121,32 +121,27 @@ __global__ void codes_kernel(const int4* __restrict__ counts, int n, int8_t* __r
     codes[id] = c.z ? 2 : (c.y ? 1 : (c.x ? 0 : 3));
 }
 
-// The 16 per-Gaussian statistics of the learned density policy (normalised so
-// that the plain rule's thresholds sit at simple values):
-//  0 mean view-space gradient / gradient threshold   1 mean |gradient| / its threshold
-//  2 log(1 + observations)                            3 opacity
-//  4 opacity logit                                    5 log(max scale / split threshold)
-//  6 log(min scale / split threshold)                 7 mean log-scale - log(split threshold)
-//  8 max scale / prune-large world size               9 |SH DC|
-// 10 RMS of the higher SH coefficients               11 distance from the scene centre / extent
-// 12 log(max / min scale)                            13-15 plain rule: clone, split, prune
+// The 16 per-Gaussian statistics of the learned density policy, the list the
+// policy is specified on (accumulated view-space gradient norm and count, max
+// screen radius, 3 log-scales, opacity, SH DC norm and higher-band energy,
+// depth mean / variance, age, last-step gradient norms of mean / scale /
+// opacity / SH), each scaled to order one:
+//  0 round mean view-space gradient / gradient threshold   1 log(1 + round observations)
+//  2 log(1 + round max screen radius, px)                  3-5 log-scale - log(split threshold)
+//  6 opacity                                               7 |SH DC|
+//  8 higher-band SH energy (sum of squares)                9 round mean depth / scene extent
+// 10 round depth variance / extent^2                       11 age / 1000 iterations
+// 12-15 log(1 + 1e4 |g|) of the last visible step's gradient of mean, log-scale, opacity logit, SH
 template <bool kBf16>
 __global__ void features_kernel(const float* __restrict__ params, const float* __restrict__ sums,
-                                const float* __restrict__ abs_sums, const unsigned int* __restrict__ obs, int n,
-                                DensityThresholds th, float3 centre, float extent, float* __restrict__ out) {
+                                const unsigned int* __restrict__ obs, int n, DensityThresholds th, float extent,
+                                LearnedStatsView ls, float* __restrict__ out) {
     const int id = blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= n) return;
     const int64_t N = n;
-    const int4 c = plain_decision(params, sums, abs_sums, obs, N, id, th);
+    const float count = static_cast<float>(obs[id]);
     const float logit = params[static_cast<int64_t>(GSN_OPACITY_INDEX) * N + id];
-    float ls[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) ls[a] = params[static_cast<int64_t>(GSN_LOG_SCALE_INDEX + a) * N + id];
-    const float lmax = fmaxf(ls[0], fmaxf(ls[1], ls[2])), lmin = fminf(ls[0], fminf(ls[1], ls[2]));
     const float lsplit = logf(fmaxf(th.split_threshold, 1e-12f));
-    const float gmean = obs[id] ? sums[id] / obs[id] : 0.0f;
-    const float amean = obs[id] ? abs_sums[id] / obs[id] : 0.0f;
-    const float athr = th.absolute_gradient_threshold > 0.0f ? th.absolute_gradient_threshold : th.gradient_threshold;
     float dc = 0.0f, rest = 0.0f;
 #pragma unroll
     for (int ch = 0; ch < 3; ++ch) {
@@ -158,24 +153,27 @@ __global__ void features_kernel(const float* __restrict__ params, const float* _
             rest += v * v;
         }
     }
-    const float dx = params[id] - centre.x, dy = params[N + id] - centre.y, dz = params[2 * N + id] - centre.z;
+    const float e = fmaxf(extent, 1e-12f);
+    const float dmean = count > 0.0f ? ls.depth_sum[id] / count : 0.0f;
+    const float dvar = count > 0.0f ? fmaxf(ls.depth_sq[id] / count - dmean * dmean, 0.0f) : 0.0f;
+    const float4 g = ls.last_grad[id];
     float f[16];
-    f[0] = fminf(gmean / th.gradient_threshold, 50.0f);
-    f[1] = fminf(amean / athr, 50.0f);
-    f[2] = log1pf(static_cast<float>(obs[id]));
-    f[3] = 1.0f / (1.0f + expf(-logit));
-    f[4] = fminf(fmaxf(logit, -10.0f), 10.0f);
-    f[5] = fminf(fmaxf(lmax - lsplit, -10.0f), 10.0f);
-    f[6] = fminf(fmaxf(lmin - lsplit, -10.0f), 10.0f);
-    f[7] = fminf(fmaxf((ls[0] + ls[1] + ls[2]) * (1.0f / 3.0f) - lsplit, -10.0f), 10.0f);
-    f[8] = fminf(expf(lmax) / fmaxf(th.max_world_size, 1e-12f), 10.0f);
-    f[9] = sqrtf(dc);
-    f[10] = sqrtf(rest * (1.0f / 45.0f));
-    f[11] = fminf(sqrtf(dx * dx + dy * dy + dz * dz) / fmaxf(extent, 1e-12f), 10.0f);
-    f[12] = fminf(lmax - lmin, 20.0f);
-    f[13] = c.y ? 1.0f : 0.0f;
-    f[14] = c.z ? 1.0f : 0.0f;
-    f[15] = !c.x && !c.y && !c.z ? 1.0f : 0.0f;
+    f[0] = fminf(count > 0.0f ? sums[id] / count / th.gradient_threshold : 0.0f, 50.0f);
+    f[1] = log1pf(count);
+    f[2] = log1pf(fmaxf(ls.max_radius[id], 0.0f));
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+        f[3 + a] = fminf(fmaxf(params[static_cast<int64_t>(GSN_LOG_SCALE_INDEX + a) * N + id] - lsplit, -10.0f), 10.0f);
+    f[6] = 1.0f / (1.0f + expf(-logit));
+    f[7] = sqrtf(dc);
+    f[8] = fminf(rest, 50.0f);
+    f[9] = fminf(dmean / e, 50.0f);
+    f[10] = fminf(dvar / (e * e), 50.0f);
+    f[11] = fminf(static_cast<float>(max(ls.iteration - ls.birth[id], 0)) * 1e-3f, 50.0f);
+    f[12] = log1pf(1e4f * g.x);
+    f[13] = log1pf(1e4f * g.y);
+    f[14] = log1pf(1e4f * g.z);
+    f[15] = log1pf(1e4f * g.w);
 #pragma unroll
     for (int k = 0; k < 16; ++k)
         if (!isfinite(f[k])) f[k] = 0.0f;
@@ -184,6 +182,17 @@ __global__ void features_kernel(const float* __restrict__ params, const float* _
     o[1] = make_float4(f[4], f[5], f[6], f[7]);
     o[2] = make_float4(f[8], f[9], f[10], f[11]);
     o[3] = make_float4(f[12], f[13], f[14], f[15]);
+}
+
+// Birth iteration after a density step: a Gaussian that keeps an old index's
+// history (history_parents >= 0) keeps that Gaussian's birth; clones and split
+// children are born now.
+__global__ void birth_remap_kernel(const int* __restrict__ history_parents, const int* __restrict__ prev_birth,
+                                   int prev_count, int* __restrict__ birth, int count, int now) {
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= count) return;
+    const int p = history_parents ? history_parents[id] : -1;
+    birth[id] = p >= 0 && p < prev_count ? prev_birth[p] : now;
 }
 
 // Cap: accept additions (clone or kept split) in id order while the count stays
@@ -488,16 +497,25 @@ int launch_density_codes(const int4* counts, int n, int8_t* codes, cudaStream_t 
     return launched(1);
 }
 
-int launch_density_features(const float* params, const float* sums, const float* abs_sums, const unsigned int* obs,
-                            int n, const DensityThresholds& th, float3 centre, float extent, bool bf16_sh,
+int launch_density_features(const float* params, const float* sums, const unsigned int* obs, int n,
+                            const DensityThresholds& th, float extent, const LearnedStatsView& ls, bool bf16_sh,
                             float* features, cudaStream_t s) {
     if (n <= 0) return GSN_OK;
+    if (!ls.max_radius || !ls.depth_sum || !ls.depth_sq || !ls.last_grad || !ls.birth || !features)
+        return GSN_ERR_INVALID_ARGUMENT;
     if (bf16_sh)
-        features_kernel<true><<<grid_for(n), kThreads, 0, s>>>(params, sums, abs_sums, obs, n, th, centre, extent,
-                                                               features);
+        features_kernel<true><<<grid_for(n), kThreads, 0, s>>>(params, sums, obs, n, th, extent, ls, features);
     else
-        features_kernel<false><<<grid_for(n), kThreads, 0, s>>>(params, sums, abs_sums, obs, n, th, centre, extent,
-                                                                features);
+        features_kernel<false><<<grid_for(n), kThreads, 0, s>>>(params, sums, obs, n, th, extent, ls, features);
+    return launched(1);
+}
+
+int launch_birth_remap(const int* history_parents, const int* prev_birth, int prev_count, int* birth, int count,
+                       int now, cudaStream_t s) {
+    if (count <= 0) return GSN_OK;
+    if (!birth || (prev_count > 0 && !prev_birth)) return GSN_ERR_INVALID_ARGUMENT;
+    birth_remap_kernel<<<grid_for(count), kThreads, 0, s>>>(history_parents, prev_birth, prev_count, birth, count,
+                                                           now);
     return launched(1);
 }
 

@@ -72,9 +72,23 @@ int launch_density_apply(const DensityApplyArgs& a, cudaStream_t s);
 // Decision codes of the last decide (0 keep, 1 clone, 2 split, 3 prune).
 int launch_density_codes(const int4* counts, int n, int8_t* codes, cudaStream_t s);
 // The 16 statistics of the learned density policy, [n][16] floats (density.cu).
-int launch_density_features(const float* params, const float* sums, const float* abs_sums, const unsigned int* obs,
-                            int n, const DensityThresholds& th, float3 centre, float extent, bool bf16_sh,
+// Per-Gaussian statistics the learned density policy adds to the round
+// statistics (device arrays of the count; iteration = the current one).
+struct LearnedStatsView {
+    const float* max_radius;
+    const float* depth_sum;
+    const float* depth_sq;
+    const float4* last_grad;
+    const int* birth;
+    int iteration;
+};
+// The 16 policy features per Gaussian ([n][16]); see density.cu.
+int launch_density_features(const float* params, const float* sums, const unsigned int* obs, int n,
+                            const DensityThresholds& th, float extent, const LearnedStatsView& ls, bool bf16_sh,
                             float* features, cudaStream_t s);
+// birth[i] = prev_birth[history_parents[i]] where that is >= 0, else now.
+int launch_birth_remap(const int* history_parents, const int* prev_birth, int prev_count, int* birth, int count,
+                       int now, cudaStream_t s);
 int launch_density_reset_opacity(const int* control, float* params, int stride, float max_logit, cudaStream_t s);
 
 }  // namespace gsn

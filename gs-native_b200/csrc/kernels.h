@@ -195,6 +195,16 @@ struct GaussianUpdateArgs {
     bool bf16_sh;             // precision-form layout of params, m and v (10 fp32 + 48 bf16 rows)
     uint32_t seed;            // stochastic-rounding seed of the step (precision form)
     bool sparse;              // visibility-masked Adam: Gaussians with tile_counts == 0 keep p, m, v
+    // optional statistics of the learned density policy (all set or all null),
+    // updated for Gaussians visible in the frame: round maximum of the screen
+    // radius, round sums of depth and depth^2, and the norms of this step's
+    // gradients of mean, log-scale, opacity logit and SH (x, y, z, w)
+    const float* radii;       // renderer's 3-sigma pixel radius of the frame
+    const float* depths;      // renderer's camera-space depth of the frame
+    float* max_radius;
+    float* depth_sum;
+    float* depth_sq;
+    float4* last_grad;
 };
 int launch_gaussian_update(const GaussianUpdateArgs& a, int sh_degree, cudaStream_t stream);
 

@@ -1,6 +1,7 @@
 """Learned density policy: data collection, GPU training and the plain-rule judge.
 
-1. collect(): a plain training run with the density log on. At every
+1. collect() / collect_many(): plain training runs (one per seeded training
+   scene) with the density log on. At every
    density-control step the trainer keeps each Gaussian's 16 statistics, the
    threshold rule's decision (keep / clone / split / prune) and the parent map
    of the step's output. The outcome of a decision is read at the next step:
@@ -63,7 +64,7 @@ def collect(scene, options, iterations, chunk=100, samples_per_step=8192, seed=0
         steps.append(dict(features=feats[pick], codes=codes[pick], pick=pick, parents=parents,
                           all_codes=codes, loss=loss_after, iteration=log["iteration"]))
     tr.close()
-    feats, labels, weights = [], [], []
+    feats, labels, weights, codes = [], [], [], []
     relabelled = 0
     for k in range(len(steps) - 1):
         cur, nxt = steps[k], steps[k + 1]
@@ -82,11 +83,24 @@ def collect(scene, options, iterations, chunk=100, samples_per_step=8192, seed=0
         wt = float(np.clip(1.0 + 10.0 * max(gain, 0.0), 1.0, 3.0))
         feats.append(cur["features"])
         labels.append(lab)
+        codes.append(cur["codes"].astype(np.int32))
         weights.append(np.full(len(lab), wt, np.float32))
     info = dict(steps=len(steps), relabelled=relabelled)
     if not feats:
+        info["codes"] = np.zeros(0, np.int32)
         return np.zeros((0, 16), np.float32), np.zeros(0, np.int32), np.zeros(0, np.float32), info
+    info["codes"] = np.concatenate(codes)  # the threshold rule's decision of every sample
     return np.concatenate(feats), np.concatenate(labels), np.concatenate(weights), info
+
+
+def collect_many(scenes, options, iterations, **kw):
+    """collect() over several seeded training scenes, concatenated."""
+    parts = [collect(sc, options, iterations, seed=k, **kw) for k, sc in enumerate(scenes)]
+    info = dict(scenes=len(parts), steps=sum(p[3]["steps"] for p in parts),
+                relabelled=sum(p[3]["relabelled"] for p in parts),
+                codes=np.concatenate([p[3]["codes"] for p in parts]))
+    return (np.concatenate([p[0] for p in parts]), np.concatenate([p[1] for p in parts]),
+            np.concatenate([p[2] for p in parts]), info)
 
 
 def fit(features, labels, weights, steps=600, lr=3e-3, seed=0):

@@ -221,24 +221,17 @@ bool DensityController::GetDecisionCodes(int8_t* codes, int count) const {
     return gsn::launch_density_codes(density_counts_.get(), count, codes, stream_) == GSN_OK;
 }
 
-bool DensityController::ComputeFeatures(const GaussianBuffers& gaussians, float scene_extent, const float centre[3],
-                                        float gradient_threshold, float percent_dense, float min_opacity,
-                                        float max_screen_size, float absolute_gradient_threshold,
-                                        float* features) const {
+bool DensityController::ComputeFeatures(const GaussianBuffers& gaussians, float scene_extent,
+                                        float gradient_threshold, float percent_dense,
+                                        const gsn::LearnedStatsView& ls, float* features) const {
     const int count = gaussians.gaussian_count_;
     if (count == 0) return true;
     if (!features || !gaussians.gaussians_ || count < 0 || count > capacity_ || !gradient_sums_.get()) return false;
     gsn::DensityThresholds th{};
     th.gradient_threshold = gradient_threshold;
     th.split_threshold = percent_dense * scene_extent;
-    th.min_opacity = min_opacity;
-    th.max_world_size = 0.1f * scene_extent;
-    th.absolute_gradient_threshold = absolute_gradient_threshold;
-    th.prune_large = max_screen_size > 0;
-    return gsn::launch_density_features(gaussians.gaussians_, gradient_sums_.get(), absolute_gradient_sums_.get(),
-                                        observation_counts_.get(), count, th,
-                                        make_float3(centre[0], centre[1], centre[2]), scene_extent, bf16_sh_,
-                                        features, stream_) == GSN_OK;
+    return gsn::launch_density_features(gaussians.gaussians_, gradient_sums_.get(), observation_counts_.get(), count,
+                                        th, scene_extent, ls, bf16_sh_, features, stream_) == GSN_OK;
 }
 
 }  // namespace gs_native

@@ -20,6 +20,7 @@
 #include <cstdint>
 
 #include "core/types/buffers.h"
+#include "density.h"
 #include "util/device_array.h"
 
 namespace gs_native {
@@ -64,10 +65,10 @@ public:
     // ControlDensity into a device int8 array of the pre-control count.
     bool GetDecisionCodes(int8_t* codes, int count) const;
     // The 16 statistics of the learned policy for the current Gaussians
-    // (device [count][16]); same thresholds as ControlDensity.
-    bool ComputeFeatures(const GaussianBuffers& gaussians, float scene_extent, const float centre[3],
-                         float gradient_threshold, float percent_dense, float min_opacity, float max_screen_size,
-                         float absolute_gradient_threshold, float* features) const;
+    // (device [count][16]) from the round statistics and the policy's own
+    // per-Gaussian statistics (ls).
+    bool ComputeFeatures(const GaussianBuffers& gaussians, float scene_extent, float gradient_threshold,
+                         float percent_dense, const gsn::LearnedStatsView& ls, float* features) const;
     const float* GetNewFlags() const { return new_flags_.get(); }
     float* GetGradientSums() { return gradient_sums_.get(); }
     float* GetAbsoluteGradientSums() { return absolute_gradient_sums_.get(); }

@@ -169,7 +169,26 @@ bool GaussianSplatting::SetParameters(const float* host_params, int count) {
     cudaFree(gaussians_.gaussians_);
     gaussians_.gaussians_ = static_cast<float*>(dev);
     gaussians_.gaussian_count_ = count;
-    return true;
+    return ResetLearnedStatistics(count, nullptr, 0);
+}
+
+bool GaussianSplatting::ResetLearnedStatistics(int count, const int* history_parents, int prev_count) {
+    const size_t n = static_cast<size_t>(std::max(count, 1));
+    // ls_birth_ still holds the previous births (read by the remap): only the
+    // destination grows here (Reserve does not keep contents)
+    if (!ls_max_radius_.Reserve(n) || !ls_depth_sum_.Reserve(n) || !ls_depth_sq_.Reserve(n) ||
+        !ls_last_grad_.Reserve(n) || !ls_birth_next_.Reserve(n))
+        return false;
+    if (gsn::launch_birth_remap(history_parents, prev_count > 0 ? ls_birth_.get() : nullptr,
+                                std::min(prev_count, ls_count_), ls_birth_next_.get(), count, completed_,
+                                stream_) != GSN_OK)
+        return false;
+    std::swap(ls_birth_, ls_birth_next_);
+    ls_count_ = count;
+    return cudaMemsetAsync(ls_max_radius_.get(), 0, n * sizeof(float), stream_) == cudaSuccess &&
+           cudaMemsetAsync(ls_depth_sum_.get(), 0, n * sizeof(float), stream_) == cudaSuccess &&
+           cudaMemsetAsync(ls_depth_sq_.get(), 0, n * sizeof(float), stream_) == cudaSuccess &&
+           cudaMemsetAsync(ls_last_grad_.get(), 0, n * sizeof(float4), stream_) == cudaSuccess;
 }
 
 bool GaussianSplatting::GetParameters(std::vector<float>& out) const {
@@ -228,6 +247,7 @@ bool GaussianSplatting::GraphSteps(int iterations) {
         const int64_t capacity = std::min<int64_t>(std::max<int64_t>(renderer_.GetRecordCapacity(), 1 << 20) * 2,
                                                    INT_MAX / 2);
         solver_.SetDensityAccumulators(nullptr, nullptr, nullptr);
+        solver_.SetLearnedStatistics(nullptr, nullptr, nullptr, nullptr);
         if (!graph_.Capture(renderer_, solver_, gaussians_, cameras_, targets_.get(), target_stride_,
                             options_.background, image_.get(), sh_degree_, capacity, stream_))
             return false;
@@ -264,6 +284,11 @@ bool GaussianSplatting::Step() {
                                        density_.GetObservationCounts());
     else
         solver_.SetDensityAccumulators(nullptr, nullptr, nullptr);
+    if (accumulate && (options_.learned_density || options_.log_density))
+        solver_.SetLearnedStatistics(ls_max_radius_.get(), ls_depth_sum_.get(), ls_depth_sq_.get(),
+                                     ls_last_grad_.get());
+    else
+        solver_.SetLearnedStatistics(nullptr, nullptr, nullptr, nullptr);
     if (!solver_.Iterate(camera, renderer_, image_.get(), target, gaussians_, lr, sh_degree_)) return false;
     completed_ = next;
     ++camera_cursor_;
@@ -287,10 +312,11 @@ bool GaussianSplatting::ControlDensity() {
     const int before = gaussians_.gaussian_count_;
     const bool learned = options_.learned_density && mlp_ready_;
     if (learned || options_.log_density) {
+        const gsn::LearnedStatsView ls{ls_max_radius_.get(), ls_depth_sum_.get(), ls_depth_sq_.get(),
+                                       ls_last_grad_.get(), ls_birth_.get(), completed_};
         if (!density_features_.Reserve(static_cast<size_t>(std::max(before, 1)) * 16) ||
-            !density_.ComputeFeatures(gaussians_, scene_extent_, scene_centre_, options_.gradient_threshold,
-                                      options_.percent_dense, options_.min_opacity, max_screen,
-                                      options_.absolute_gradient_threshold, density_features_.get()))
+            !density_.ComputeFeatures(gaussians_, scene_extent_, options_.gradient_threshold,
+                                      options_.percent_dense, ls, density_features_.get()))
             return false;
     }
     if (learned) {
@@ -333,7 +359,7 @@ bool GaussianSplatting::ControlDensity() {
         }
         history = spatial_.GetParents();
     }
-    return solver_.RemapGaussians(history, after);
+    return ResetLearnedStatistics(after, history, before) && solver_.RemapGaussians(history, after);
 }
 
 bool GaussianSplatting::SetDensityMlp(const float* weights) {
@@ -418,7 +444,7 @@ bool GaussianSplatting::Load(const std::string& path) {
 namespace {
 
 constexpr char kCheckpointMagic[8] = {'G', 'S', 'N', 'C', 'K', 'P', 'T', '1'};
-constexpr uint32_t kCheckpointVersion = 1;
+constexpr uint32_t kCheckpointVersion = 2;
 
 struct CheckpointHeader {
     char magic[8];
@@ -466,13 +492,19 @@ bool GaussianSplatting::SaveCheckpoint(const std::string& path) {
     h.camera_count = static_cast<int32_t>(camera_order_.size());
     h.scene_extent = scene_extent_;
     for (int a = 0; a < 3; ++a) h.scene_centre[a] = scene_centre_[a];
-    std::vector<float> block, m, v, sums, abs_sums;
+    std::vector<float> block, m, v, sums, abs_sums, max_radius, depth_sum, depth_sq, last_grad;
     std::vector<unsigned int> obs;
+    std::vector<int> birth;
     if (!Download(block, gaussians_.gaussians_, rows * n) || !Download(m, solver_.GetFirstMoments(), rows * n) ||
         !Download(v, solver_.GetSecondMoments(), rows * n) ||
         !Download(sums, static_cast<const float*>(density_.GetGradientSums()), n) ||
         !Download(abs_sums, static_cast<const float*>(density_.GetAbsoluteGradientSums()), n) ||
-        !Download(obs, static_cast<const unsigned int*>(density_.GetObservationCounts()), n))
+        !Download(obs, static_cast<const unsigned int*>(density_.GetObservationCounts()), n) ||
+        !Download(max_radius, static_cast<const float*>(ls_max_radius_.get()), n) ||
+        !Download(depth_sum, static_cast<const float*>(ls_depth_sum_.get()), n) ||
+        !Download(depth_sq, static_cast<const float*>(ls_depth_sq_.get()), n) ||
+        !Download(last_grad, reinterpret_cast<const float*>(ls_last_grad_.get()), 4 * n) ||
+        !Download(birth, static_cast<const int*>(ls_birth_.get()), n))
         return false;
     std::ofstream out(path, std::ios::binary);
     if (!out) return false;
@@ -481,6 +513,10 @@ bool GaussianSplatting::SaveCheckpoint(const std::string& path) {
     for (const std::vector<float>* a : {&block, &m, &v, &sums, &abs_sums})
         out.write(reinterpret_cast<const char*>(a->data()), a->size() * sizeof(float));
     out.write(reinterpret_cast<const char*>(obs.data()), obs.size() * sizeof(unsigned int));
+    // learned-policy statistics (version 2)
+    for (const std::vector<float>* a : {&max_radius, &depth_sum, &depth_sq, &last_grad})
+        out.write(reinterpret_cast<const char*>(a->data()), a->size() * sizeof(float));
+    out.write(reinterpret_cast<const char*>(birth.data()), birth.size() * sizeof(int));
     return static_cast<bool>(out);
 }
 
@@ -497,11 +533,16 @@ bool GaussianSplatting::LoadCheckpoint(const std::string& path) {
     const size_t rows = PhysicalRows(), n = static_cast<size_t>(h.count);
     std::vector<int> order(static_cast<size_t>(h.camera_count));
     std::vector<float> block(rows * n), m(rows * n), v(rows * n), sums(n), abs_sums(n);
+    std::vector<float> max_radius(n), depth_sum(n), depth_sq(n), last_grad(4 * n);
     std::vector<unsigned int> obs(n);
+    std::vector<int> birth(n);
     in.read(reinterpret_cast<char*>(order.data()), order.size() * sizeof(int));
     for (std::vector<float>* a : {&block, &m, &v, &sums, &abs_sums})
         in.read(reinterpret_cast<char*>(a->data()), a->size() * sizeof(float));
     in.read(reinterpret_cast<char*>(obs.data()), obs.size() * sizeof(unsigned int));
+    for (std::vector<float>* a : {&max_radius, &depth_sum, &depth_sq, &last_grad})
+        in.read(reinterpret_cast<char*>(a->data()), a->size() * sizeof(float));
+    in.read(reinterpret_cast<char*>(birth.data()), birth.size() * sizeof(int));
     if (!in) return false;
     for (int k : order)
         if (k < 0 || k >= h.camera_count) return false;
@@ -518,7 +559,11 @@ bool GaussianSplatting::LoadCheckpoint(const std::string& path) {
     gaussians_.gaussian_count_ = h.count;
     if (!Upload(solver_.GetFirstMoments(), m) || !Upload(solver_.GetSecondMoments(), v) ||
         !Upload(density_.GetGradientSums(), sums) || !Upload(density_.GetAbsoluteGradientSums(), abs_sums) ||
-        !Upload(density_.GetObservationCounts(), obs))
+        !Upload(density_.GetObservationCounts(), obs) || !ResetLearnedStatistics(h.count, nullptr, 0) ||
+        cudaStreamSynchronize(stream_) != cudaSuccess ||
+        !Upload(ls_max_radius_.get(), max_radius) || !Upload(ls_depth_sum_.get(), depth_sum) ||
+        !Upload(ls_depth_sq_.get(), depth_sq) || !Upload(reinterpret_cast<float*>(ls_last_grad_.get()), last_grad) ||
+        !Upload(ls_birth_.get(), birth))
         return false;
     solver_.SetIteration(h.adam_step);
     completed_ = h.completed;

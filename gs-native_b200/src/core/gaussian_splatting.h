@@ -175,6 +175,14 @@ private:
     float scene_centre_[3] = {0.0f, 0.0f, 0.0f};
     DensityMlp mlp_;
     bool mlp_ready_ = false;
+    // statistics of the learned policy beyond the round statistics (see
+    // LearnedStatsView): round max radius, depth sums, last-step gradient
+    // norms, and each Gaussian's birth iteration
+    bool ResetLearnedStatistics(int count, const int* history_parents, int prev_count);
+    DeviceArray<float> ls_max_radius_, ls_depth_sum_, ls_depth_sq_;
+    DeviceArray<float4> ls_last_grad_;
+    DeviceArray<int> ls_birth_, ls_birth_next_;
+    int ls_count_ = 0;
     DeviceArray<float> density_features_;
     DeviceArray<int8_t> density_actions_;
     DeviceArray<int8_t> density_codes_;

@@ -161,6 +161,15 @@ bool Solver::UpdateGaussians(const CameraParams& camera, const Renderer& rendere
         a.grad_sums = acc_grad_;
         a.abs_sums = acc_abs_;
         a.obs_counts = acc_count_;
+        if (ls_max_radius_ && ls_depth_sum_ && ls_depth_sq_ && ls_last_grad_ && renderer.GetRadii() &&
+            renderer.GetDepths()) {
+            a.radii = renderer.GetRadii();
+            a.depths = renderer.GetDepths();
+            a.max_radius = ls_max_radius_;
+            a.depth_sum = ls_depth_sum_;
+            a.depth_sq = ls_depth_sq_;
+            a.last_grad = ls_last_grad_;
+        }
     }
     a.grads_out = grads_out;
     a.frame = frame_;

@@ -67,6 +67,16 @@ public:
     // Optional fused accumulation of the density statistics (pointers owned by
     // the caller, all three or none); equivalent to calling
     // DensityController::AccumulateStatistics after Iterate().
+    // Statistics of the learned density policy, updated with the density
+    // accumulators for visible Gaussians (null: off): round maximum of the
+    // screen radius, round sums of depth and depth^2, and the step's gradient
+    // norms of mean, log-scale, opacity and SH (float4 per Gaussian).
+    void SetLearnedStatistics(float* max_radius, float* depth_sum, float* depth_sq, float4* last_grad) {
+        ls_max_radius_ = max_radius;
+        ls_depth_sum_ = depth_sum;
+        ls_depth_sq_ = depth_sq;
+        ls_last_grad_ = last_grad;
+    }
     void SetDensityAccumulators(float* gradient_sums, float* absolute_sums, unsigned int* counts) {
         acc_grad_ = gradient_sums;
         acc_abs_ = absolute_sums;
@@ -125,6 +135,10 @@ private:
     size_t per_gaussian_capacity_ = 0;
     uint64_t iteration_ = 0;
     float* acc_grad_ = nullptr;
+    float* ls_max_radius_ = nullptr;
+    float* ls_depth_sum_ = nullptr;
+    float* ls_depth_sq_ = nullptr;
+    float4* ls_last_grad_ = nullptr;
     float* acc_abs_ = nullptr;
     unsigned int* acc_count_ = nullptr;
     const gsn::StepFrame* frame_ = nullptr;
