@@ -32,12 +32,16 @@ constexpr int kSeg1 = 7;               // outputs per thread in the moment passe
 constexpr int kSeg2 = 4;               // outputs per thread in the back-filter passes (32 = 8 x 4)
 constexpr float kC1 = 0.0001f;
 constexpr float kC2 = 0.0009f;
-// shared arena (floats): raw image + target, five moment planes, three partial
-// planes; the back-filtered partials reuse the moment planes.
+// shared arena (floats): raw image + target and five moment planes. The three
+// partial planes reuse the raw planes once the horizontal pass has consumed them
+// (each thread first copies its own output pixels' I and T to registers), and
+// the back-filtered partials reuse the moment planes: 65 KB, three CTAs per SM.
 constexpr int kRaw = kIn * kIn;
 constexpr int kMom = kIn * kCen;
 constexpr int kPart = kCen * kCen;
-constexpr size_t kSmemBytes = sizeof(float) * (2 * kRaw + 5 * kMom + 3 * kPart);
+constexpr size_t kSmemBytes = sizeof(float) * (2 * kRaw + 5 * kMom);
+static_assert(3 * kPart <= 2 * kRaw, "partials alias the raw planes");
+static_assert((kT / kSeg2) * kT == kThreads, "one output column segment per thread");
 
 __device__ __forceinline__ double block_sum(double v, double* red) {
     for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -54,7 +58,7 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
 // One block per 32x32 output tile and colour channel. Every filter output is
 // produced by one thread from a register window of its row (or column), with
 // the 11 taps accumulated in ascending order as in solver.cu:65-161.
-__global__ void __launch_bounds__(kThreads, 2) loss_gradient_kernel(const float* __restrict__ image,
+__global__ void __launch_bounds__(kThreads, 3) loss_gradient_kernel(const float* __restrict__ image,
                                                                    const uint8_t* __restrict__ target_arg,
                                                                    const StepFrame* __restrict__ frame,
                                                                    float* __restrict__ grad, int width, int height,
@@ -65,7 +69,7 @@ __global__ void __launch_bounds__(kThreads, 2) loss_gradient_kernel(const float*
     float* raw_i = smem;                 // [kIn][kIn]
     float* raw_t = raw_i + kRaw;         // [kIn][kIn]
     float* mom = raw_t + kRaw;           // [5][kIn][kCen]
-    float* part = mom + 5 * kMom;        // [3][kCen][kCen]
+    float* part = smem;                  // [3][kCen][kCen] (after the raw planes are consumed)
     float* back = mom;                   // [3][kCen][kT] (after the moments are consumed)
     const int t = threadIdx.x;
     const int ch = blockIdx.z;
@@ -111,6 +115,16 @@ __global__ void __launch_bounds__(kThreads, 2) loss_gradient_kernel(const float*
             mom[3 * kMom + idx] = h3;
             mom[4 * kMom + idx] = h4;
         }
+    }
+    __syncthreads();
+    // this thread's output pixels (column x_out, rows y_out .. y_out + 3) of the
+    // raw planes, kept in registers before the partials overwrite them
+    const int x_out = t % kT, y_out = (t / kT) * kSeg2;
+    float keep_i[kSeg2], keep_t[kSeg2];
+#pragma unroll
+    for (int o = 0; o < kSeg2; ++o) {
+        keep_i[o] = raw_i[(y_out + o + 10) * kIn + x_out + 10];
+        keep_t[o] = raw_t[(y_out + o + 10) * kIn + x_out + 10];
     }
     __syncthreads();
 
@@ -183,9 +197,9 @@ __global__ void __launch_bounds__(kThreads, 2) loss_gradient_kernel(const float*
     // vertical back-filter at the output pixels and the combined gradient
     double l1_sum = 0.0, sq_sum = 0.0;
     const float norm = 1.0f / (3.0f * static_cast<float>(width) * height);
-    for (int item = t; item < (kT / kSeg2) * kT; item += kThreads) {
-        const int x = item % kT;
-        const int y0 = (item / kT) * kSeg2;
+    {
+        const int x = x_out;
+        const int y0 = y_out;
         float f[3][kSeg2];
 #pragma unroll
         for (int p = 0; p < 3; ++p) {
@@ -204,8 +218,8 @@ __global__ void __launch_bounds__(kThreads, 2) loss_gradient_kernel(const float*
         for (int o = 0; o < kSeg2; ++o) {
             const int px = ox + x, py = oy + y0 + o;
             if (px < width && py < height) {
-                const float I = raw_i[(y0 + o + 10) * kIn + x + 10];
-                const float R = raw_t[(y0 + o + 10) * kIn + x + 10];
+                const float I = keep_i[o];
+                const float R = keep_t[o];
                 float r = I - R;
                 float l1 = static_cast<float>(r > 0) - static_cast<float>(r < 0);
                 float dssim = -(f[0][o] + R * f[1][o] + 2 * I * f[2][o]);
