@@ -30,8 +30,10 @@ form. The held-out PSNR of each form's full training run is measured by
 synthetic_run.py (the metric's 0.1 dB condition).
 
 Printed JSON line: `value` is iterations/s with targets resident in HBM,
-`e2e` the same through host buffers (pinned H2D target upload and a D2H loss
-read every step), plus per-stage device times, the roofline of the dominant
+`e2e` the same through host buffers (every step uploads its target from pinned
+host memory - the next step's upload overlapping the current step on a copy
+stream - and copies its loss back to pinned memory, which the host reads two
+steps later), plus per-stage device times, the roofline of the dominant
 kernel, SM clocks sampled during the timed region and the FP64 CPU oracle
 timed on the host cores (`cpu_baseline`). `--impl reference` times only the CPU
 implementation of the path (the oracle restatement of the reference's code).
@@ -337,7 +339,18 @@ def run_gsn(args):
         targets[k] = (img * 255.0).round().clamp(0, 255).to(torch.uint8)
     del tm, maker
     host_targets = targets.cpu().pin_memory()
-    staging = torch.empty((1064, 1600, 3), dtype=torch.uint8, device="cuda")
+    # end-to-end runs upload every step's target from pinned host memory; the
+    # upload of step k + 1 runs on a copy stream into the other staging buffer
+    # while step k computes (as a training loop prefetches its next input)
+    # and each step's loss is copied back into a pinned ring the host reads two
+    # steps later (it waits for step k - 2 before issuing step k + 1's upload)
+    ring = 3
+    staging = [torch.empty((1064, 1600, 3), dtype=torch.uint8, device="cuda") for _ in range(ring)]
+    copy_stream = torch.cuda.Stream()
+    ready = [torch.cuda.Event() for _ in range(ring)]
+    done = [torch.cuda.Event() for _ in range(ring)]
+    loss_ring = torch.zeros((ring, 4), dtype=torch.float64).pin_memory()
+    e2e_seen = []
     lr = position_lr(15000, extent)
     loss_host = torch.zeros(4, dtype=torch.float64).pin_memory()
 
@@ -366,19 +379,54 @@ def run_gsn(args):
             else:
                 self.params = torch.from_numpy(np.ascontiguousarray(block)).cuda()
 
-    def step(f, k, e2e=False):
+    upload_view = [0]  # view offset of the run being uploaded
+
+    def upload(dst, k, buf):
+        """Pinned-host upload of step k's target into dst on the copy stream."""
+        with torch.cuda.stream(copy_stream):
+            dst.copy_(host_targets[(upload_view[0] + k) % len(train)], non_blocking=True)
+            ready[buf].record(copy_stream)
+
+    def step(f, k, tgt=None):
         cam = train[k % len(train)]
-        if e2e:
-            staging.copy_(host_targets[k % len(train)], non_blocking=True)
-            tgt = staging
-        else:
+        if tgt is None:
             tgt = targets[k % len(train)]
         assert f.renderer.render(f.params.data_ptr(), n, cam, [0, 0, 0], img.data_ptr(), SH_DEGREE) == 0
         assert f.solver.iterate(cam, f.renderer, img.data_ptr(), tgt.data_ptr(), f.params.data_ptr(), n, lr,
                                 SH_DEGREE) == 0
-        if e2e:
-            gsn.memcpy_async(loss_host.data_ptr(), f.solver.loss_device(), 32, sp)
-            stream.synchronize()
+
+    def read_loss(f, b):
+        """Async D2H copy of the step's loss into ring slot b, marked by done[b]."""
+        gsn.memcpy_async(loss_ring[b].data_ptr(), f.solver.loss_device(), 32, sp)
+        done[b].record(stream)
+
+    def pipelined(steps, dst, issue):
+        """Every step uploads its target (dst(k): device buffer of step k) and
+        reads its loss back; the host waits for step k - 2 (its loss) before
+        reusing that step's slot for step k + 1's upload."""
+        upload(dst(0), 0, 0)
+        for k in range(steps):
+            b = k % ring
+            if k + 1 < steps:
+                nb = (k + 1) % ring
+                if k + 1 >= ring:
+                    done[nb].synchronize()
+                    e2e_seen.append(float(loss_ring[nb, 3]))
+                upload(dst(k + 1), k + 1, nb)
+            stream.wait_event(ready[b])
+            issue(k, b)
+        stream.synchronize()
+        e2e_seen.extend(float(loss_ring[(k % ring), 3]) for k in range(max(0, steps - ring), steps))
+        loss_host.copy_(loss_ring[(steps - 1) % ring])
+
+    def e2e_steps(f, k0):
+        """Steps through host buffers (see pipelined)."""
+        def run(steps):
+            def issue(k, b):
+                step(f, k0 + k, staging[b])
+                read_loss(f, b)
+            pipelined(steps, lambda k: staging[k % ring], issue)
+        return run
 
     def barrier():
         if dist is not None:
@@ -404,8 +452,8 @@ def run_gsn(args):
         barrier()
         return max_over_ranks(e0.elapsed_time(e1)), launches
 
-    def eager_steps(f, k0, e2e=False):
-        return lambda steps: [step(f, k0 + k, e2e) for k in range(steps)]
+    def eager_steps(f, k0):
+        return lambda steps: [step(f, k0 + k) for k in range(steps)]
 
     def profile_stages(f):
         gsn.profile_enable(True)
@@ -423,9 +471,10 @@ def run_gsn(args):
         ms, launches = timed(eager_steps(f, args.warmup), args.steps)
         stages = profile_stages(f) if with_stages else None
         f.solver.set_compute_loss(True)
-        for k in range(2):
-            step(f, k, True)
-        ms_e2e, _ = timed(eager_steps(f, args.warmup, True), args.steps)
+        upload_view[0] = 0
+        e2e_steps(f, 0)(2)
+        upload_view[0] = args.warmup
+        ms_e2e, _ = timed(e2e_steps(f, args.warmup), args.steps)
         records = int(f.renderer.buffers().record_count_host)
         # visible Gaussians of the last frame, read while the renderer is alive
         counts = torch.empty(n, dtype=torch.int32, device="cuda")
@@ -443,13 +492,13 @@ def run_gsn(args):
         status = graph.check()
 
         def graph_e2e(steps):
-            # pinned target upload, one replay and the loss read per step
-            for k in range(steps):
-                v = schedule[k]
-                targets[v].copy_(host_targets[v], non_blocking=True)
-                graph.run([v], [lr])
-                gsn.memcpy_async(loss_host.data_ptr(), f.solver.loss_device(), 32, sp)
-                stream.synchronize()
+            # one replay per step; the uploads go straight into the view's resident
+            # slot (the steps in flight use other views: the schedule cycles 180)
+            def issue(k, b):
+                graph.run([schedule[k]], [lr])
+                read_loss(f, b)
+            upload_view[0] = args.warmup  # schedule[k] = (warmup + k) % views
+            pipelined(steps, lambda k: targets[schedule[k]], issue)
 
         ms_graph_e2e, _ = timed(graph_e2e, args.steps)
         status = status or graph.check()
@@ -576,7 +625,10 @@ def run_gsn(args):
         "forms": forms,
         "chosen_over_plain": round(forms[chosen]["value"] / value, 4),
         "e2e": {"value": forms[chosen]["e2e"], "unit": UNIT, "h2d_bytes_per_step": 1600 * 1064 * 3,
-                "d2h_bytes_per_step": 32, "psnr_db_last_step": forms[chosen]["psnr_db_last_step"]},
+                "d2h_bytes_per_step": 32, "psnr_db_last_step": forms[chosen]["psnr_db_last_step"],
+                "pipelining": ("next step's target upload on a copy stream; each step's loss read back "
+                               "asynchronously, the host waits for step k - 2 before issuing step k + 1"),
+                "results_read": len(e2e_seen), "results_finite": bool(np.all(np.isfinite(e2e_seen)))},
         "roofline": roofline,
         "roofline_plain": roofline_of("plain_fp32"),
         "psnr_note": ("psnr_db_last_step is the training view's PSNR after this run's ~1,000 steps from the random "
