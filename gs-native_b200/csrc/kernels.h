@@ -134,6 +134,11 @@ struct RasterForwardArgs {
     float* image;                  // HWC RGB fp32
     float* final_transmittance;    // [P] optional
     int* contributors;             // [P] optional: records consumed before the pixel finished
+    // optional: two bit planes of record_words words (plane w at record_warps +
+    // w * record_words, cleared by the caller); bit r of plane w is set when a
+    // pixel of warp w's strip took record r
+    uint32_t* record_warps;
+    int64_t record_words;
 };
 int launch_raster_forward(const RasterForwardArgs& a, cudaStream_t stream);
 
@@ -169,6 +174,8 @@ struct RasterBackwardArgs {
     const float* image;        // final colours of the forward pass
     const float* image_grad;   // dL/dimage
     const int* contributors;   // per-pixel record bound from the forward pass (optional)
+    const uint32_t* record_warps;  // the forward pass's bit planes (optional)
+    int64_t record_words;
     gsn_camera cam;
     float* grad_out;           // [N][12] screen-space accumulators, zeroed by the caller
 };

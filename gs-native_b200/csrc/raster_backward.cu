@@ -14,9 +14,11 @@
 //   * warp sums are accumulated per batch in shared memory (shared-memory
 //     float atomics) and flushed with one global atomic per (Gaussian, value)
 //     and tile, instead of one per warp;
-//   * each warp walks only the records whose conservative alpha >= 1/255 box
-//     reaches its 16x8 pixel strip, powers below a record's alpha floor skip
-//     expf, and the three divisions by (1 - alpha) share one reciprocal;
+//   * each warp walks only the records that some pixel of its 16x8 strip took
+//     in the forward pass (per-record strip flags the forward writes) and whose
+//     conservative alpha >= 1/255 box reaches the strip, powers below a
+//     record's alpha floor skip expf, and the three divisions by (1 - alpha)
+//     share one reciprocal;
 //   * the colour term of dL/dalpha is carried per pixel as two scalars (the
 //     gradient-weighted final colour and the gradient-weighted colour in front
 //     of the record) instead of three channel sums;
@@ -42,11 +44,13 @@ __global__ void __launch_bounds__(kRasterThreads, 12) raster_backward_kernel(Ras
     __shared__ float3 s_color[kRasterBatch];
     __shared__ float4 s_box[kRasterBatch];
     __shared__ float s_floor[kRasterBatch];
+    __shared__ uint16_t s_warps[kRasterBatch];
     __shared__ float s_acc[kRasterBatch * kVals];
     __shared__ int s_bound;
 
     const int t = threadIdx.x;
     const int lane = t & 31;
+    const int warp_shift = 8 * (t >> 5);
     const TileGeometry g = tile_geometry(a.cam);
     const float fx = static_cast<float>(g.px);
     const int64_t begin = a.tile_offsets[g.tile];
@@ -105,6 +109,14 @@ __global__ void __launch_bounds__(kRasterThreads, 12) raster_backward_kernel(Ras
                 s_color[slot] = make_float3(__ldg(c), __ldg(c + 1), __ldg(c + 2));
                 s_box[slot] = alpha_box(mean, q);
                 s_floor[slot] = alpha_floor(q.w);
+                uint16_t flags = 0x0101;
+                if (a.record_warps) {
+                    const int64_t r = base + slot;
+                    const uint32_t bit = 1u << (r & 31);
+                    flags = static_cast<uint16_t>(((a.record_warps[r >> 5] & bit) ? 0x0001 : 0) |
+                                                  ((a.record_warps[a.record_words + (r >> 5)] & bit) ? 0x0100 : 0));
+                }
+                s_warps[slot] = flags;
             }
         }
         for (int k = t; k < kRasterBatch * kVals; k += kRasterThreads) s_acc[k] = 0.0f;
@@ -113,7 +125,10 @@ __global__ void __launch_bounds__(kRasterThreads, 12) raster_backward_kernel(Ras
 #pragma unroll 1
         for (int k = 0; k < kRasterBatch / 32; ++k) {
             const int jl = k * 32 + lane;
-            uint32_t m = __ballot_sync(0xffffffffu, jl < batch && box_hits(s_box[jl], g.sx0, g.sx1, g.sy0, g.sy1));
+            // records the forward pass took somewhere in this warp's strip (every
+            // other record leaves the strip's pixels unchanged)
+            uint32_t m = __ballot_sync(0xffffffffu, jl < batch && ((s_warps[jl] >> warp_shift) & 1u) &&
+                                                        box_hits(s_box[jl], g.sx0, g.sx1, g.sy0, g.sy1));
             while (m) {
                 if (__all_sync(0xffffffffu, done[0] && done[1] && done[2] && done[3])) break;
                 const int j = k * 32 + __ffs(m) - 1;

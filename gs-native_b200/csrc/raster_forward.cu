@@ -58,6 +58,7 @@ __global__ void __launch_bounds__(kRasterThreads) raster_forward_kernel(RasterFo
 
     const int t = threadIdx.x;
     const int lane = t & 31;
+    const int warp = t >> 5;
     const TileGeometry g = tile_geometry(a.cam);
     const float fx = static_cast<float>(g.px);
     float fy[kPixPerThread];
@@ -96,10 +97,12 @@ __global__ void __launch_bounds__(kRasterThreads) raster_forward_kernel(RasterFo
         n0 = fetch(a, base + kRasterBatch + t, end);
         n1 = fetch(a, base + kRasterBatch + kRasterThreads + t, end);
         const int batch = static_cast<int>(min(static_cast<int64_t>(kRasterBatch), end - base));
+        uint32_t* plane = a.record_warps ? a.record_warps + warp * a.record_words : nullptr;
 #pragma unroll 1
         for (int k = 0; k < kRasterBatch / 32; ++k) {
             const int jl = k * 32 + lane;
             uint32_t m = __ballot_sync(0xffffffffu, jl < batch && box_hits(s_box[jl], g.sx0, g.sx1, g.sy0, g.sy1));
+            uint32_t took = 0;  // records of this chunk a pixel of this lane took
             while (m && !(done[0] && done[1] && done[2] && done[3])) {
                 const int j = k * 32 + __ffs(m) - 1;
                 m &= m - 1;
@@ -136,6 +139,19 @@ __global__ void __launch_bounds__(kRasterThreads) raster_forward_kernel(RasterFo
                     C[p].z = take ? C[p].z + c.z * w : C[p].z;
                     T[p] = take ? nextT : T[p];
                     consumed[p] = take ? static_cast<int>(base - begin) + j + 1 : consumed[p];
+                    took |= take ? 1u << (j & 31) : 0u;
+                }
+            }
+            if (plane) {
+                // this warp strip's took-flags of the chunk's 32 records, one bit
+                // each, into the plane at the records' global positions
+#pragma unroll
+                for (int o = 16; o; o >>= 1) took |= __shfl_xor_sync(0xffffffffu, took, o);
+                if (lane == 0 && took) {
+                    const int64_t r0 = base + k * 32;
+                    const int off = static_cast<int>(r0 & 31);
+                    atomicOr(plane + (r0 >> 5), took << off);
+                    if (off) atomicOr(plane + (r0 >> 5) + 1, took >> (32 - off));
                 }
             }
         }

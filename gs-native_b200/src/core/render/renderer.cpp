@@ -59,8 +59,9 @@ bool Renderer::ReserveRecords(int64_t records) {
     grow = std::min<size_t>(grow, INT_MAX);
     if (grow < r) return false;
     bool ok = tile_keys_[0].Reserve(grow) && tile_keys_[1].Reserve(grow) && record_ids_[0].Reserve(grow) &&
-              record_ids_[1].Reserve(grow);
+              record_ids_[1].Reserve(grow) && record_warps_.Reserve(2 * (grow / 32 + 1));
     if (!ok) return false;
+    record_words_ = static_cast<int64_t>(grow / 32 + 1);
     record_capacity_ = static_cast<int64_t>(grow);
     return true;
 }
@@ -191,6 +192,12 @@ bool Renderer::Render(const GaussianBuffers& gaussians, const CameraParams& came
     ra.image = image;
     ra.final_transmittance = nullptr;
     ra.contributors = contributors_.get();
+    ra.record_warps = record_warps_.get();
+    ra.record_words = record_words_;
+    if (record_warps_.get() &&
+        cudaMemsetAsync(record_warps_.get(), 0, 2 * static_cast<size_t>(record_words_) * sizeof(uint32_t), s) !=
+            cudaSuccess)
+        return false;
     gsn::stage_mark(s, gsn::kStageRasterForward);
     const bool ok = gsn::launch_raster_forward(ra, s) == GSN_OK;
     gsn::stage_mark(s, gsn::kStageOther);

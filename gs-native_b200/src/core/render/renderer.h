@@ -72,6 +72,12 @@ public:
     const float* GetDepths() const { return depths_.get(); }
     const float* GetRadii() const { return radii_.get(); }
     const int* GetContributors() const { return contributors_.get(); }
+    // Two bit planes over the records of the last frame (plane w at
+    // GetRecordWarps() + w * GetRecordWords()): bit r of plane w is set when a
+    // pixel of warp strip w (rows 8w..8w+7 of its tile) took record r in the
+    // forward pass. The backward pass skips the others.
+    const uint32_t* GetRecordWarps() const { return record_warps_.get(); }
+    int64_t GetRecordWords() const { return record_words_; }
     const int* GetRecordCountDevice() const { return counters_.get(); }
     const int* GetOverflowFlag() const { return counters_.get() + 1; }
     int64_t GetRecordCapacity() const { return record_capacity_; }
@@ -112,6 +118,8 @@ private:
     DeviceArray<uint32_t> record_ids_[2];
     uint32_t* sorted_ids_ = nullptr;
     DeviceArray<int> contributors_;
+    DeviceArray<uint32_t> record_warps_;
+    int64_t record_words_ = 0;
     size_t pixel_capacity_ = 0;
     DeviceArray<unsigned char> sort_scratch_;
     size_t sort_scratch_count_ = 0;

@@ -126,6 +126,8 @@ bool Solver::ComputeScreenGradients(const CameraParams& camera, const Renderer& 
     a.image = image;
     a.image_grad = image_gradients_.get();
     a.contributors = renderer.GetContributors();
+    a.record_warps = renderer.GetRecordWarps();
+    a.record_words = renderer.GetRecordWords();
     a.cam = AsGsnCamera(camera);
     a.grad_out = screen_.get();
     return gsn::launch_raster_backward(a, stream_) == GSN_OK;
