@@ -87,6 +87,15 @@ int launch_radix_sort(uint32_t* keys, uint32_t* values, uint32_t* keys_alt, uint
                       int end_bit, const RadixSortScratch& scratch, bool* result_in_alt,
                       cudaStream_t stream);
 
+// The same sort leaving out every key equal to 0xFFFFFFFF (the culled-Gaussian
+// depth key, which sorts last): the first pass drops them and writes the
+// number of kept pairs to *kept_device (device int); later passes and the
+// sorted output cover only those.
+int launch_radix_sort_dropping(uint32_t* keys, uint32_t* values, uint32_t* keys_alt, uint32_t* values_alt,
+                               bool identity_values, int max_count, const int* count_device, int begin_bit,
+                               int end_bit, const RadixSortScratch& scratch, bool* result_in_alt, int* kept_device,
+                               cudaStream_t stream);
+
 // Same sort with its scratch in a static device array of the library (no
 // allocation); count <= noalloc_sort_max_count(), else GSN_ERR_CAPACITY.
 int noalloc_sort_max_count();
@@ -97,8 +106,9 @@ int launch_radix_sort_noalloc(uint32_t* keys, uint32_t* values, uint32_t* keys_a
 // outputs with out[n] = total. `gather` (optional) reads in[gather[i]] instead of
 // in[i]. Scratch: scan_scratch_bytes(n).
 size_t scan_scratch_bytes(int n);
+// valid_device (optional): entries from index *valid_device on count as zero.
 int launch_exclusive_scan(const int* in, const uint32_t* gather, int* out, int n, void* scratch,
-                          cudaStream_t stream);
+                          cudaStream_t stream, const int* valid_device = nullptr);
 
 // Emit one (tile, gaussian id) record per tile of every visible Gaussian, in
 // depth order. record_start[p] is the exclusive scan of tile counts in sorted

@@ -27,6 +27,7 @@ constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kSortItems = 8;                       // per thread
 constexpr int kSortChunk = kSortThreads * kSortItems;  // 2048 keys per block
 constexpr int kBins = 256;
+constexpr uint32_t kSortSentinel = 0xFFFFFFFFu;  // the key a dropping sort leaves out
 
 // Device-resident counts are clamped to the host-side capacity the grid was sized
 // for, so an overflowing count can never drive an access past the buffers.
@@ -39,6 +40,7 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
 }
 
 // Per-block digit histogram of one 8-bit digit.
+template <bool kDrop>
 __global__ void __launch_bounds__(kSortThreads) radix_upsweep(const uint32_t* __restrict__ keys,
                                                               const int* n_dev, int n_host, int bit, uint32_t mask,
                                                               uint32_t* __restrict__ block_hist,
@@ -55,7 +57,10 @@ __global__ void __launch_bounds__(kSortThreads) radix_upsweep(const uint32_t* __
 #pragma unroll 4
     for (int k = 0; k < kSortItems; ++k) {
         int64_t idx = start + k * kSortThreads + threadIdx.x;
-        if (idx < end) atomicAdd(&hist[warp][(__ldg(keys + idx) >> bit) & mask], 1u);
+        if (idx < end) {
+            const uint32_t k = __ldg(keys + idx);
+            if (!kDrop || k != kSortSentinel) atomicAdd(&hist[warp][(k >> bit) & mask], 1u);
+        }
     }
     __syncthreads();
     const int d = threadIdx.x;
@@ -125,7 +130,7 @@ __global__ void __launch_bounds__(kSortThreads) radix_scan(const int* n_dev, int
 // order among equal digits. The ranked keys are first placed digit-sorted in
 // shared memory and then written out linearly, so each warp store covers a run
 // of consecutive addresses of one digit bucket instead of 32 scattered words.
-template <bool kIdentityValues>
+template <bool kIdentityValues, bool kDrop>
 __global__ void __launch_bounds__(kSortThreads) radix_downsweep(
     const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ values_in,
     uint32_t* __restrict__ keys_out, uint32_t* __restrict__ values_out, const int* n_dev, int n_host,
@@ -139,7 +144,7 @@ __global__ void __launch_bounds__(kSortThreads) radix_downsweep(
     const int64_t start = static_cast<int64_t>(blockIdx.x) * kSortChunk;
     if (start >= n) return;
     const int64_t end = min(static_cast<int64_t>(n), start + kSortChunk);
-    const int total = static_cast<int>(end - start);
+    __shared__ int s_total;  // keys of this chunk that are written (all but dropped sentinels)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int i = threadIdx.x; i < kSortWarps * kBins; i += kSortThreads) (&counts[0][0])[i] = 0;
     global_base[threadIdx.x] = block_hist[threadIdx.x * hist_stride + blockIdx.x];
@@ -155,6 +160,7 @@ __global__ void __launch_bounds__(kSortThreads) radix_downsweep(
         key[s] = valid ? keys_in[idx] : 0u;
         if (kIdentityValues) val[s] = static_cast<uint32_t>(idx);
         else val[s] = valid ? values_in[idx] : 0u;
+        if (kDrop) valid = valid && key[s] != kSortSentinel;
         uint32_t digit = valid ? ((key[s] >> bit) & mask) : 0u;
         // lanes holding the same digit: intersect the eight per-bit ballots
         uint32_t peers = __ballot_sync(0xffffffffu, valid);
@@ -190,13 +196,17 @@ __global__ void __launch_bounds__(kSortThreads) radix_downsweep(
         __shared__ uint32_t warp_tot[kSortWarps];
         if (lane == 31) warp_tot[warp] = inc;
         __syncthreads();
-        uint32_t prefix = 0;
+        uint32_t prefix = 0, all = 0;
 #pragma unroll
-        for (int w = 0; w < kSortWarps; ++w)
+        for (int w = 0; w < kSortWarps; ++w) {
             if (w < warp) prefix += warp_tot[w];
+            all += warp_tot[w];
+        }
         local_base[d] = prefix + inc - run;
+        if (kDrop && d == 0) s_total = static_cast<int>(all);
     }
     __syncthreads();
+    const int total = kDrop ? s_total : static_cast<int>(end - start);
 #pragma unroll
     for (int s = 0; s < kSortItems; ++s) {
         if (rank[s] == 0xFFFFFFFFu) continue;
@@ -212,6 +222,21 @@ __global__ void __launch_bounds__(kSortThreads) radix_downsweep(
         uint32_t pos = global_base[digit] + (j - local_base[digit]);
         keys_out[pos] = k;
         values_out[pos] = s_vals[j];
+    }
+}
+
+// Keys kept by a dropping first pass: the sum of its digit totals.
+__global__ void radix_kept(const uint32_t* __restrict__ digit_total, int* __restrict__ kept) {
+    __shared__ uint32_t part[kSortWarps];
+    uint32_t v = digit_total[threadIdx.x];
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t s = 0;
+        for (int w = 0; w < kSortWarps; ++w) s += part[w];
+        *kept = static_cast<int>(s);
     }
 }
 
@@ -244,14 +269,16 @@ __device__ __forceinline__ int block_exclusive_scan(int x, int* warp_sums, int* 
 
 __global__ void __launch_bounds__(kScanThreads) scan_reduce(const int* __restrict__ in,
                                                             const uint32_t* __restrict__ gather, int n,
+                                                            const int* __restrict__ valid_dev,
                                                             int* __restrict__ block_sums) {
     __shared__ int warp_sums[kScanThreads / 32];
     const int64_t start = static_cast<int64_t>(blockIdx.x) * kScanChunk;
+    const int valid = valid_dev ? min(*valid_dev, n) : n;
     int s = 0;
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
         int64_t i = start + k * kScanThreads + threadIdx.x;
-        if (i < n) s += gather ? in[gather[i]] : in[i];
+        if (i < valid) s += gather ? in[gather[i]] : in[i];
     }
     int total;
     block_exclusive_scan(s, warp_sums, &total);
@@ -274,17 +301,19 @@ __global__ void __launch_bounds__(kScanThreads) scan_block_sums(int* __restrict_
 }
 
 __global__ void __launch_bounds__(kScanThreads) scan_downsweep(const int* in, const uint32_t* __restrict__ gather,
-                                                               int n, const int* __restrict__ block_sums,
-                                                               int* out) {
+                                                               int n, const int* __restrict__ valid_dev,
+                                                               const int* __restrict__ block_sums, int* out) {
     __shared__ int warp_sums[kScanThreads / 32];
     __shared__ int tile[kScanChunk];
     const int64_t start = static_cast<int64_t>(blockIdx.x) * kScanChunk;
-    // striped coalesced load -> blocked per-thread sequences via shared memory
+    const int valid = valid_dev ? min(*valid_dev, n) : n;
+    // striped coalesced load -> blocked per-thread sequences via shared memory;
+    // entries from `valid` on count as zero
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
         int j = k * kScanThreads + threadIdx.x;
         int64_t i = start + j;
-        tile[j] = i < n ? (gather ? in[gather[i]] : in[i]) : 0;
+        tile[j] = i < valid ? (gather ? in[gather[i]] : in[i]) : 0;
     }
     __syncthreads();
     int v[kScanItems];
@@ -375,10 +404,10 @@ RadixSortScratch radix_sort_scratch(void* base, int max_count) {
     return s;
 }
 
-int launch_radix_sort(uint32_t* keys, uint32_t* values, uint32_t* keys_alt, uint32_t* values_alt,
-                      bool identity_values, int max_count, const int* count_device, int begin_bit,
-                      int end_bit, const RadixSortScratch& scratch, bool* result_in_alt,
-                      cudaStream_t stream) {
+static int radix_sort_impl(uint32_t* keys, uint32_t* values, uint32_t* keys_alt, uint32_t* values_alt,
+                           bool identity_values, int max_count, const int* count_device, int begin_bit,
+                           int end_bit, const RadixSortScratch& scratch, bool* result_in_alt, int* kept_device,
+                           cudaStream_t stream) {
     *result_in_alt = false;
     if (max_count <= 0 || end_bit <= begin_bit) return GSN_OK;
     const int passes = (end_bit - begin_bit + 7) / 8;
@@ -387,26 +416,60 @@ int launch_radix_sort(uint32_t* keys, uint32_t* values, uint32_t* keys_alt, uint
         return GSN_ERR_CUDA;
     const int blocks = ceil_div(max_count, kSortChunk);
     uint32_t *kin = keys, *vin = values, *kout = keys_alt, *vout = values_alt;
+    const int* count = count_device;
     for (int p = 0; p < passes; ++p) {
         int bit = begin_bit + 8 * p;
         // the last pass only looks at the bits below end_bit
         uint32_t mask = end_bit - bit >= 8 ? 0xFFu : ((1u << (end_bit - bit)) - 1u);
         uint32_t* dt = scratch.digit_total + kBins * p;
-        radix_upsweep<<<blocks, kSortThreads, 0, stream>>>(kin, count_device, max_count, bit, mask,
-                                                           scratch.block_hist, scratch.max_blocks, dt);
-        radix_scan<<<kBins, kSortThreads, 0, stream>>>(count_device, max_count, scratch.block_hist,
-                                                       scratch.max_blocks, dt);
-        if (identity_values && p == 0)
-            radix_downsweep<true><<<blocks, kSortThreads, 0, stream>>>(
-                kin, nullptr, kout, vout, count_device, max_count, bit, mask, scratch.block_hist, scratch.max_blocks);
+        const bool drop = kept_device && p == 0;
+        if (drop)
+            radix_upsweep<true><<<blocks, kSortThreads, 0, stream>>>(kin, count, max_count, bit, mask,
+                                                                     scratch.block_hist, scratch.max_blocks, dt);
         else
-            radix_downsweep<false><<<blocks, kSortThreads, 0, stream>>>(
-                kin, vin, kout, vout, count_device, max_count, bit, mask, scratch.block_hist, scratch.max_blocks);
+            radix_upsweep<false><<<blocks, kSortThreads, 0, stream>>>(kin, count, max_count, bit, mask,
+                                                                      scratch.block_hist, scratch.max_blocks, dt);
+        radix_scan<<<kBins, kSortThreads, 0, stream>>>(count, max_count, scratch.block_hist, scratch.max_blocks, dt);
+        const uint32_t* vsrc = identity_values && p == 0 ? nullptr : vin;
+        if (identity_values && p == 0 && drop)
+            radix_downsweep<true, true><<<blocks, kSortThreads, 0, stream>>>(
+                kin, vsrc, kout, vout, count, max_count, bit, mask, scratch.block_hist, scratch.max_blocks);
+        else if (identity_values && p == 0)
+            radix_downsweep<true, false><<<blocks, kSortThreads, 0, stream>>>(
+                kin, vsrc, kout, vout, count, max_count, bit, mask, scratch.block_hist, scratch.max_blocks);
+        else if (drop)
+            radix_downsweep<false, true><<<blocks, kSortThreads, 0, stream>>>(
+                kin, vsrc, kout, vout, count, max_count, bit, mask, scratch.block_hist, scratch.max_blocks);
+        else
+            radix_downsweep<false, false><<<blocks, kSortThreads, 0, stream>>>(
+                kin, vsrc, kout, vout, count, max_count, bit, mask, scratch.block_hist, scratch.max_blocks);
+        if (drop) {
+            // later passes (and the caller) see only the kept keys
+            radix_kept<<<1, kBins, 0, stream>>>(dt, kept_device);
+            count = kept_device;
+        }
         uint32_t* tk = kin; kin = kout; kout = tk;
         uint32_t* tv = vin; vin = vout; vout = tv;
     }
     *result_in_alt = (passes % 2) == 1;
-    return launched(3 * passes);
+    return launched(3 * passes + (kept_device ? 1 : 0));
+}
+
+int launch_radix_sort(uint32_t* keys, uint32_t* values, uint32_t* keys_alt, uint32_t* values_alt,
+                      bool identity_values, int max_count, const int* count_device, int begin_bit,
+                      int end_bit, const RadixSortScratch& scratch, bool* result_in_alt,
+                      cudaStream_t stream) {
+    return radix_sort_impl(keys, values, keys_alt, values_alt, identity_values, max_count, count_device, begin_bit,
+                           end_bit, scratch, result_in_alt, nullptr, stream);
+}
+
+int launch_radix_sort_dropping(uint32_t* keys, uint32_t* values, uint32_t* keys_alt, uint32_t* values_alt,
+                               bool identity_values, int max_count, const int* count_device, int begin_bit,
+                               int end_bit, const RadixSortScratch& scratch, bool* result_in_alt, int* kept_device,
+                               cudaStream_t stream) {
+    if (!kept_device) return GSN_ERR_INVALID_ARGUMENT;
+    return radix_sort_impl(keys, values, keys_alt, values_alt, identity_values, max_count, count_device, begin_bit,
+                           end_bit, scratch, result_in_alt, kept_device, stream);
 }
 
 // ---------------------------------------------------------------- no-alloc sort
@@ -453,14 +516,14 @@ size_t scan_scratch_bytes(int n) {
 }
 
 int launch_exclusive_scan(const int* in, const uint32_t* gather, int* out, int n, void* scratch,
-                          cudaStream_t stream) {
+                          cudaStream_t stream, const int* valid_device) {
     if (n < 0) return GSN_ERR_INVALID_ARGUMENT;
     int* block_sums = static_cast<int*>(scratch);
     int blocks = ceil_div(n > 0 ? n : 1, kScanChunk);
-    if (n > 0) scan_reduce<<<blocks, kScanThreads, 0, stream>>>(in, gather, n, block_sums);
+    if (n > 0) scan_reduce<<<blocks, kScanThreads, 0, stream>>>(in, gather, n, valid_device, block_sums);
     else cudaMemsetAsync(block_sums, 0, sizeof(int), stream);
     scan_block_sums<<<1, kScanThreads, 0, stream>>>(block_sums, n > 0 ? blocks : 0, out + n);
-    if (n > 0) scan_downsweep<<<blocks, kScanThreads, 0, stream>>>(in, gather, n, block_sums, out);
+    if (n > 0) scan_downsweep<<<blocks, kScanThreads, 0, stream>>>(in, gather, n, valid_device, block_sums, out);
     return launched(n > 0 ? 3 : 1);
 }
 

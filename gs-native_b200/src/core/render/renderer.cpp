@@ -46,7 +46,7 @@ bool Renderer::ReserveGaussians(int count) {
               tile_counts_.Reserve(grow) && cull_counts_.Reserve(grow) && depth_keys_[0].Reserve(grow) &&
               depth_keys_[1].Reserve(grow) &&
               depth_ids_[0].Reserve(grow) && depth_ids_[1].Reserve(grow) && record_start_.Reserve(grow + 1) &&
-              counters_.Reserve(2);
+              counters_.Reserve(3);
     if (!ok) return false;
     gaussian_capacity_ = grow;
     return true;
@@ -121,14 +121,18 @@ bool Renderer::Render(const GaussianBuffers& gaussians, const CameraParams& came
         gsn::stage_mark(s, gsn::kStageDepthSort);
         gsn::RadixSortScratch scratch = gsn::radix_sort_scratch(sort_scratch_.get(), sort_max);
         bool in_alt = false;
-        if (gsn::launch_radix_sort(depth_keys_[0].get(), depth_ids_[0].get(), depth_keys_[1].get(),
-                                   depth_ids_[1].get(), true, count, nullptr, 0, 32, scratch, &in_alt,
-                                   s) != GSN_OK)
+        // culled Gaussians (depth key 0xFFFFFFFF) leave the sort in its first
+        // pass: the later passes, the record scan and the emission see only the
+        // visible ones (their order - depth, then id - is unchanged)
+        int* visible = counters_.get() + 2;
+        if (gsn::launch_radix_sort_dropping(depth_keys_[0].get(), depth_ids_[0].get(), depth_keys_[1].get(),
+                                            depth_ids_[1].get(), true, count, nullptr, 0, 32, scratch, &in_alt,
+                                            visible, s) != GSN_OK)
             return false;
         const uint32_t* by_depth = depth_ids_[in_alt ? 1 : 0].get();
         gsn::stage_mark(s, gsn::kStageRecordScan);
         if (gsn::launch_exclusive_scan(exact_culling_ ? cull_counts_.get() : tile_counts_.get(), by_depth,
-                                       record_start_.get(), count, scan_scratch_.get(), s) != GSN_OK)
+                                       record_start_.get(), count, scan_scratch_.get(), s, visible) != GSN_OK)
             return false;
         if (cudaMemcpyAsync(record_count, record_start_.get() + count, sizeof(int), cudaMemcpyDeviceToDevice,
                             s) != cudaSuccess)

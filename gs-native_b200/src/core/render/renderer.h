@@ -125,7 +125,7 @@ private:
     size_t sort_scratch_count_ = 0;
     mutable DeviceArray<unsigned char> scan_scratch_;
     mutable size_t scan_scratch_count_ = 0;
-    DeviceArray<int> counters_;  // [0] record count, [1] overflow flag
+    DeviceArray<int> counters_;  // [0] record count, [1] overflow flag, [2] visible Gaussians
     int* host_records_ = nullptr;  // pinned
 };
 
