@@ -21,7 +21,8 @@ capacity and replayed from a device schedule of views), `culled_fp32` /
 >= 1/255 ellipse reaches are emitted and sorted; images and gradients are
 unchanged), `culled_sparse_fp32` / `culled_sparse_graph_fp32` (culling plus the
 visibility-masked Adam step on the Morton-ordered model the trainer's spatial
-order keeps; Gaussians outside the view keep p, m, v) and
+order keeps - Gaussians outside the view keep p, m, v - and the fast blend
+arithmetic) and
 `precision_bf16_culled_sparse` / `..._graph` (all of that plus SH rows and their
 Adam moments stored in bf16 with stochastic rounding; fp32 blending and
 accumulation). `value` is the fastest form that completed without a record
@@ -363,6 +364,9 @@ def run_gsn(args):
             self.solver.set_stream(sp)
             self.renderer.set_exact_culling(culled)
             self.solver.set_sparse_adam(sparse)
+            # the sparse forms already leave the reference's arithmetic: they also
+            # take the fast blend arithmetic (Horner power, hardware exp2)
+            self.renderer.set_fast_blend(sparse)
             block = model
             if sparse:
                 # the trainer's spatial order (Morton order of the means after every
@@ -623,6 +627,13 @@ def run_gsn(args):
                    "l2": "inputs larger than L2 (params + Adam moments 835 MB, a new 5 MB target per step)"},
         "gpu_launches": forms[chosen]["gpu_launches"],
         "forms": forms,
+        "form_switches": {
+            "plain_fp32": "reference arithmetic, dense Adam", "graph_fp32": "plain as one CUDA graph per step",
+            "culled_fp32": "exact tile culling (images bit-identical to plain)", "culled_graph_fp32": "culled + graph",
+            "culled_sparse_fp32": "culled + visibility-masked Adam on the Morton-ordered model + fast blend arithmetic",
+            "culled_sparse_graph_fp32": "culled_sparse + graph",
+            "precision_bf16_culled_sparse": "culled_sparse + bf16 SH storage and moments + tcgen05 SSIM",
+            "precision_bf16_culled_sparse_graph": "precision + graph"},
         "chosen_over_plain": round(forms[chosen]["value"] / value, 4),
         "e2e": {"value": forms[chosen]["e2e"], "unit": UNIT, "h2d_bytes_per_step": 1600 * 1064 * 3,
                 "d2h_bytes_per_step": 32, "psnr_db_last_step": forms[chosen]["psnr_db_last_step"],

@@ -234,6 +234,12 @@ int gsn_renderer_set_exact_culling(gsn_renderer* r, int enabled) {
     return GSN_OK;
 }
 
+int gsn_renderer_set_fast_blend(gsn_renderer* r, int enabled) {
+    if (!r) return GSN_ERR_INVALID_ARGUMENT;
+    r->impl.SetFastBlend(enabled != 0);
+    return GSN_OK;
+}
+
 int gsn_renderer_set_record_capacity(gsn_renderer* r, int64_t records) {
     if (!r) return GSN_ERR_INVALID_ARGUMENT;
     return r->impl.SetRecordCapacity(records) ? GSN_OK : GSN_ERR_INVALID_ARGUMENT;
@@ -495,6 +501,7 @@ int gsn_training_options_default(gsn_training_options* out) {
     out->exact_culling = o.exact_culling ? 1 : 0;
     out->sparse_adam = o.sparse_adam ? 1 : 0;
     out->spatial_order = o.spatial_order ? 1 : 0;
+    out->fast_blend = o.fast_blend ? 1 : 0;
     return GSN_OK;
 }
 
@@ -535,6 +542,7 @@ gs_native::TrainingOptions ToOptions(const gsn_training_options& in) {
     o.exact_culling = in.exact_culling != 0;
     o.sparse_adam = in.sparse_adam != 0;
     o.spatial_order = in.spatial_order != 0;
+    o.fast_blend = in.fast_blend != 0;
     return o;
 }
 }  // namespace

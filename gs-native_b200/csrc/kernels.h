@@ -149,6 +149,7 @@ struct RasterForwardArgs {
     // pixel of warp w's strip took record r
     uint32_t* record_warps;
     int64_t record_words;
+    bool fast;                     // fast power / exp arithmetic (see raster_common.cuh Power)
 };
 int launch_raster_forward(const RasterForwardArgs& a, cudaStream_t stream);
 
@@ -186,6 +187,7 @@ struct RasterBackwardArgs {
     const int* contributors;   // per-pixel record bound from the forward pass (optional)
     const uint32_t* record_warps;  // the forward pass's bit planes (optional)
     int64_t record_words;
+    bool fast;                 // the forward pass's arithmetic form (must match it)
     gsn_camera cam;
     float* grad_out;           // [N][12] screen-space accumulators, zeroed by the caller
 };

@@ -37,6 +37,7 @@ constexpr int kVals = 12;
 
 __device__ __forceinline__ float sel(bool c, float a, float b) { return c ? a : b; }
 
+template <bool kFast>
 __global__ void __launch_bounds__(kRasterThreads, 12) raster_backward_kernel(RasterBackwardArgs a) {
     __shared__ uint32_t s_id[kRasterBatch];
     __shared__ float2 s_mean[kRasterBatch];
@@ -139,6 +140,7 @@ __global__ void __launch_bounds__(kRasterThreads, 12) raster_backward_kernel(Ras
                 const float3 col = s_color[j];
                 const float cc[3] = {col.x, col.y, col.z};
                 const float dx = mu.x - fx;
+                const Power<kFast> power(q, dx);
                 float v[kVals];
 #pragma unroll
                 for (int i = 0; i < kVals; ++i) v[i] = 0.0f;
@@ -151,7 +153,7 @@ __global__ void __launch_bounds__(kRasterThreads, 12) raster_backward_kernel(Ras
                 for (int p = 0; p < kPixPerThread; ++p) {
                     done[p] = done[p] || rel + j >= limit[p];
                     dyv[p] = mu.y - fy[p];
-                    pw[p] = -0.5f * (q.x * dx * dx + q.z * dyv[p] * dyv[p]) - q.y * dx * dyv[p];
+                    pw[p] = power.at(dyv[p]);
                     act[p] = !done[p] && !(pw[p] > 0.0f) && !(pw[p] < lim);
                     any |= act[p];
                 }
@@ -160,7 +162,7 @@ __global__ void __launch_bounds__(kRasterThreads, 12) raster_backward_kernel(Ras
 #pragma unroll
                     for (int p = 0; p < kPixPerThread; ++p) {
                         const float dy = dyv[p];
-                        float raw = q.w * expf(pw[p]);
+                        float raw = gaussian_weight<kFast>(q.w, pw[p]);
                         float alpha = fminf(kAlphaMax, raw);
                         bool take = act[p] && !(alpha < kAlphaMin);
                         float nextT = T[p] * (1.0f - alpha);
@@ -237,7 +239,8 @@ __global__ void __launch_bounds__(kRasterThreads, 12) raster_backward_kernel(Ras
 int launch_raster_backward(const RasterBackwardArgs& a, cudaStream_t stream) {
     int64_t tiles = static_cast<int64_t>(a.cam.tile_count_x) * a.cam.tile_count_y;
     if (tiles <= 0) return GSN_OK;
-    raster_backward_kernel<<<static_cast<unsigned>(tiles), kRasterThreads, 0, stream>>>(a);
+    if (a.fast) raster_backward_kernel<true><<<static_cast<unsigned>(tiles), kRasterThreads, 0, stream>>>(a);
+    else raster_backward_kernel<false><<<static_cast<unsigned>(tiles), kRasterThreads, 0, stream>>>(a);
     return launched(1);
 }
 

@@ -75,6 +75,37 @@ __device__ __forceinline__ float alpha_floor(float opacity) {
     return -logf(lo) - 1e-3f;
 }
 
+// Gaussian power -(A dx^2 + C dy^2) / 2 - B dx dy of a record at the pixels of
+// one column (shared dx). The exact form evaluates the reference's expression
+// per pixel (renderer.cu:300-303) so images match it bit for bit; the fast form
+// (kFast) hoists the per-record terms and evaluates two FMAs per pixel, which
+// moves the result by a few ulps - far inside the alpha floor's and the alpha
+// box's margins, so every skip decision stays conservative.
+template <bool kFast>
+struct Power {
+    float a, b, c;  // fast form: a + dy * (b + c * dy)
+    float4 q;
+    float dx;
+    __device__ __forceinline__ Power(float4 conic, float delta_x) : q(conic), dx(delta_x) {
+        if (kFast) {
+            a = -0.5f * q.x * dx * dx;
+            b = -q.y * dx;
+            c = -0.5f * q.z;
+        }
+    }
+    __device__ __forceinline__ float at(float dy) const {
+        if (kFast) return fmaf(fmaf(c, dy, b), dy, a);
+        return -0.5f * (q.x * dx * dx + q.z * dy * dy) - q.y * dx * dy;
+    }
+};
+
+// o * e^power: the reference's expf in the exact form, the hardware exp2
+// approximation (__expf) in the fast form.
+template <bool kFast>
+__device__ __forceinline__ float gaussian_weight(float opacity, float power) {
+    return kFast ? opacity * __expf(power) : opacity * expf(power);
+}
+
 // Does the box of a record overlap the pixel rectangle [x0, x1] x [y0, y1]?
 __device__ __forceinline__ bool box_hits(float4 b, float x0, float x1, float y0, float y1) {
     return b.x <= x1 && b.y >= x0 && b.z <= y1 && b.w >= y0;

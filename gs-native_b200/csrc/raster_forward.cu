@@ -49,6 +49,7 @@ __device__ __forceinline__ Staged fetch(const RasterForwardArgs& a, int64_t r, i
     return s;
 }
 
+template <bool kFast>
 __global__ void __launch_bounds__(kRasterThreads) raster_forward_kernel(RasterForwardArgs a) {
     __shared__ float2 s_mean[kRasterBatch];
     __shared__ float4 s_conic[kRasterBatch];
@@ -111,6 +112,7 @@ __global__ void __launch_bounds__(kRasterThreads) raster_forward_kernel(RasterFo
                 const float lim = s_floor[j];
                 const float3 c = s_color[j];
                 const float dx = mu.x - fx;
+                const Power<kFast> power(q, dx);
                 // the four pixels are evaluated without branches (selects only),
                 // so their dependency chains interleave; values of a pixel that
                 // does not take the record are computed but discarded
@@ -120,14 +122,14 @@ __global__ void __launch_bounds__(kRasterThreads) raster_forward_kernel(RasterFo
 #pragma unroll
                 for (int p = 0; p < kPixPerThread; ++p) {
                     float dy = mu.y - fy[p];
-                    pw[p] = -0.5f * (q.x * dx * dx + q.z * dy * dy) - q.y * dx * dy;
+                    pw[p] = power.at(dy);
                     act[p] = !done[p] && !(pw[p] > 0.0f) && !(pw[p] < lim);
                     any |= act[p];
                 }
                 if (!any) continue;
 #pragma unroll
                 for (int p = 0; p < kPixPerThread; ++p) {
-                    float alpha = fminf(kAlphaMax, q.w * expf(pw[p]));
+                    float alpha = fminf(kAlphaMax, gaussian_weight<kFast>(q.w, pw[p]));
                     bool take = act[p] && !(alpha < kAlphaMin);
                     float nextT = T[p] * (1.0f - alpha);
                     bool stop = take && nextT < kTransmittanceMin;
@@ -174,7 +176,8 @@ __global__ void __launch_bounds__(kRasterThreads) raster_forward_kernel(RasterFo
 int launch_raster_forward(const RasterForwardArgs& a, cudaStream_t stream) {
     int64_t tiles = static_cast<int64_t>(a.cam.tile_count_x) * a.cam.tile_count_y;
     if (tiles <= 0) return GSN_OK;
-    raster_forward_kernel<<<static_cast<unsigned>(tiles), kRasterThreads, 0, stream>>>(a);
+    if (a.fast) raster_forward_kernel<true><<<static_cast<unsigned>(tiles), kRasterThreads, 0, stream>>>(a);
+    else raster_forward_kernel<false><<<static_cast<unsigned>(tiles), kRasterThreads, 0, stream>>>(a);
     return launched(1);
 }
 

@@ -179,6 +179,10 @@ class Renderer:
     def set_exact_culling(self, enabled=True):
         _check(lib().gsn_renderer_set_exact_culling(self.handle, int(bool(enabled))), "set_exact_culling")
 
+    def set_fast_blend(self, enabled=True):
+        fn = declare("gsn_renderer_set_fast_blend", [ctypes.c_void_p, ctypes.c_int])
+        _check(fn(self.handle, int(bool(enabled))), "set_fast_blend")
+
 
 def launch_count():
     return int(lib().gsn_kernel_launch_count())
@@ -441,6 +445,7 @@ class TrainingOptions(ctypes.Structure):
         ("precision", ctypes.c_int), ("graph", ctypes.c_int),
         ("learned_density", ctypes.c_int), ("learned_confidence", ctypes.c_float), ("log_density", ctypes.c_int),
         ("exact_culling", ctypes.c_int), ("sparse_adam", ctypes.c_int), ("spatial_order", ctypes.c_int),
+        ("fast_blend", ctypes.c_int),
     ]
 
     @classmethod

@@ -91,6 +91,7 @@ bool GaussianSplatting::Initialize(const TrainingScene& scene, const TrainingOpt
     density_.SetMaxGaussians(options_.max_gaussians);
     renderer_.SetBf16Sh(options_.bf16_sh);
     renderer_.SetExactCulling(options_.exact_culling);
+    renderer_.SetFastBlend(options_.fast_blend);
     eval_renderer_.SetBf16Sh(options_.bf16_sh);
     solver_.SetBf16Sh(options_.bf16_sh);
     density_.SetBf16Sh(options_.bf16_sh);

@@ -78,6 +78,7 @@ struct TrainingOptions {
     // Morton order of the Gaussians after initialisation and every density step
     // (SpatialOrder): no value changes, the sparse update skips whole sectors
     bool spatial_order = false;
+    bool fast_blend = false;  // training renderer's fast blend arithmetic (Renderer::SetFastBlend)
 };
 
 // Statistics, decisions and parent map of the last density-control step

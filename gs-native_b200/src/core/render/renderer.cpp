@@ -198,6 +198,7 @@ bool Renderer::Render(const GaussianBuffers& gaussians, const CameraParams& came
     ra.contributors = contributors_.get();
     ra.record_warps = record_warps_.get();
     ra.record_words = record_words_;
+    ra.fast = fast_blend_;
     if (record_warps_.get() &&
         cudaMemsetAsync(record_warps_.get(), 0, 2 * static_cast<size_t>(record_words_) * sizeof(uint32_t), s) !=
             cudaSuccess)

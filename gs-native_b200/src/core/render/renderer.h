@@ -65,6 +65,13 @@ public:
     // reference's lists minus records that never contribute. GetTileCounts and
     // GetRecordOffsets keep the rectangle counts (the visibility statistic).
     void SetExactCulling(bool enabled) { exact_culling_ = enabled; }
+    // Fast blend arithmetic: the Gaussian power in Horner form with per-record
+    // terms hoisted and the hardware exp2 approximation, instead of the
+    // reference's per-pixel expression and expf. Images move by a few ulps
+    // (no longer bit-identical to the reference); the solver's backward
+    // follows the renderer's setting.
+    void SetFastBlend(bool enabled) { fast_blend_ = enabled; }
+    bool GetFastBlend() const { return fast_blend_; }
     bool GetExactCulling() const { return exact_culling_; }
     bool GetBf16Sh() const { return bf16_sh_; }
     const int* GetTileCounts() const { return tile_counts_.get(); }
@@ -97,6 +104,7 @@ private:
     const gsn_camera* device_camera_ = nullptr;
     bool bf16_sh_ = false;
     bool exact_culling_ = false;
+    bool fast_blend_ = false;
     int64_t last_records_ = 0;
     int last_count_ = 0;
 

@@ -128,6 +128,7 @@ bool Solver::ComputeScreenGradients(const CameraParams& camera, const Renderer& 
     a.contributors = renderer.GetContributors();
     a.record_warps = renderer.GetRecordWarps();
     a.record_words = renderer.GetRecordWords();
+    a.fast = renderer.GetFastBlend();
     a.cam = AsGsnCamera(camera);
     a.grad_out = screen_.get();
     return gsn::launch_raster_backward(a, stream_) == GSN_OK;

@@ -10,7 +10,7 @@ wall and device time, the final Gaussian count and the mean FP64 PSNR of the
 held-out views.
 
     python synthetic_run.py [--iterations 30000] [--cap 1200000] [--width 1600 --height 1064]
-                            [--precision] [--graph] [--culled] [--sparse]
+                            [--precision] [--graph] [--culled] [--sparse] [--fast]
 """
 import argparse
 import json
@@ -67,6 +67,7 @@ def main():
     p.add_argument("--graph", action="store_true", help="steady-state iterations as CUDA-graph replays")
     p.add_argument("--culled", action="store_true", help="exact tile culling in the training renderer")
     p.add_argument("--sparse", action="store_true", help="visibility-masked Adam on the Morton-ordered model")
+    p.add_argument("--fast", action="store_true", help="fast blend arithmetic (Horner power, hardware exp2)")
     args = p.parse_args()
     import torch
 
@@ -76,7 +77,8 @@ def main():
     setup_s = time.time() - t0
     opts = gsn.TrainingOptions.defaults(max_gaussians=args.cap, precision=int(args.precision),
                                         graph=int(args.graph), exact_culling=int(args.culled),
-                                        sparse_adam=int(args.sparse), spatial_order=int(args.sparse))
+                                        sparse_adam=int(args.sparse), spatial_order=int(args.sparse),
+                                        fast_blend=int(args.fast))
     trainer = gsn.Trainer()
     assert trainer.initialize(train, train_images, points, colors, opts) == 0
     torch.cuda.synchronize()
@@ -104,7 +106,8 @@ def main():
         "psnr_test_db": round(psnr, 4), "loss_test": round(loss, 6), "psnr_train_subset_db": round(psnr_train, 4),
         "setup_s": round(setup_s, 1), "resolution": [args.width, args.height], "cap": args.cap,
         "form": ("precision_bf16" if args.precision else "plain_fp32") + ("_culled" if args.culled else "") +
-                ("_sparse" if args.sparse else "") + ("_graph" if args.graph else ""), "log": log,
+                ("_sparse" if args.sparse else "") + ("_fast" if args.fast else "") + ("_graph" if args.graph else ""),
+        "log": log,
     }), flush=True)
 
 

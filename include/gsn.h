@@ -169,6 +169,11 @@ int gsn_renderer_set_bf16_sh(gsn_renderer* r, int enabled);
  * that never contribute. Tile counts / record offsets keep the rectangle
  * counts (the solver's visibility statistic, solver.cu:484). */
 int gsn_renderer_set_exact_culling(gsn_renderer* r, int enabled);
+/* Fast blend arithmetic (gs-native extension): the per-pixel Gaussian power in
+ * Horner form with per-record terms hoisted and the hardware exp2
+ * approximation, instead of the expression and expf of renderer.cu:300-305.
+ * Images move by a few ulps; the solver's backward pass follows the setting. */
+int gsn_renderer_set_fast_blend(gsn_renderer* r, int enabled);
 
 
 /* ------------------------------------------------------------------ solver
@@ -324,6 +329,7 @@ typedef struct gsn_training_options {
     int exact_culling;               /* 1: exact tile culling in the training renderer (gsn_renderer_set_exact_culling) */
     int sparse_adam;                 /* 1: visibility-masked Adam (gsn_solver_set_sparse_adam) */
     int spatial_order;               /* 1: Morton order of the Gaussians after init and every density step */
+    int fast_blend;                  /* 1: fast blend arithmetic in the training renderer (gsn_renderer_set_fast_blend) */
 } gsn_training_options;
 
 int gsn_training_options_default(gsn_training_options* out);

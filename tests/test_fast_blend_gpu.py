@@ -1,0 +1,54 @@
+"""Fast blend arithmetic (Renderer::SetFastBlend): the Gaussian power in Horner
+form with hoisted per-record terms and the hardware exp2 approximation. The
+image stays within float rounding of the reference arithmetic's, the backward
+follows the renderer's setting, and its gradients agree to the tolerance the
+solver's parity tests use for reordered float sums."""
+import numpy as np
+import pytest
+
+import gsn
+import scenes
+from helpers import dev, empty, host, sync, torch
+from test_solver_gpu import rows_close
+
+pytestmark = pytest.mark.gpu
+
+
+def _frame(fast, params, cam, target):
+    t = torch()
+    p = dev(params)
+    img = empty((cam.height, cam.width, 3), t.float32)
+    r, s = gsn.Renderer(), gsn.Solver()
+    r.set_fast_blend(fast)
+    assert r.render(p.data_ptr(), params.shape[1], cam, [0.2, 0.3, 0.4], img.data_ptr(), 3) == 0
+    tgt = dev(target)
+    s.image_gradients(cam, img.data_ptr(), tgt.data_ptr())
+    ptr = s.screen_gradients(cam, r, img.data_ptr(), p.data_ptr(), params.shape[1])
+    sync()
+    return img.cpu().numpy(), host(ptr, np.float32, 12 * params.shape[1]).reshape(-1, 12)
+
+
+@pytest.mark.parametrize("culled", [False, True])
+def test_fast_blend_matches_reference_arithmetic(culled):
+    params = scenes.random_gaussians(40000, 12, mean_sigma=3.0)
+    cam = scenes.ring_cameras(8, 8.0, 15.0, 480, 360, 420.0, 420.0)[2]
+    target = np.random.default_rng(3).integers(0, 256, size=(cam.height, cam.width, 3), dtype=np.uint8)
+    exact_img, exact_g = _frame(False, params, cam, target)
+    fast_img, fast_g = _frame(True, params, cam, target)
+    diff = np.abs(fast_img - exact_img)
+    assert diff.max() < 1e-4 and diff.mean() < 1e-6
+    ok, where = rows_close(fast_g[:, :11].T, exact_g[:, :11].T, rel=1e-3, floor=1e-4)
+    assert ok, where
+
+
+def test_training_with_fast_blend():
+    import test_trainer_gpu as tt
+    cams, images, points, colors = tt.ring_scene()
+    res = []
+    for fast in (0, 1):
+        opts = gsn.TrainingOptions.defaults(densify_from=100000, densify_until=100, fast_blend=fast)
+        tr = gsn.Trainer()
+        assert tr.initialize(cams, images, points, colors, opts) == 0
+        assert tr.train(400) == 0
+        res.append(tr.evaluate_metrics(cams, images)["psnr"])
+    assert abs(res[0] - res[1]) < 0.02
