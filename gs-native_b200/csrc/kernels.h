@@ -158,8 +158,10 @@ int launch_raster_forward(const RasterForwardArgs& a, cudaStream_t stream);
 // HWC target. `sums` (optional, 3 doubles, zeroed by the launcher) receives
 // sum|I - T|, sum SSIM and sum (I - T)^2 in FP64.
 // frame (optional): the target is frame->target instead of `target`.
+// fast: products of the moments formed once per input, not once per tap (the
+// sums round differently from the reference's kernel; the fast forms only).
 int launch_loss_gradient(const float* image, const uint8_t* target, const StepFrame* frame, float* grad, int width,
-                         int height, double* sums, cudaStream_t stream);
+                         int height, double* sums, cudaStream_t stream, bool fast = false);
 // Precision form of the same gradient: the 11x11 window runs as banded-Toeplitz
 // GEMMs on the tcgen05 tensor cores with a hi/lo bf16 split and fp32
 // accumulation (loss_tc.cu). *status (device) is set to GSN_ERR_TIMEOUT if a

@@ -58,6 +58,7 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
 // One block per 32x32 output tile and colour channel. Every filter output is
 // produced by one thread from a register window of its row (or column), with
 // the 11 taps accumulated in ascending order as in solver.cu:65-161.
+template <bool kFast>
 __global__ void __launch_bounds__(kThreads, 3) loss_gradient_kernel(const float* __restrict__ image,
                                                                    const uint8_t* __restrict__ target_arg,
                                                                    const StepFrame* __restrict__ frame,
@@ -95,6 +96,24 @@ __global__ void __launch_bounds__(kThreads, 3) loss_gradient_kernel(const float*
             a[k] = raw_i[r * kIn + c0 + k];
             b[k] = raw_t[r * kIn + c0 + k];
         }
+        if constexpr (kFast) {
+            // fast form: each product (x^2, y^2, xy) is formed once per input
+            // instead of once per tap, and every moment is one 11-FMA chain
+#pragma unroll
+            for (int m = 0; m < 5; ++m) {
+                float v[kSeg1 + 10];
+#pragma unroll
+                for (int k = 0; k < kSeg1 + 10; ++k)
+                    v[k] = m == 0 ? a[k] : m == 1 ? b[k] : m == 2 ? a[k] * a[k] : m == 3 ? b[k] * b[k] : a[k] * b[k];
+#pragma unroll
+                for (int o = 0; o < kSeg1; ++o) {
+                    float acc = 0.0f;
+#pragma unroll
+                    for (int dx = 0; dx < 11; ++dx) acc = fmaf(c_window[dx], v[o + dx], acc);
+                    mom[m * kMom + r * kCen + c0 + o] = acc;
+                }
+            }
+        } else {
 #pragma unroll
         for (int o = 0; o < kSeg1; ++o) {
             float h0 = 0.f, h1 = 0.f, h2 = 0.f, h3 = 0.f, h4 = 0.f;
@@ -114,6 +133,7 @@ __global__ void __launch_bounds__(kThreads, 3) loss_gradient_kernel(const float*
             mom[2 * kMom + idx] = h2;
             mom[3 * kMom + idx] = h3;
             mom[4 * kMom + idx] = h4;
+        }
         }
     }
     __syncthreads();
@@ -256,21 +276,30 @@ __global__ void finalize_loss_kernel(const double* sums, int width, int height, 
 }  // namespace
 
 int launch_loss_gradient(const float* image, const uint8_t* target, const StepFrame* frame, float* grad, int width,
-                         int height, double* sums, cudaStream_t stream) {
+                         int height, double* sums, cudaStream_t stream, bool fast) {
     if (width <= 0 || height <= 0) return GSN_ERR_INVALID_ARGUMENT;
     if (sums && cudaMemsetAsync(sums, 0, 3 * sizeof(double), stream) != cudaSuccess) return GSN_ERR_CUDA;
-    // the dynamic shared-memory opt-in is a per-device function attribute
-    static bool configured[64] = {};
+    // the dynamic shared-memory opt-in is a per-device, per-kernel attribute
+    static bool configured[64][2] = {};
     int device = 0;
     if (cudaGetDevice(&device) != cudaSuccess) return GSN_ERR_CUDA;
-    if (device < 0 || device >= 64 || !configured[device]) {
-        if (cudaFuncSetAttribute(loss_gradient_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(kSmemBytes)) != cudaSuccess)
-            return GSN_ERR_CUDA;
-        if (device >= 0 && device < 64) configured[device] = true;
+    if (device < 0 || device >= 64) return GSN_ERR_CUDA;
+    if (!configured[device][fast ? 1 : 0]) {
+        const cudaError_t e =
+            fast ? cudaFuncSetAttribute(loss_gradient_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(kSmemBytes))
+                 : cudaFuncSetAttribute(loss_gradient_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(kSmemBytes));
+        if (e != cudaSuccess) return GSN_ERR_CUDA;
+        configured[device][fast ? 1 : 0] = true;
     }
     dim3 grid(ceil_div(width, kT), ceil_div(height, kT), 3);
-    loss_gradient_kernel<<<grid, kThreads, kSmemBytes, stream>>>(image, target, frame, grad, width, height, sums);
+    if (fast)
+        loss_gradient_kernel<true><<<grid, kThreads, kSmemBytes, stream>>>(image, target, frame, grad, width, height,
+                                                                          sums);
+    else
+        loss_gradient_kernel<false><<<grid, kThreads, kSmemBytes, stream>>>(image, target, frame, grad, width, height,
+                                                                           sums);
     return launched(1);
 }
 

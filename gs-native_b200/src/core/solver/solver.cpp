@@ -30,7 +30,11 @@ void Solver::SetBf16Sh(bool enabled) {
 
 bool Solver::Iterate(const CameraParams& camera, const Renderer& renderer, const float* image, const uint8_t* target,
                      GaussianBuffers& gaussians, float position_learning_rate, int sh_degree) {
-    if (!ComputeImageGradients(camera, image, target)) return false;
+    // the fast blend forms also take the fast SSIM moments
+    fast_loss_ = renderer.GetFastBlend();
+    const bool ok = ComputeImageGradients(camera, image, target);
+    fast_loss_ = false;
+    if (!ok) return false;
     if (!ComputeScreenGradients(camera, renderer, gaussians, image)) return false;
     return UpdateGaussians(camera, renderer, gaussians, position_learning_rate, sh_degree, true, nullptr);
 }
@@ -91,7 +95,7 @@ bool Solver::ComputeImageGradients(const CameraParams& camera, const float* imag
                                          camera.height_, sums, status_.get(), stream_) != GSN_OK)
             return false;
     } else if (gsn::launch_loss_gradient(image, target, frame_, image_gradients_.get(), camera.width_,
-                                         camera.height_, sums, stream_) != GSN_OK) {
+                                         camera.height_, sums, stream_, fast_loss_) != GSN_OK) {
         return false;
     }
     if (sums && gsn::launch_finalize_loss(sums, camera.width_, camera.height_, loss_.get() + 3, stream_) != GSN_OK)

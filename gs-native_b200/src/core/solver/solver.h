@@ -145,6 +145,7 @@ private:
     bool bf16_sh_ = false;
     bool tensor_core_loss_ = false;
     bool sparse_adam_ = false;
+    bool fast_loss_ = false;  // set by Iterate from the renderer's fast blend setting
     DeviceArray<int> status_;
 };
 
