@@ -13,7 +13,7 @@ means N(0, 3^2)); 200 cameras on a ring of radius 8 at elevation +/-15 deg,
 hidden model and quantised to u8. The model being optimised is a 1.2M-Gaussian
 draw of the same distribution (seed 8).
 
-Eight forms of the same iteration are timed, each from the same initial model:
+Ten forms of the same iteration are timed, each from the same initial model:
 `plain_fp32` (eager launches from the host, the reference-parity form),
 `graph_fp32` (the iteration captured once as a CUDA graph over a fixed record
 capacity and replayed from a device schedule of views), `culled_fp32` /
@@ -24,8 +24,9 @@ visibility-masked Adam step on the Morton-ordered model the trainer's spatial
 order keeps - Gaussians outside the view keep p, m, v - and the fast blend
 arithmetic) and
 `precision_bf16_culled_sparse` / `..._graph` (all of that plus SH rows and their
-Adam moments stored in bf16 with stochastic rounding; fp32 blending and
-accumulation). `value` is the fastest form that completed without a record
+Adam moments stored in bf16 with stochastic rounding and the tcgen05 SSIM; fp32
+blending and accumulation) and `precision_bf16_fp32ssim_culled_sparse` /
+`..._graph` (the same with the fp32 CUDA-core SSIM gradient). `value` is the fastest form that completed without a record
 overflow; all are in `forms`, with `chosen_over_plain` the ratio to the plain
 form. The held-out PSNR of each form's full training run is measured by
 synthetic_run.py (the metric's 0.1 dB condition).
@@ -358,7 +359,7 @@ def run_gsn(args):
     class Form:
         """One form of the iteration: its own renderer, solver and parameter block."""
 
-        def __init__(self, bf16, culled=False, sparse=False):
+        def __init__(self, bf16, culled=False, sparse=False, tc_loss=True):
             self.renderer, self.solver = gsn.Renderer(), gsn.Solver()
             self.renderer.set_stream(sp)
             self.solver.set_stream(sp)
@@ -379,6 +380,7 @@ def run_gsn(args):
             if bf16:
                 self.renderer.set_bf16_sh(True)
                 self.solver.set_bf16_sh(True)
+                self.solver.set_tensor_core_loss(tc_loss)
                 self.params = gsn.to_precision_layout(block, torch)
             else:
                 self.params = torch.from_numpy(np.ascontiguousarray(block)).cuda()
@@ -553,8 +555,12 @@ def run_gsn(args):
     torch.cuda.empty_cache()
     prec = Form(True, True, True)
     prec_eager, prec_graph, prec_stages, _, _ = measure(prec)
-    clocks = sampler.stop() if sampler else None
     del prec
+    torch.cuda.empty_cache()
+    prec32 = Form(True, True, True, tc_loss=False)
+    prec32_eager, prec32_graph, prec32_stages, _, _ = measure(prec32, with_stages=True)
+    clocks = sampler.stop() if sampler else None
+    del prec32
     value = plain_eager["value"]
     ms = plain_eager["ms_per_step"] * args.steps
     psnr = plain_eager["psnr_db_last_step"]
@@ -581,14 +587,17 @@ def run_gsn(args):
     forms = {"plain_fp32": plain_eager, "graph_fp32": plain_graph, "culled_fp32": culled_eager,
              "culled_graph_fp32": culled_graph, "culled_sparse_fp32": sparse_eager,
              "culled_sparse_graph_fp32": sparse_graph, "precision_bf16_culled_sparse": prec_eager,
-             "precision_bf16_culled_sparse_graph": prec_graph}
+             "precision_bf16_culled_sparse_graph": prec_graph,
+             "precision_bf16_fp32ssim_culled_sparse": prec32_eager,
+             "precision_bf16_fp32ssim_culled_sparse_graph": prec32_graph}
     valid = {k: v for k, v in forms.items() if v.get("status", 0) == 0}
     chosen = max(valid, key=lambda k: valid[k]["value"])
 
     def roofline_of(form):
         """Roofline of the largest HBM-bound stage of a form, from its live stage times."""
         culled_f, sparse_f, bf16_f = "culled" in form, "sparse" in form, form.startswith("precision")
-        st = prec_stages if bf16_f else sparse_stages if sparse_f else culled_stages if culled_f else stages
+        st = (prec32_stages if "fp32ssim" in form else prec_stages) if bf16_f else \
+            sparse_stages if sparse_f else culled_stages if culled_f else stages
         rec = culled_records if culled_f else records
         ab = algorithmic_bytes(n, rec, tiles, pixels, tile_passes=passes, visible=vis, culled=culled_f,
                                sparse=sparse_f, bf16=bf16_f)
@@ -633,7 +642,9 @@ def run_gsn(args):
             "culled_sparse_fp32": "culled + visibility-masked Adam on the Morton-ordered model + fast blend arithmetic",
             "culled_sparse_graph_fp32": "culled_sparse + graph",
             "precision_bf16_culled_sparse": "culled_sparse + bf16 SH storage and moments + tcgen05 SSIM",
-            "precision_bf16_culled_sparse_graph": "precision + graph"},
+            "precision_bf16_culled_sparse_graph": "precision + graph",
+            "precision_bf16_fp32ssim_culled_sparse": "precision with the fp32 CUDA-core SSIM gradient",
+            "precision_bf16_fp32ssim_culled_sparse_graph": "precision_bf16_fp32ssim + graph"},
         "chosen_over_plain": round(forms[chosen]["value"] / value, 4),
         "e2e": {"value": forms[chosen]["e2e"], "unit": UNIT, "h2d_bytes_per_step": 1600 * 1064 * 3,
                 "d2h_bytes_per_step": 32, "psnr_db_last_step": forms[chosen]["psnr_db_last_step"],
@@ -648,6 +659,7 @@ def run_gsn(args):
         "stages_culled": {k: round(v, 4) for k, v in culled_stages.items()},
         "stages_culled_sparse": {k: round(v, 4) for k, v in sparse_stages.items()},
         "stages_precision": {k: round(v, 4) for k, v in prec_stages.items()},
+        "stages_precision_fp32ssim": {k: round(v, 4) for k, v in prec32_stages.items()},
         "records": {"plain": records, "culled": culled_records},
         "multiview": multiview,
         "clocks": clocks,

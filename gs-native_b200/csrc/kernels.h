@@ -56,6 +56,7 @@ struct ProjectOutputs {
     uint32_t* depth_keys;    // [N] float bits of z, 0xFFFFFFFF when culled
     float* radii;            // [N] optional 3-sigma pixel radius (0 = culled), may be null
     int* cull_counts;        // [N] optional exact-culling record counts (16 x 16 tiles only), may be null
+    int depth_key_shift;     // depth key = float bits >> shift (0: exact order; 8: 24-bit keys, fast forms)
 };
 // cam_dev (optional): device camera read instead of `cam` (batched form).
 // bf16_sh: precision-form parameter layout (10 fp32 rows + 48 bf16 SH rows).

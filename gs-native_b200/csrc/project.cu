@@ -272,7 +272,7 @@ __global__ void __launch_bounds__(256) project_kernel(const float* __restrict__ 
     if (rect.x >= rect.z || rect.y >= rect.w) return;
 
     out.depths[i] = z;
-    out.depth_keys[i] = __float_as_uint(z);
+    out.depth_keys[i] = __float_as_uint(z) >> out.depth_key_shift;  // z > 0: monotonic in z
     out.rects[i] = rect;
     out.tile_counts[i] = (rect.z - rect.x) * (rect.w - rect.y);
     if (out.radii) out.radii[i] = radius;

@@ -91,7 +91,7 @@ bool MultiViewRenderer::Prepare(View& v, const GaussianBuffers& g, const CameraP
     }
     if (!SortScratch(v.sort_scratch, v.sort_scratch_count, n)) return false;
     gsn::ProjectOutputs po{v.means.get(), v.conic.get(), v.colors.get(), v.depths.get(),
-                           v.rects.get(), v.tile_counts.get(), v.depth_keys[0].get(), nullptr, nullptr};
+                           v.rects.get(), v.tile_counts.get(), v.depth_keys[0].get(), nullptr, nullptr, 0};
     if (gsn::launch_project_tiled(g.gaussians_, n, v.cam, config_.tile_w, config_.tile_h, sh_degree, po, stream_) !=
         GSN_OK)
         return false;

@@ -115,7 +115,10 @@ bool Renderer::Render(const GaussianBuffers& gaussians, const CameraParams& came
     if (count > 0) {
         gsn::ProjectOutputs po{means_.get(), conic_opacities_.get(), colors_.get(), depths_.get(),
                                rects_.get(), tile_counts_.get(), depth_keys_[0].get(), radii_.get(),
-                               exact_culling_ ? cull_counts_.get() : nullptr};
+                               exact_culling_ ? cull_counts_.get() : nullptr,
+                               // the fast forms order depths on 24-bit keys (one radix pass less;
+                               // depths equal to 2^-16 relative may swap their blend order)
+                               fast_blend_ ? 8 : 0};
         gsn::stage_mark(s, gsn::kStageProject);
         if (gsn::launch_project(gaussians.gaussians_, count, cam, device_camera_, sh_degree, bf16_sh_, po, s) != GSN_OK) return false;
         gsn::stage_mark(s, gsn::kStageDepthSort);
@@ -126,8 +129,8 @@ bool Renderer::Render(const GaussianBuffers& gaussians, const CameraParams& came
         // visible ones (their order - depth, then id - is unchanged)
         int* visible = counters_.get() + 2;
         if (gsn::launch_radix_sort_dropping(depth_keys_[0].get(), depth_ids_[0].get(), depth_keys_[1].get(),
-                                            depth_ids_[1].get(), true, count, nullptr, 0, 32, scratch, &in_alt,
-                                            visible, s) != GSN_OK)
+                                            depth_ids_[1].get(), true, count, nullptr, 0, fast_blend_ ? 24 : 32,
+                                            scratch, &in_alt, visible, s) != GSN_OK)
             return false;
         const uint32_t* by_depth = depth_ids_[in_alt ? 1 : 0].get();
         gsn::stage_mark(s, gsn::kStageRecordScan);

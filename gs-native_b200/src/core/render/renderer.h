@@ -69,7 +69,8 @@ public:
     // terms hoisted and the hardware exp2 approximation, instead of the
     // reference's per-pixel expression and expf. Images move by a few ulps
     // (no longer bit-identical to the reference); the solver's backward
-    // follows the renderer's setting.
+    // follows the renderer's setting. The fast form also orders depths on
+    // 24-bit keys (three radix passes instead of four).
     void SetFastBlend(bool enabled) { fast_blend_ = enabled; }
     bool GetFastBlend() const { return fast_blend_; }
     bool GetExactCulling() const { return exact_culling_; }

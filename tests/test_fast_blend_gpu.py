@@ -1,15 +1,14 @@
 """Fast blend arithmetic (Renderer::SetFastBlend): the Gaussian power in Horner
-form with hoisted per-record terms and the hardware exp2 approximation. The
-image stays within float rounding of the reference arithmetic's, the backward
-follows the renderer's setting, and its gradients agree to the tolerance the
-solver's parity tests use for reordered float sums."""
+form with hoisted per-record terms, the hardware exp2 approximation and depth
+order on 24-bit keys. The image stays within float rounding of the reference
+arithmetic's except where near-equal depths swap, the backward follows the
+renderer's setting, and training matches."""
 import numpy as np
 import pytest
 
 import gsn
 import scenes
 from helpers import dev, empty, host, sync, torch
-from test_solver_gpu import rows_close
 
 pytestmark = pytest.mark.gpu
 
@@ -35,10 +34,14 @@ def test_fast_blend_matches_reference_arithmetic(culled):
     target = np.random.default_rng(3).integers(0, 256, size=(cam.height, cam.width, 3), dtype=np.uint8)
     exact_img, exact_g = _frame(False, params, cam, target)
     fast_img, fast_g = _frame(True, params, cam, target)
+    # the fast form also orders depths on 24-bit keys: Gaussians whose depths
+    # agree to 2^-16 relative may swap their blend order, which moves a few
+    # pixels by up to ~1e-2; everything else moves by float rounding
     diff = np.abs(fast_img - exact_img)
-    assert diff.max() < 1e-4 and diff.mean() < 1e-6
-    ok, where = rows_close(fast_g[:, :11].T, exact_g[:, :11].T, rel=1e-3, floor=1e-4)
-    assert ok, where
+    assert diff.mean() < 1e-5 and np.mean(diff > 1e-4) < 1e-3 and diff.max() < 5e-2
+    scale = np.abs(exact_g[:, :11]).max(axis=0, keepdims=True)
+    bad = np.abs(fast_g[:, :11] - exact_g[:, :11]) > 1e-3 * np.abs(exact_g[:, :11]) + 1e-4 * scale
+    assert bad.any(axis=1).mean() < 5e-3
 
 
 def test_training_with_fast_blend():
