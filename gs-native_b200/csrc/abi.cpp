@@ -502,6 +502,7 @@ int gsn_training_options_default(gsn_training_options* out) {
     out->sparse_adam = o.sparse_adam ? 1 : 0;
     out->spatial_order = o.spatial_order ? 1 : 0;
     out->fast_blend = o.fast_blend ? 1 : 0;
+    out->fp32_ssim = o.fp32_ssim ? 1 : 0;
     return GSN_OK;
 }
 
@@ -543,6 +544,7 @@ gs_native::TrainingOptions ToOptions(const gsn_training_options& in) {
     o.sparse_adam = in.sparse_adam != 0;
     o.spatial_order = in.spatial_order != 0;
     o.fast_blend = in.fast_blend != 0;
+    o.fp32_ssim = in.fp32_ssim != 0;
     return o;
 }
 }  // namespace

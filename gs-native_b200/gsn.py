@@ -445,7 +445,7 @@ class TrainingOptions(ctypes.Structure):
         ("precision", ctypes.c_int), ("graph", ctypes.c_int),
         ("learned_density", ctypes.c_int), ("learned_confidence", ctypes.c_float), ("log_density", ctypes.c_int),
         ("exact_culling", ctypes.c_int), ("sparse_adam", ctypes.c_int), ("spatial_order", ctypes.c_int),
-        ("fast_blend", ctypes.c_int),
+        ("fast_blend", ctypes.c_int), ("fp32_ssim", ctypes.c_int),
     ]
 
     @classmethod

@@ -94,6 +94,7 @@ bool GaussianSplatting::Initialize(const TrainingScene& scene, const TrainingOpt
     renderer_.SetFastBlend(options_.fast_blend);
     eval_renderer_.SetBf16Sh(options_.bf16_sh);
     solver_.SetBf16Sh(options_.bf16_sh);
+    if (options_.bf16_sh && options_.fp32_ssim) solver_.SetTensorCoreLoss(false);
     density_.SetBf16Sh(options_.bf16_sh);
     solver_.SetSparseAdam(options_.sparse_adam);
     spatial_.SetStream(stream_);

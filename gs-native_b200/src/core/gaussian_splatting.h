@@ -79,6 +79,7 @@ struct TrainingOptions {
     // (SpatialOrder): no value changes, the sparse update skips whole sectors
     bool spatial_order = false;
     bool fast_blend = false;  // training renderer's fast blend arithmetic (Renderer::SetFastBlend)
+    bool fp32_ssim = false;   // precision form keeps the fp32 CUDA-core SSIM gradient (not the tcgen05 one)
 };
 
 // Statistics, decisions and parent map of the last density-control step

@@ -330,6 +330,7 @@ typedef struct gsn_training_options {
     int sparse_adam;                 /* 1: visibility-masked Adam (gsn_solver_set_sparse_adam) */
     int spatial_order;               /* 1: Morton order of the Gaussians after init and every density step */
     int fast_blend;                  /* 1: fast blend arithmetic in the training renderer (gsn_renderer_set_fast_blend) */
+    int fp32_ssim;                   /* 1: the precision form keeps the fp32 SSIM gradient kernel */
 } gsn_training_options;
 
 int gsn_training_options_default(gsn_training_options* out);
