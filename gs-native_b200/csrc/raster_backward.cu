@@ -108,7 +108,9 @@ __global__ void __launch_bounds__(kRasterThreads, 12) raster_backward_kernel(Ras
                 s_conic[slot] = q;
                 const float* c = reinterpret_cast<const float*>(a.colors) + 3ull * id;
                 s_color[slot] = make_float3(__ldg(c), __ldg(c + 1), __ldg(c + 2));
-                s_box[slot] = alpha_box(mean, q);
+                // with the forward's take bits the box test is implied (a record
+                // some strip pixel took reaches that strip); without them it runs
+                if (!a.record_warps) s_box[slot] = alpha_box(mean, q);
                 s_floor[slot] = alpha_floor(q.w);
                 uint16_t flags = 0x0101;
                 if (a.record_warps) {
@@ -129,7 +131,8 @@ __global__ void __launch_bounds__(kRasterThreads, 12) raster_backward_kernel(Ras
             // records the forward pass took somewhere in this warp's strip (every
             // other record leaves the strip's pixels unchanged)
             uint32_t m = __ballot_sync(0xffffffffu, jl < batch && ((s_warps[jl] >> warp_shift) & 1u) &&
-                                                        box_hits(s_box[jl], g.sx0, g.sx1, g.sy0, g.sy1));
+                                                        (a.record_warps ||
+                                                         box_hits(s_box[jl], g.sx0, g.sx1, g.sy0, g.sy1)));
             while (m) {
                 if (__all_sync(0xffffffffu, done[0] && done[1] && done[2] && done[3])) break;
                 const int j = k * 32 + __ffs(m) - 1;
