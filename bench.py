@@ -68,6 +68,8 @@ NCU_TRAFFIC = {
               "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/gaussian_update_plain_1.2M.md"),
     "sparse": (604_525_312 + 483_656_704,
                "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/gaussian_update_sparse_1.2M.md"),
+    "sparse_bf16": (385_936_896 + 276_065_792,
+                    "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/gaussian_update_bf16_sparse_1.2M.md"),
 }
 
 
@@ -607,8 +609,8 @@ def run_gsn(args):
         top = max(hbm, key=hbm.get)
         achieved = ab[top] / (st[top] / 1000.0) / 1e9
         traffic = None
-        if top == "gaussian_update" and n == MODEL_GAUSSIANS and not bf16_f:
-            traffic = NCU_TRAFFIC["sparse" if sparse_f else "dense"]
+        if top == "gaussian_update" and n == MODEL_GAUSSIANS and (sparse_f or not bf16_f):
+            traffic = NCU_TRAFFIC[("sparse_bf16" if bf16_f else "sparse") if sparse_f else "dense"]
         return {"bound": "hbm", "kernel": top, "form": form, "achieved": round(achieved, 1), "peak": peak,
                 "unit": "GB/s", "frac": round(achieved / peak, 4), "algorithmic_bytes": int(ab[top]),
                 "traffic": traffic[0] if traffic else None, "traffic_source": traffic[1] if traffic else None,
