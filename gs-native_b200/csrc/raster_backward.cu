@@ -18,7 +18,7 @@
 //     in the forward pass (per-record strip flags the forward writes) and whose
 //     conservative alpha >= 1/255 box reaches the strip, powers below a
 //     record's alpha floor skip expf, and the three divisions by (1 - alpha)
-//     share one reciprocal;
+//     share one reciprocal (the hardware approximation in the fast form);
 //   * the colour term of dL/dalpha is carried per pixel as two scalars (the
 //     gradient-weighted final colour and the gradient-weighted colour in front
 //     of the record) instead of three channel sums;
@@ -174,7 +174,7 @@ __global__ void __launch_bounds__(kRasterThreads, 12) raster_backward_kernel(Ras
                         take = take && !stop;
                         has |= take;
                         float w = alpha * T[p];
-                        float inv = __frcp_rn(1.0f - alpha);
+                        float inv = one_over<kFast>(1.0f - alpha);
                         // dL/dalpha = (dL/dC . (colour in front + T c - final)) / (1 - alpha)
                         const float G = gI[p][0] * cc[0] + gI[p][1] * cc[1] + gI[p][2] * cc[2];
                         float dalpha = (P[p] + T[p] * G - S[p]) * inv;

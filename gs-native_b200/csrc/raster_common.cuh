@@ -106,6 +106,17 @@ __device__ __forceinline__ float gaussian_weight(float opacity, float power) {
     return kFast ? opacity * __expf(power) : opacity * expf(power);
 }
 
+// 1 / x for x in [0.01, 1] (one minus a clamped alpha): the correctly rounded
+// reciprocal in the exact form, the single hardware approximation (PTX
+// rcp.approx, within an ulp) in the fast form.
+template <bool kFast>
+__device__ __forceinline__ float one_over(float x) {
+    if (!kFast) return __frcp_rn(x);
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 // Does the box of a record overlap the pixel rectangle [x0, x1] x [y0, y1]?
 __device__ __forceinline__ bool box_hits(float4 b, float x0, float x1, float y0, float y1) {
     return b.x <= x1 && b.y >= x0 && b.z <= y1 && b.w >= y0;
