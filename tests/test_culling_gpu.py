@@ -116,7 +116,8 @@ def test_training_with_culling_matches_plain():
     assert a[1] == b[1] and abs(a[0] - b[0]) < 0.02
     # with density control, threshold decisions amplify that noise chaotically:
     # plain runs of this 10-view scene spread by up to ~0.3 dB from one process
-    # to the next, so only a loose bound is meaningful here
+    # to the next, and their Gaussian counts by about 1 %, so only loose bounds
+    # are meaningful here
     p, c = _train(0, 900, 700), _train(1, 900, 700)
     assert abs(c[0] - p[0]) < 0.35
-    assert abs(c[1] - p[1]) <= 0.01 * p[1]
+    assert abs(c[1] - p[1]) <= 0.03 * p[1]
