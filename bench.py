@@ -85,6 +85,8 @@ def parse():
                    help="warm-up steps plus one step on 3 views, no JSON (for ncu captures)")
     p.add_argument("--views", type=int, default=0, help="number of training views used (0 = all 180)")
     p.add_argument("--precision", action="store_true", help="with --profile-only: run the precision form")
+    p.add_argument("--fp32-ssim", action="store_true",
+                   help="with --profile-only --precision: the fp32 SSIM gradient instead of the tcgen05 one")
     p.add_argument("--culled", action="store_true", help="with --profile-only: exact tile culling on")
     p.add_argument("--sparse", action="store_true", help="with --profile-only: sparse Adam on the Morton-ordered model")
     p.add_argument("--multiview", action="store_true", help="with --profile-only: the 32-view multi-view render")
@@ -534,7 +536,7 @@ def run_gsn(args):
                 mv.render(p.data_ptr(), n, cams, [x.data_ptr() for x in imgs], [0, 0, 0], SH_DEGREE)
             torch.cuda.synchronize()
             return
-        f = Form(args.precision, args.culled, args.sparse)
+        f = Form(args.precision, args.culled, args.sparse, tc_loss=not args.fp32_ssim)
         for k in range(args.warmup + 1):
             step(f, k)
         torch.cuda.synchronize()
