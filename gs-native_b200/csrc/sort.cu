@@ -27,6 +27,7 @@ constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kSortItems = 8;                       // per thread
 constexpr int kSortChunk = kSortThreads * kSortItems;  // 2048 keys per block
 constexpr int kBins = 256;
+constexpr int kScanPer = 4;                          // per-block counts per thread in radix_scan
 constexpr uint32_t kSortSentinel = 0xFFFFFFFFu;  // the key a dropping sort leaves out
 
 // Device-resident counts are clamped to the host-side capacity the grid was sized
@@ -54,13 +55,17 @@ __global__ void __launch_bounds__(kSortThreads) radix_upsweep(const uint32_t* __
     const int warp = threadIdx.x >> 5;
     for (int i = threadIdx.x; i < kSortWarps * kBins; i += kSortThreads) (&hist[0][0])[i] = 0;
     __syncthreads();
-#pragma unroll 4
+    // the chunk's loads first, then the shared-memory counts
+    uint32_t key[kSortItems];
+#pragma unroll
     for (int k = 0; k < kSortItems; ++k) {
-        int64_t idx = start + k * kSortThreads + threadIdx.x;
-        if (idx < end) {
-            const uint32_t k = __ldg(keys + idx);
-            if (!kDrop || k != kSortSentinel) atomicAdd(&hist[warp][(k >> bit) & mask], 1u);
-        }
+        const int64_t idx = start + k * kSortThreads + threadIdx.x;
+        key[k] = idx < end ? __ldg(keys + idx) : kSortSentinel;
+    }
+#pragma unroll
+    for (int k = 0; k < kSortItems; ++k) {
+        const int64_t idx = start + k * kSortThreads + threadIdx.x;
+        if (idx < end && (!kDrop || key[k] != kSortSentinel)) atomicAdd(&hist[warp][(key[k] >> bit) & mask], 1u);
     }
     __syncthreads();
     const int d = threadIdx.x;
@@ -96,11 +101,19 @@ __global__ void __launch_bounds__(kSortThreads) radix_scan(const int* n_dev, int
     }
     __syncthreads();
     uint32_t* row = block_hist + d * hist_stride;
-    for (int base = 0; base < blocks; base += kSortThreads) {
-        int i = base + threadIdx.x;
-        uint32_t x = i < blocks ? row[i] : 0u;
-        // inclusive warp scan
-        uint32_t inc = x;
+    // kScanPer consecutive counts per thread: a quarter of the rounds (and of
+    // their barriers) of one count per thread
+    for (int base = 0; base < blocks; base += kSortThreads * kScanPer) {
+        const int i0 = base + threadIdx.x * kScanPer;
+        uint32_t x[kScanPer];
+        uint32_t sum = 0;
+#pragma unroll
+        for (int k = 0; k < kScanPer; ++k) {
+            x[k] = i0 + k < blocks ? row[i0 + k] : 0u;
+            sum += x[k];
+        }
+        // inclusive warp scan of the thread sums
+        uint32_t inc = sum;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
@@ -116,8 +129,13 @@ __global__ void __launch_bounds__(kSortThreads) radix_scan(const int* n_dev, int
             if (w < warp) warp_prefix += s;
             chunk_total += s;
         }
-        uint32_t c = carry;
-        if (i < blocks) row[i] = c + warp_prefix + inc - x;
+        const uint32_t c = carry;
+        uint32_t run = c + warp_prefix + inc - sum;
+#pragma unroll
+        for (int k = 0; k < kScanPer; ++k) {
+            if (i0 + k < blocks) row[i0 + k] = run;
+            run += x[k];
+        }
         __syncthreads();
         if (threadIdx.x == 0) carry = c + chunk_total;
     }
@@ -153,13 +171,19 @@ __global__ void __launch_bounds__(kSortThreads) radix_downsweep(
     const uint32_t lt = lanemask_lt();
     const int64_t slice = start + static_cast<int64_t>(warp) * (kSortItems * 32);
     uint32_t key[kSortItems], val[kSortItems], rank[kSortItems];
+    // all of the slice's loads first, so they are in flight together (the
+    // warp-synchronous ranking below would otherwise wait for each step's pair)
 #pragma unroll
     for (int s = 0; s < kSortItems; ++s) {
-        int64_t idx = slice + s * 32 + lane;
-        bool valid = idx < end;
+        const int64_t idx = slice + s * 32 + lane;
+        const bool valid = idx < end;
         key[s] = valid ? keys_in[idx] : 0u;
         if (kIdentityValues) val[s] = static_cast<uint32_t>(idx);
         else val[s] = valid ? values_in[idx] : 0u;
+    }
+#pragma unroll
+    for (int s = 0; s < kSortItems; ++s) {
+        bool valid = slice + s * 32 + lane < end;
         if (kDrop) valid = valid && key[s] != kSortSentinel;
         uint32_t digit = valid ? ((key[s] >> bit) & mask) : 0u;
         // lanes holding the same digit: intersect the eight per-bit ballots
@@ -370,6 +394,12 @@ __global__ void __launch_bounds__(256) emit_records(const uint32_t* __restrict__
     }
 }
 
+// Tile t's records are [offsets[t], offsets[t + 1]) of the tile-sorted keys. With
+// v(-1) = -1, v(r) = the tile of record r and v(n) = tile_count, position r in
+// [0, n] starts every tile in (v(r - 1), v(r)]. Each thread takes a run of
+// kRangeItems consecutive positions and issues the run's loads together.
+constexpr int kRangeItems = 8;
+
 __global__ void __launch_bounds__(256) tile_ranges(const uint32_t* __restrict__ tiles, const int* n_dev,
                                                    int max_records, int tile_count, int64_t* __restrict__ offsets) {
     const int n = min(*n_dev, max_records);
@@ -379,12 +409,22 @@ __global__ void __launch_bounds__(256) tile_ranges(const uint32_t* __restrict__ 
         for (int64_t i = first; i <= tile_count; i += stride) offsets[i] = 0;
         return;
     }
-    for (int64_t r = first; r < n; r += stride) {
-        int t = static_cast<int>(tiles[r]);
-        int prev = r == 0 ? -1 : static_cast<int>(tiles[r - 1]);
-        for (int e = prev + 1; e <= t; ++e) offsets[e] = r;
-        if (r == n - 1)
-            for (int e = t + 1; e <= tile_count; ++e) offsets[e] = n;
+    const int64_t positions = static_cast<int64_t>(n) + 1;
+    for (int64_t r0 = first * kRangeItems; r0 < positions; r0 += stride * kRangeItems) {
+        int v[kRangeItems + 1];
+#pragma unroll
+        for (int k = 0; k <= kRangeItems; ++k) {
+            const int64_t r = r0 - 1 + k;
+            // keys are tile ids below tile_count; the clamp keeps every write in range
+            v[k] = r < 0 ? -1 : r < n ? static_cast<int>(min(__ldg(tiles + r), static_cast<uint32_t>(tile_count)))
+                                      : tile_count;
+        }
+#pragma unroll
+        for (int k = 1; k <= kRangeItems; ++k) {
+            const int64_t r = r0 - 1 + k;
+            if (r >= positions) break;
+            for (int e = v[k - 1] + 1; e <= v[k]; ++e) offsets[e] = r;
+        }
     }
 }
 
@@ -538,8 +578,9 @@ int launch_emit_records(const uint32_t* sorted_ids, const int* record_start, con
 
 int launch_tile_ranges(const uint32_t* sorted_tiles, const int* record_count_device, int max_records,
                        int tile_count, int64_t* offsets, cudaStream_t stream) {
-    int64_t work = max_records > tile_count + 1 ? max_records : tile_count + 1;
-    int blocks = ceil_div(work, 256);
+    const int64_t runs = ceil_div(static_cast<int64_t>(max_records) + 1, kRangeItems);
+    int64_t work = runs > tile_count + 1 ? runs : tile_count + 1;
+    int blocks = static_cast<int>(ceil_div(work, 256));
     if (blocks > 148 * 32) blocks = 148 * 32;
     tile_ranges<<<blocks, 256, 0, stream>>>(sorted_tiles, record_count_device, max_records, tile_count,
                                            offsets);
