@@ -19,11 +19,17 @@
 //     conservative alpha >= 1/255 box reaches the strip, powers below a
 //     record's alpha floor skip expf, and the three divisions by (1 - alpha)
 //     share one reciprocal (the hardware approximation in the fast form);
+//   * the 12 per-Gaussian sums of a batch are flushed with 16-byte vector
+//     reductions (three per Gaussian) when grad_out is 16-byte aligned;
 //   * the colour term of dL/dalpha is carried per pixel as two scalars (the
 //     gradient-weighted final colour and the gradient-weighted colour in front
-//     of the record) instead of three channel sums;
-//   * 80 registers (12 CTAs, 24 warps per SM): measured 0.81 ms against 0.88 ms
-//     at the unconstrained 122 registers; 72 and 64 registers spill and lose.
+//     of the record) instead of three channel sums; the fast form carries their
+//     difference as one value;
+//   * d(cov a) and d(cov c) are accumulated without the power's factor 1/2,
+//     which is applied once per record before the warp reduction;
+//   * at most 80 registers (12 CTAs, 24 warps per SM): measured 0.81 ms against
+//     0.88 ms at the unconstrained 122 registers (the exact form uses 80, the
+//     fast form 69).
 // Per-Gaussian output (12 floats, Gaussian-major): d(u, v), d(cov a, b, c),
 // d(opacity logit), d(r, g, b), sum|du|, sum|dv|, 0.
 #include "raster_common.cuh"
@@ -37,6 +43,14 @@ constexpr int kVals = 12;
 
 __device__ __forceinline__ float sel(bool c, float a, float b) { return c ? a : b; }
 
+// Element-wise atomic add of four floats at a 16-byte aligned global address
+// (PTX red.global.add with a .v4.f32 vector, sm_90 and later).
+__device__ __forceinline__ void red_add_v4(float* address, float4 v) {
+    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(address), "f"(v.x), "f"(v.y), "f"(v.z),
+                 "f"(v.w)
+                 : "memory");
+}
+
 template <bool kFast>
 __global__ void __launch_bounds__(kRasterThreads, 12) raster_backward_kernel(RasterBackwardArgs a) {
     __shared__ uint32_t s_id[kRasterBatch];
@@ -46,7 +60,7 @@ __global__ void __launch_bounds__(kRasterThreads, 12) raster_backward_kernel(Ras
     __shared__ float4 s_box[kRasterBatch];
     __shared__ float s_floor[kRasterBatch];
     __shared__ uint16_t s_warps[kRasterBatch];
-    __shared__ float s_acc[kRasterBatch * kVals];
+    __shared__ __align__(16) float s_acc[kRasterBatch * kVals];
     __shared__ int s_bound;
 
     const int t = threadIdx.x;
@@ -84,6 +98,8 @@ __global__ void __launch_bounds__(kRasterThreads, 12) raster_backward_kernel(Ras
         }
         done[p] = limit[p] == 0;
         my_bound = max(my_bound, limit[p]);
+        // the fast form carries P - S in P (one add less per pixel and record)
+        if (kFast) P[p] = -S[p];
     }
     if (t == 0) s_bound = 0;
     __syncthreads();
@@ -177,26 +193,30 @@ __global__ void __launch_bounds__(kRasterThreads, 12) raster_backward_kernel(Ras
                         float inv = one_over<kFast>(1.0f - alpha);
                         // dL/dalpha = (dL/dC . (colour in front + T c - final)) / (1 - alpha)
                         const float G = gI[p][0] * cc[0] + gI[p][1] * cc[1] + gI[p][2] * cc[2];
-                        float dalpha = (P[p] + T[p] * G - S[p]) * inv;
+                        float dalpha = (kFast ? fmaf(T[p], G, P[p]) : P[p] + T[p] * G - S[p]) * inv;
                         const float wt = take ? w : 0.0f;
 #pragma unroll
                         for (int c = 0; c < 3; ++c) v[6 + c] += wt * gI[p][c];
                         float common = (take && raw < kAlphaMax) ? dalpha * raw : 0.0f;
                         float qx = q.x * dx + q.y * dy;
                         float qy = q.y * dx + q.z * dy;
-                        v[0] += -common * qx;
-                        v[1] += -common * qy;
-                        v[2] += 0.5f * common * qx * qx;
-                        v[3] += common * qx * qy;
-                        v[4] += 0.5f * common * qy * qy;
+                        const float cqx = common * qx, cqy = common * qy;
+                        v[0] -= cqx;
+                        v[1] -= cqy;
+                        v[2] += cqx * qx;  // halved once per record below
+                        v[3] += cqx * qy;
+                        v[4] += cqy * qy;  // halved once per record below
                         v[5] += common * (1.0f - q.w);
-                        v[9] += fabsf(common * qx);
-                        v[10] += fabsf(common * qy);
+                        v[9] += fabsf(cqx);
+                        v[10] += fabsf(cqy);
                         P[p] += wt * G;
                         T[p] = take ? nextT : T[p];
                     }
                 }
                 if (__any_sync(0xffffffffu, has)) {
+                    // d(cov a) and d(cov c) carry the factor 1/2 of the power (exact)
+                    v[2] *= 0.5f;
+                    v[4] *= 0.5f;
                     // butterfly reduce-scatter of the 12 slots (slot 11 is padding)
                     const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4, b1 = lane & 2;
                     float k6[6];
@@ -229,9 +249,20 @@ __global__ void __launch_bounds__(kRasterThreads, 12) raster_backward_kernel(Ras
             }
         }
         __syncthreads();
-        for (int k = t; k < batch * kVals; k += kRasterThreads) {
-            float val = s_acc[k];
-            if (val != 0.0f) atomicAdd(a.grad_out + static_cast<int64_t>(s_id[k / kVals]) * kVals + k % kVals, val);
+        if ((reinterpret_cast<uintptr_t>(a.grad_out) & 15) == 0) {
+            // one 16-byte vector reduction per group of four values (a Gaussian's 12
+            // floats are a 48-byte row of the 16-byte aligned grad_out)
+            for (int k = t; k < batch * (kVals / 4); k += kRasterThreads) {
+                const float4 val = reinterpret_cast<const float4*>(s_acc)[k];
+                if (val.x != 0.0f || val.y != 0.0f || val.z != 0.0f || val.w != 0.0f)
+                    red_add_v4(a.grad_out + static_cast<int64_t>(s_id[k / (kVals / 4)]) * kVals + 4 * (k % (kVals / 4)),
+                               val);
+            }
+        } else {
+            for (int k = t; k < batch * kVals; k += kRasterThreads) {
+                float val = s_acc[k];
+                if (val != 0.0f) atomicAdd(a.grad_out + static_cast<int64_t>(s_id[k / kVals]) * kVals + k % kVals, val);
+            }
         }
         __syncthreads();
     }
