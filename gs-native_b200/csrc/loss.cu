@@ -76,13 +76,28 @@ __global__ void __launch_bounds__(kThreads, 3) loss_gradient_kernel(const float*
     const int ch = blockIdx.z;
     const int ox = blockIdx.x * kT, oy = blockIdx.y * kT;
 
-    // raw inputs with a zero-padded halo
-    for (int j = t; j < kRaw; j += kThreads) {
-        int hx = ox + j % kIn - 10, hy = oy + j / kIn - 10;
-        bool ok = hx >= 0 && hy >= 0 && hx < width && hy < height;
-        int64_t k = (static_cast<int64_t>(hy) * width + hx) * 3 + ch;
-        raw_i[j] = ok ? image[k] : 0.0f;
-        raw_t[j] = ok ? target[k] * (1.0f / 255.0f) : 0.0f;
+    // raw inputs with a zero-padded halo: all of a thread's loads are issued
+    // before the first shared-memory store, so they are in flight together
+    {
+        constexpr int kRawPer = (kRaw + kThreads - 1) / kThreads;
+        float ri[kRawPer], rt[kRawPer];
+#pragma unroll
+        for (int u = 0; u < kRawPer; ++u) {
+            const int j = t + u * kThreads;
+            const int hx = ox + j % kIn - 10, hy = oy + j / kIn - 10;
+            const bool ok = j < kRaw && hx >= 0 && hy >= 0 && hx < width && hy < height;
+            const int64_t k = (static_cast<int64_t>(hy) * width + hx) * 3 + ch;
+            ri[u] = ok ? image[k] : 0.0f;
+            rt[u] = ok ? target[k] * (1.0f / 255.0f) : 0.0f;
+        }
+#pragma unroll
+        for (int u = 0; u < kRawPer; ++u) {
+            const int j = t + u * kThreads;
+            if (j < kRaw) {
+                raw_i[j] = ri[u];
+                raw_t[j] = rt[u];
+            }
+        }
     }
     __syncthreads();
 

@@ -140,20 +140,21 @@ __global__ void __launch_bounds__(256) emit_records_culled(const uint32_t* __res
     const int sub = static_cast<int>(gidx & 3);
     bool active = p < n;
     int begin = 0, count = 0;
+    uint32_t id = 0;
     if (active) {
+        // the id is loaded with the offsets, ahead of the count checks
         begin = record_start[p];
         count = record_start[p + 1] - begin;
+        id = sorted_ids[p];
         active = count > 0;
         if (active && begin + static_cast<int64_t>(count) > capacity) {
             if (sub == 0 && overflow) atomicExch(overflow, 1);
             active = false;
         }
     }
-    uint32_t id = 0;
     int4 r = make_int4(0, 0, 0, 0);
     CullShape s{};
     if (active) {
-        id = sorted_ids[p];
         r = rects[id];
         s = cull_shape(means[id], conic_opacity[id]);
     }
