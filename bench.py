@@ -59,8 +59,6 @@ UNIT = "iters/sec"
 SH_DEGREE = 3
 TARGET_GAUSSIANS = 1_500_000
 MODEL_GAUSSIANS = 1_200_000
-# DRAM bytes (read + write) of one gaussian_update launch on this workload, from
-# the ncu capture summarised in profiles/gaussian_update_plain_1.2M.md.
 # DRAM bytes (read + write) of one gaussian_update launch on this workload, per
 # update form, from the ncu captures summarised in profiles/.
 NCU_TRAFFIC = {
@@ -160,8 +158,8 @@ class ClockSampler:
 
 def algorithmic_bytes(n, records, tiles, pixels, s=16, tile_passes=2, visible=None, culled=False, sparse=False,
                       bf16=False):
-    """Compulsory HBM bytes per launch of each stage (formulas in DESIGN.md) for
-    a form: culled records are emitted with their conic (36 B per visible
+    """Compulsory HBM bytes per launch of each stage for a form (N Gaussians, V
+    visible, R records, T tiles, P pixels): culled records are emitted with their conic (36 B per visible
     Gaussian), the sparse update moves only visible Gaussians' rows, the
     precision layout stores the 48 SH rows in 2 bytes."""
     vis = n if visible is None else visible
