@@ -5,7 +5,13 @@
 //
 //   gsn_train --scene DIR --output DIR [--downscale 1] [--iterations 30000]
 //             [--precision] [--graph] [--max_gaussians 0]
+//             [--culled] [--sparse] [--fast] [--fp32_ssim]
 //             [--checkpoint PATH] [--resume PATH]
+//
+// --culled: exact tile culling; --sparse: visibility-masked Adam on the
+// Morton-ordered model; --fast: the fast blend arithmetic; --fp32_ssim: with
+// --precision, the fp32 SSIM gradient instead of the tcgen05 one. All four with
+// --precision and --graph give the fastest form.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -36,6 +42,10 @@ int main(int argc, char** argv) {
                                {"precision", "false"},
                                {"graph", "false"},
                                {"max_gaussians", "0"},
+                               {"culled", "false"},
+                               {"sparse", "false"},
+                               {"fast", "false"},
+                               {"fp32_ssim", "false"},
                                {"checkpoint", "none"},
                                {"resume", "none"}});
     if (args.help()) {
@@ -72,6 +82,10 @@ int main(int argc, char** argv) {
     options.bf16_sh = args.flag("precision");
     options.graph = args.flag("graph");
     options.max_gaussians = std::max(0, args.integer("max_gaussians"));
+    options.exact_culling = args.flag("culled");
+    options.sparse_adam = options.spatial_order = args.flag("sparse");
+    options.fast_blend = args.flag("fast");
+    options.fp32_ssim = args.flag("fp32_ssim");
     gs_native::GaussianSplatting gs;
     if (!gs.Initialize(scene, options)) {
         std::cerr << "Initialization failed.\n";
