@@ -312,6 +312,24 @@ def run_reference(args):
     }), flush=True)
 
 
+def reduce_max_over_ranks(dist, value, device):
+    """The largest of every rank's value (each rank's device time of the same
+    timed region, so the job is timed by its slowest rank); the value itself
+    without a process group."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(world, steps_per_rank, ms):
+    """Whole-job iterations per second: every rank runs its own steps (replicas,
+    weak scaling) and the job takes the slowest rank's `ms`."""
+    return world * steps_per_rank / (ms / 1000.0)
+
+
 def run_gsn(args):
     import torch
     import gsn
@@ -441,11 +459,7 @@ def run_gsn(args):
             dist.barrier()
 
     def max_over_ranks(ms):
-        if dist is not None:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
+        return reduce_max_over_ranks(dist, ms, "cuda")
 
     def timed(run, steps):
         barrier()
@@ -512,7 +526,7 @@ def run_gsn(args):
         status = status or graph.check()
         per_step = graph.launches_per_step()
         graph.close()
-        rate = lambda t: world * args.steps / (t / 1000.0)  # noqa: E731
+        rate = lambda t: job_rate(world, args.steps, t)  # noqa: E731
         eager = {"value": round(rate(ms), 3), "ms_per_step": round(ms / args.steps, 4), "e2e": round(rate(ms_e2e), 3),
                  "gpu_launches": int(launches), "psnr_db_last_step": round(float(loss_host[3]), 3)}
         graphed = {"value": round(rate(ms_graph), 3), "ms_per_step": round(ms_graph / args.steps, 4),
