@@ -45,3 +45,16 @@ def test_invalid_arguments_fail_without_touching_the_gpu():
     assert L.gsn_renderer_create(None) != 0
     assert L.gsn_solver_create(None) != 0
     assert L.gsn_sort_pairs_workspace(-1, None) != 0
+    # the allocation-free sort checks its arguments and its fixed capacity
+    # (16,777,216 pairs) before any device work
+    fn = L.gsn_sort_pairs_noalloc
+    fn.argtypes = [ctypes.c_void_p] * 4 + [ctypes.c_int] * 3 + [ctypes.POINTER(ctypes.c_int), ctypes.c_void_p]
+    fn.restype = ctypes.c_int
+    flag = ctypes.c_int(7)
+    assert fn(None, None, None, None, (1 << 24) + 1, 0, 32, ctypes.byref(flag), None) == -4  # GSN_ERR_CAPACITY
+    assert flag.value == 0
+    assert fn(None, None, None, None, 5, 0, 33, ctypes.byref(flag), None) == -1  # end bit past 32
+    assert fn(None, None, None, None, 5, 8, 4, ctypes.byref(flag), None) == -1  # end before begin
+    assert fn(None, None, None, None, 5, 0, 32, None, None) == -1  # no result flag
+    assert fn(None, None, None, None, 5, 0, 32, ctypes.byref(flag), None) == -1  # no buffers
+    assert fn(None, None, None, None, 0, 0, 32, ctypes.byref(flag), None) == 0  # nothing to sort
