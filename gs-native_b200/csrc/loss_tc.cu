@@ -24,6 +24,8 @@
 // loss.cu.
 #include <cuda_bf16.h>
 
+#include <mutex>
+
 #include "common.cuh"
 #include "kernels.h"
 #include "tcgen05.cuh"
@@ -414,19 +416,27 @@ int launch_loss_gradient_tc(const float* image, const uint8_t* target, const Ste
                             int height, double* sums, int* status, cudaStream_t stream) {
     if (width <= 0 || height <= 0 || !status) return GSN_ERR_INVALID_ARGUMENT;
     if (sums && cudaMemsetAsync(sums, 0, 3 * sizeof(double), stream) != cudaSuccess) return GSN_ERR_CUDA;
+    // per-device launch set-up, once per device; host threads calling on the
+    // same device serialise on the lock
+    static std::mutex mutex;
     static bool configured[64] = {};
     static int sm_count[64] = {};
     int device = 0;
     if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= 64) return GSN_ERR_CUDA;
-    if (!configured[device]) {
-        if (cudaFuncSetAttribute(loss_gradient_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(kSmemBytes)) != cudaSuccess ||
-            cudaDeviceGetAttribute(&sm_count[device], cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
-            return GSN_ERR_CUDA;
-        configured[device] = true;
+    int sms = 0;
+    {
+        std::lock_guard<std::mutex> lock(mutex);
+        if (!configured[device]) {
+            if (cudaFuncSetAttribute(loss_gradient_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(kSmemBytes)) != cudaSuccess ||
+                cudaDeviceGetAttribute(&sm_count[device], cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+                return GSN_ERR_CUDA;
+            configured[device] = true;
+        }
+        sms = sm_count[device];
     }
     const int items = ((width + kOutCols - 1) / kOutCols) * ((height + kOutRows - 1) / kOutRows) * 3;
-    const int grid = items < sm_count[device] ? items : sm_count[device];
+    const int grid = items < sms ? items : sms;
     loss_gradient_tc_kernel<<<grid, kThreads, kSmemBytes, stream>>>(image, target, frame, grad, width, height, sums,
                                                                status);
     return launched(1);

@@ -431,9 +431,17 @@ __global__ void __launch_bounds__(256) tile_ranges(const uint32_t* __restrict__ 
 }  // namespace
 
 // ---------------------------------------------------------------- host side
+// Words of the sort scratch for max_count pairs: four passes' digit totals,
+// then one 256-bin histogram per 2048-key block (the byte size adds 256 bytes
+// of alignment slack).
+constexpr size_t radix_sort_scratch_words(int max_count) {
+    return static_cast<size_t>(kBins) * ((static_cast<size_t>(max_count > 0 ? max_count : 1) + kSortChunk - 1) /
+                                         kSortChunk) +
+           kBins * 4;
+}
+
 size_t radix_sort_scratch_bytes(int max_count) {
-    size_t blocks = static_cast<size_t>(ceil_div(max_count > 0 ? max_count : 1, kSortChunk));
-    return (static_cast<size_t>(kBins) * blocks + kBins * 4) * sizeof(uint32_t) + 256;
+    return radix_sort_scratch_words(max_count) * sizeof(uint32_t) + 256;
 }
 
 RadixSortScratch radix_sort_scratch(void* base, int max_count) {
@@ -517,11 +525,16 @@ int launch_radix_sort_dropping(uint32_t* keys, uint32_t* values, uint32_t* keys_
 // of the sort for up to kNoAllocMaxCount pairs, in a file-scope device array
 // (8.4 MB on every GPU that loads the library, held until exit). Host code
 // cannot use the array's name as a device address, so its address is looked up
-// once per device with cudaGetSymbolAddress.
+// once per device with cudaGetSymbolAddress and cached; the cached address is
+// that of the module loaded in the device's current context, so it does not
+// survive cudaDeviceReset (the library's other entry points do not either: a
+// reset frees every buffer they hold).
 constexpr int kNoAllocMaxCount = 1 << 24;
-constexpr size_t kNoAllocScratchWords =
-    static_cast<size_t>(kBins) * (kNoAllocMaxCount / kSortChunk) + kBins * 4 + 64;
+constexpr size_t kNoAllocScratchWords = radix_sort_scratch_words(kNoAllocMaxCount);
 static __device__ __align__(256) uint32_t g_noalloc_sort_scratch[kNoAllocScratchWords];
+// the array is 256-byte aligned, so it needs the layout's words without the slack
+static_assert(sizeof(g_noalloc_sort_scratch) >= radix_sort_scratch_words(kNoAllocMaxCount) * sizeof(uint32_t),
+              "the no-alloc scratch array must hold the sort layout for its maximum count");
 
 int noalloc_sort_max_count() { return kNoAllocMaxCount; }
 

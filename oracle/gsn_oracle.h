@@ -12,7 +12,8 @@
  * reference's own tests (renderer_test.cu, solver_test.cu, density_test.cu,
  * knn_test.cu) by tests/test_oracle_*.py, against FP64 central finite
  * differences of its own forward model, and against the reference's CUDA
- * kernels run on the GPU (tests/golden fixtures).
+ * kernels (compiled unmodified into _ref/libgsref.so) run on the GPU by the
+ * -m gpu tests on identical inputs.
  */
 #ifndef GSN_ORACLE_H
 #define GSN_ORACLE_H

@@ -263,6 +263,31 @@ def knn3(points):
     return d, nb
 
 
+def initial_parameters(points, colors, mean_dist2, initial_opacity=0.1):
+    """The 58 x n parameter block GaussianSplatting::InitializeGaussians packs
+    from a point cloud (gaussian_splatting.cpp:96-113), in float32 as the
+    reference computes it: position rows 0-2 = the point; log-scale rows 3-5 =
+    0.5 * log(max(mean_dist2, 1e-7)); axis-angle rows 6-8 = 0; opacity logit
+    row 9 = log(0.1 / 0.9); SH DC rows 10, 26, 42 = (colour - 0.5) / C0 with
+    C0 = 0.28209479177387814; every other SH row 0. mean_dist2 is the 3-NN mean
+    squared distance of ComputeMeanDist2Cuda (knn.cu:180-255)."""
+    pts = np.asarray(points, dtype=np.float32)
+    col = np.asarray(colors, dtype=np.float32)
+    d = np.asarray(mean_dist2, dtype=np.float32)
+    n = pts.shape[0]
+    out = np.zeros((58, n), dtype=np.float32)
+    f32 = np.float32
+    scale = (f32(0.5) * np.log(np.maximum(d, f32(1e-7)))).astype(np.float32)
+    o = f32(initial_opacity)
+    logit = np.log(o / (f32(1) - o)).astype(np.float32)
+    for a in range(3):
+        out[a] = pts[:, a]
+        out[3 + a] = scale
+        out[10 + 16 * a] = (col[:, a] - f32(0.5)) / f32(0.28209479177387814)
+    out[9] = logit
+    return out
+
+
 def set_threads(k):
     return oracle().orc_set_threads(int(k))
 

@@ -5,7 +5,7 @@ import pytest
 import gsn
 import oracle
 import scenes
-from helpers import dev, empty, sync, torch
+from helpers import dev, empty, host, sync, torch
 
 pytestmark = pytest.mark.gpu
 
@@ -138,3 +138,34 @@ def test_checkpoint_resumes_training(tmp_path):
     c = gsn.Trainer()
     assert c.initialize(cams, images, points, colors, opts_p) == 0
     assert c.load_checkpoint(ck) != 0
+
+
+def test_initialization_packs_points_as_the_reference():
+    """InitializeGaussians (gaussian_splatting.cpp:96-113): the trainer's
+    initial 58 x n block against the oracle's float32 restatement, given the
+    3-NN mean squared distances; positions, colours (DC rows), the zero rows and
+    the opacity logit bit-exact, the log-scales within an ulp of float32 log."""
+    rng = np.random.default_rng(5)
+    n = 777
+    points = rng.normal(0.0, 2.0, size=(n, 3)).astype(np.float32)
+    points[5] = points[4]            # a duplicate: its nearest distance is 0
+    colors = rng.uniform(0.0, 1.0, size=(n, 3)).astype(np.float32)
+    cam = scenes.make_camera(64, 48)
+    image = np.full((48, 64, 3), 128, dtype=np.uint8)
+    tr = gsn.Trainer()
+    assert tr.initialize([cam], [image], points, colors) == 0
+    st = tr.state()
+    assert st["count"] == n
+    got = host(st["params"], np.float32, 58 * n).reshape(58, n)
+    d, _ = gsn.knn3_host(points)
+    # the trainer's 3-NN distances are the exhaustive search's (knn_test.cu:23-32 bound)
+    d64, _ = oracle.knn3(points)
+    assert np.all(np.abs(d.astype(np.float64) - d64) <= 2e-6 * np.maximum(1.0, d64))
+    want = oracle.initial_parameters(points, colors, d)
+    exact = [r for r in range(58) if r not in (3, 4, 5)]
+    assert np.array_equal(got[exact], want[exact])
+    assert np.all(got[6:9] == 0) and np.all(got[11:26] == 0)
+    assert np.all(got[9] == np.float32(np.log(np.float32(0.1) / np.float32(0.9))))
+    ulp = np.spacing(np.abs(want[3:6]))
+    assert np.all(np.abs(got[3:6] - want[3:6]) <= ulp)
+    assert np.all(got[3] == got[4]) and np.all(got[4] == got[5])
