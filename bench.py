@@ -36,9 +36,14 @@ Printed JSON line: `value` is iterations/s with targets resident in HBM,
 host memory - the next step's upload overlapping the current step on a copy
 stream - and copies its loss back to pinned memory, which the host reads two
 steps later), plus per-stage device times, the roofline of the dominant
-kernel, SM clocks sampled during the timed region and the FP64 CPU oracle
-timed on the host cores (`cpu_baseline`). `--impl reference` times only the CPU
-implementation of the path (the oracle restatement of the reference's code).
+kernel and SM clocks sampled during the timed region. After the timed regions:
+`reference_cuda`, the reference's own CUDA build (compiled unmodified) running
+the steady-state loop of its trainer on the same workload; `psnr_gate`,
+held-out PSNR of plain and chosen training runs on a reduced schedule (the
+metric's 0.1 dB condition); and `cpu_baseline`, one full CPU training step
+timed on the host cores (the reference's own test/cpu_reference.h forward and
+loss, the FP64 oracle port for the gradients and Adam). `--impl reference`
+times only that CPU implementation of the path.
 """
 import argparse
 import json
@@ -56,6 +61,8 @@ sys.path[:0] = [os.path.join(ROOT, "gs-native_b200")]
 
 METRIC = "iters/sec @1.2M Gaussians 1600×1064: chosen form vs plain FP32, ΔPSNR≤0.1 dB"
 UNIT = "iters/sec"
+WORKLOAD = ("training step (render, L1+SSIM gradient, backward, Adam) at the 1.2M-Gaussian cap, 1600x1064, "
+            "SH degree 3, one ring view per step")
 SH_DEGREE = 3
 TARGET_GAUSSIANS = 1_500_000
 MODEL_GAUSSIANS = 1_200_000
@@ -89,6 +96,10 @@ def parse():
     p.add_argument("--sparse", action="store_true", help="with --profile-only: sparse Adam on the Morton-ordered model")
     p.add_argument("--multiview", action="store_true", help="with --profile-only: the 32-view multi-view render")
     p.add_argument("--no-multiview", action="store_true", help="skip the 32-view multi-view measurement")
+    p.add_argument("--no-reference-cuda", action="store_true", help="skip the reference CUDA build's leg")
+    p.add_argument("--no-psnr-gate", action="store_true", help="skip the held-out PSNR gate runs")
+    p.add_argument("--gate-iterations", type=int, default=6000,
+                   help="iterations of each held-out PSNR gate run (reduced schedule)")
     return p.parse_args()
 
 
@@ -190,48 +201,129 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
-def cpu_baseline(model, cam, target_u8, extent, steps=1, threads=None):
-    """FP64 oracle (the CPU restatement of the reference's path) on a bounded
-    sample: per-Gaussian stages on all Gaussians, per-tile stages on one band of
-    tile rows, scaled to a full step by the band fraction."""
+def cpu_step(oracle, params64, m, v, cam, target_u8, lr, step, use_reference):
+    """One full CPU training step on the whole frame (no sampling), legs timed:
+    the forward render and the loss value by the reference's own CPU reference
+    (test/cpu_reference.h RenderReference + ComputeLoss, single-threaded as
+    written) when `use_reference`, else by the FP64 oracle; projection, tile
+    lists, loss gradient, backward, chain rule and Adam by the FP64 oracle port
+    on its OpenMP threads (the reference has no CPU backward)."""
+    legs = {}
+    t = time.perf_counter()
+    p32 = params64.astype(np.float32)
+    proj = oracle.project(p32, cam, SH_DEGREE)
+    offsets, ids = oracle.tile_lists(proj, cam)
+    legs["project_and_lists"] = time.perf_counter() - t
+    t = time.perf_counter()
+    if use_reference:
+        image = oracle.ref_cpu_render(p32, cam, [0, 0, 0], SH_DEGREE)
+        loss = oracle.ref_cpu_loss(image, target_u8)
+    else:
+        image, _, _ = oracle.render(proj, cam, offsets, ids, [0, 0, 0])
+        loss = oracle.loss(image, target_u8)
+    legs["forward_and_loss"] = time.perf_counter() - t
+    t = time.perf_counter()
+    gI = oracle.loss_gradient(image, target_u8)
+    g9, _ = oracle.backward(proj, cam, offsets, ids, image, gI)
+    g58 = oracle.map_gradients(p32, cam, SH_DEGREE, g9)
+    oracle.adam(params64, m, v, g58, lr, step)
+    legs["gradients_and_adam"] = time.perf_counter() - t
+    return legs, loss
+
+
+def cpu_baseline(model, cam, target_u8, extent, steps=1, budget_s=None, threads=None):
+    """Full training steps on the CPU (see cpu_step) over the whole frame:
+    `steps` of them, or as many as fit in `budget_s` seconds (at least one).
+    Returns the rate, the steps actually run and the per-leg seconds."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     cores = threads or len(os.sched_getaffinity(0))
     oracle.set_threads(cores)
+    use_reference = oracle.ref_cpu_available()
     n = model.shape[1]
-    tiles_x, tiles_y = cam.tile_count_x, cam.tile_count_y
-    band_row = tiles_y // 2
-    t0, t1 = band_row * tiles_x, (band_row + 1) * tiles_x
-    rows = (band_row * 16, min(cam.height, (band_row + 1) * 16))
-    frac = (t1 - t0) / (tiles_x * tiles_y)
     params64 = model.astype(np.float64)
     m = np.zeros_like(params64)
     v = np.zeros_like(params64)
     lr = dict(oracle.REFERENCE_LR)
     lr["position"] = position_lr(15000, extent)
-    per_step = []
+    per_step, legs_all = [], []
+    t0 = time.perf_counter()
     for step in range(steps):
-        p32 = params64.astype(np.float32)
         a = time.perf_counter()
-        proj = oracle.project(p32, cam, SH_DEGREE)
-        offsets, ids = oracle.tile_lists(proj, cam)
-        b = time.perf_counter()
-        image, _, _ = oracle.render(proj, cam, offsets, ids, [0, 0, 0], (t0, t1))
-        gI = oracle.loss_gradient(image, target_u8, rows)
-        g9, a2 = oracle.backward(proj, cam, offsets, ids, image, gI, (t0, t1))
-        c = time.perf_counter()
-        g58 = oracle.map_gradients(p32, cam, SH_DEGREE, g9)
-        oracle.adam(params64, m, v, g58, lr, step + 1)
-        d = time.perf_counter()
-        per_step.append((b - a) + (c - b) / frac + (d - c))
-        sampled = d - a
-    sec = float(np.median(per_step))
-    return {"value": 1.0 / sec, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": (f"FP64 oracle step on {n} Gaussians: projection, tile lists, chain rule and Adam on all "
-                       f"Gaussians; blend, loss gradient and backward on tile row {band_row} "
-                       f"({t1 - t0} of {tiles_x * tiles_y} tiles), scaled by {1 / frac:.1f}; "
-                       f"{steps} step(s), {sampled:.1f} s sampled CPU time per step"),
-            "seconds_per_step": sec}
+        legs, _ = cpu_step(oracle, params64, m, v, cam, target_u8, lr, step + 1, use_reference)
+        per_step.append(time.perf_counter() - a)
+        legs_all.append(legs)
+        if budget_s is not None and time.perf_counter() - t0 + per_step[-1] > budget_s:
+            break
+    total = sum(per_step)
+    run = len(per_step)
+    legs = {k: round(float(np.mean([l[k] for l in legs_all])), 3) for k in legs_all[0]}
+    fwd = ("RenderReference + ComputeLoss of the reference's test/cpu_reference.h (compiled unmodified "
+           "against an OpenCV shim), single-threaded as written" if use_reference else
+           "FP64 oracle render and loss (the reference's CPU reference was not built)")
+    return {"value": run / total, "unit": UNIT, "cores": cores, "kind": "reference" if use_reference else "port",
+            "sample": (f"{run} full training step(s) of the whole 1600x1064 frame on {n} Gaussians, no sampling "
+                       f"or scaling: forward and loss by {fwd}; projection, tile lists, loss gradient, backward, "
+                       f"chain rule and Adam by the FP64 oracle port on {cores} threads"),
+            "threads": {"forward_and_loss": 1 if use_reference else cores, "port": cores},
+            "legs_s": legs, "steps_run": run, "seconds": round(total, 2)}
+
+
+def measure_reference_cuda(gsn, torch, model, train, targets, lr, args):
+    """The reference's own CUDA build (renderer.cu + solver.cu compiled
+    unmodified for sm_100a into oracle/_ref/libgsref.so) on the same workload
+    as the forms: the steady-state loop of GaussianSplatting::Train (Render +
+    Iterate per step, no log line) from the same initial model and views, with
+    the targets resident in HBM (`value`) and uploaded from pageable host
+    memory with cudaMemcpy2D every step as Train does (`e2e`). Timed by CUDA
+    events around the loop inside the harness (no Python in the loop). This is
+    a baseline leg: it runs after, and outside, the timed regions of the
+    library's forms."""
+    import ctypes
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    if not oracle.ref_available():
+        return {"unavailable": "oracle/_ref/libgsref.so was not built (no reference tree where build() ran)"}
+    V, I, F, P = ctypes.c_void_p, ctypes.c_int, ctypes.c_float, ctypes.POINTER
+    r, s = V(), V()
+    oracle.ref_fn("ref_renderer_create", [P(V)])(ctypes.byref(r))
+    oracle.ref_fn("ref_solver_create", [P(V)])(ctypes.byref(s))
+    replay = oracle.ref_fn("ref_train_replay", [V, V, V, I, V, V, I, V, V, V, V, V, F, I, P(F)])
+    n = model.shape[1]
+    p = torch.from_numpy(np.ascontiguousarray(model)).cuda()
+    img = torch.empty((1064, 1600, 3), device="cuda")
+    tbuf = torch.empty((1064, 1600, 3), dtype=torch.uint8, device="cuda")
+    cams = (gsn.Camera * len(train))(*train)
+    bg = (ctypes.c_float * 3)(0, 0, 0)
+    warm = [k % len(train) for k in range(args.warmup)]
+    views = [(args.warmup + k) % len(train) for k in range(args.steps)]
+    # pageable host copies of the targets the timed steps use (the reference
+    # trainer keeps its images in cv::Mat host memory)
+    pageable = {v: np.ascontiguousarray(targets[v].cpu().numpy()) for v in set(views)}
+    hptr = (V * len(train))(*[pageable[v].ctypes.data if v in pageable else None for v in range(len(train))])
+
+    def run(vs, host):
+        arr = (I * len(vs))(*vs)
+        ms = F()
+        torch.cuda.synchronize()
+        st = replay(r, s, V(p.data_ptr()), n, cams, arr, len(vs), hptr if host else None,
+                    V(0) if host else V(targets.data_ptr()), V(tbuf.data_ptr()), bg, V(img.data_ptr()), lr,
+                    SH_DEGREE, ctypes.byref(ms))
+        torch.cuda.synchronize()
+        assert st == 0, f"reference replay failed ({st})"
+        return ms.value
+
+    run(warm, False)
+    ms = run(views, False)
+    ms_e2e = run(views, True)
+    oracle.ref_fn("ref_solver_destroy", [V])(s)
+    oracle.ref_fn("ref_renderer_destroy", [V])(r)
+    return {"value": round(args.steps / (ms / 1000.0), 3), "ms_per_step": round(ms / args.steps, 4),
+            "e2e": round(args.steps / (ms_e2e / 1000.0), 3), "e2e_ms_per_step": round(ms_e2e / args.steps, 4),
+            "steps": args.steps, "warmup": args.warmup,
+            "build": "renderer.cu + solver.cu compiled unmodified for sm_100a (oracle/_ref/libgsref.so)",
+            "loop": ("GaussianSplatting::Train steady state: Render + Solver::Iterate per step, same initial "
+                     "1.2M model, views and position learning rate as the forms; per-iteration log line off")}
 
 
 def measure_multiview(gsn, torch, model, stream, sp, args, world):
@@ -287,10 +379,15 @@ def measure_multiview(gsn, torch, model, stream, sp, args, world):
 
 
 def run_reference(args):
+    """The CPU implementation of the path on the host cores (rank 0 only): full
+    training steps of the bench workload (cpu_step: the reference's own
+    test/cpu_reference.h forward and loss, the FP64 oracle port for the rest)
+    for as many of the requested steps as fit in about 90 s (at least one). No
+    warm-up steps are run: CPU code has nothing to warm across steps of ~15 s.
+    The line reports the steps actually run."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    import scenes
     target_model, model, train, extent = scene(args.gaussians)
     cam = train[0]
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -298,16 +395,17 @@ def run_reference(args):
     img = oracle.render_params(target_model, cam, [0, 0, 0], SH_DEGREE)
     target = np.clip(np.rint(img * 255), 0, 255).astype(np.uint8)
     steps = max(1, args.steps)
-    warm = max(0, args.warmup)
-    res = cpu_baseline(model, cam, target, extent, steps=min(steps + warm, 3))
+    res = cpu_baseline(model, cam, target, extent, steps=steps, budget_s=90.0)
     value = res["value"]
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": steps, "warmup": warm, "ms_per_step": 1000.0 / value, "higher_is_better": True,
+        "steps": res["steps_run"], "warmup": 0, "requested": {"steps": args.steps, "warmup": args.warmup},
+        "ms_per_step": 1000.0 / value, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "plain training step, 1.2M Gaussians, 1600x1064, SH degree 3, ring view 0",
-                   "gaussians": args.gaussians, "width": 1600, "height": 1064},
-        "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "config": {"workload": WORKLOAD, "form": "CPU: reference test/cpu_reference.h forward + loss, FP64 port "
+                                                 "for the gradients and Adam",
+                   "gaussians": args.gaussians, "width": 1600, "height": 1064, "sampling": "none (whole frame)"},
+        "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample", "threads", "legs_s")},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
@@ -581,6 +679,16 @@ def run_gsn(args):
     ms = plain_eager["ms_per_step"] * args.steps
     psnr = plain_eager["psnr_db_last_step"]
     multiview = None if args.no_multiview else measure_multiview(gsn, torch, model, stream, sp, args, world)
+    target0 = targets[0].cpu().numpy()
+    # baselines and the accuracy gate, after (and outside) every timed region of the forms
+    ref_cuda = None
+    if not args.no_reference_cuda and world == 1:
+        ref_cuda = measure_reference_cuda(gsn, torch, model, train, targets, lr, args)
+    gate = None
+    if not args.no_psnr_gate and world == 1:
+        import synthetic_run
+        torch.cuda.empty_cache()
+        gate = synthetic_run.psnr_gate(torch, iterations=args.gate_iterations)
 
     if rank != 0:
         if dist is not None:
@@ -637,16 +745,14 @@ def run_gsn(args):
     roofline = roofline_of(chosen)
     cpu = None
     if not args.no_cpu_baseline and world == 1:
-        tgt0 = targets[0].cpu().numpy()
-        res = cpu_baseline(model, train[0], tgt0, extent, steps=1)
-        cpu = {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        res = cpu_baseline(model, train[0], target0, extent, steps=1)
+        cpu = {k: res[k] for k in ("value", "unit", "cores", "kind", "sample", "threads", "legs_s")}
     out = {
         "metric": METRIC, "value": forms[chosen]["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": forms[chosen]["ms_per_step"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "bf16+f32" if chosen.startswith("precision") else "f32",
         "data": "synthetic",
-        "config": {"workload": ("training step (render, L1+SSIM gradient, backward, Adam) at the "
-                                "1.2M-Gaussian cap, 1600x1064, SH degree 3, one ring view per step"),
+        "config": {"workload": WORKLOAD,
                    "form": chosen, "gaussians": n, "width": 1600, "height": 1064,
                    "records_per_step": records, "visible_gaussians": vis, "parallelism": f"replicas{world}",
                    "l2": "inputs larger than L2 (params + Adam moments 835 MB, a new 5 MB target per step)"},
@@ -667,10 +773,19 @@ def run_gsn(args):
                 "pipelining": ("next step's target upload on a copy stream; each step's loss read back "
                                "asynchronously, the host waits for step k - 2 before issuing step k + 1"),
                 "results_read": len(e2e_seen), "results_finite": bool(np.all(np.isfinite(e2e_seen)))},
+        "reference_cuda": ref_cuda,
+        "plain_over_reference_cuda": (round(value / ref_cuda["value"], 4) if ref_cuda and "value" in ref_cuda
+                                      else None),
+        "chosen_over_reference_cuda": (round(forms[chosen]["value"] / ref_cuda["value"], 4)
+                                       if ref_cuda and "value" in ref_cuda else None),
+        "e2e_chosen_over_reference_cuda": (round(forms[chosen]["e2e"] / ref_cuda["e2e"], 4)
+                                           if ref_cuda and "e2e" in ref_cuda else None),
+        "psnr_gate": gate,
         "roofline": roofline,
         "roofline_plain": roofline_of("plain_fp32"),
-        "psnr_note": ("psnr_db_last_step is the training view's PSNR after this run's ~1,000 steps from the random "
-                      "model; the 0.1 dB condition is on held-out PSNR of full training runs (synthetic_run.py)"),
+        "psnr_note": ("psnr_db_last_step is the training view's PSNR after this run's steps from the random "
+                      "model; the 0.1 dB condition is checked by psnr_gate: held-out PSNR of plain and chosen "
+                      "training runs on the reduced schedule, same scene, density seeds and iterations"),
         "stages": stage_table,
         "stages_culled": {k: round(v, 4) for k, v in culled_stages.items()},
         "stages_culled_sparse": {k: round(v, 4) for k, v in sparse_stages.items()},

@@ -54,6 +54,55 @@ def build_scene(args, torch):
     return train, test, train_images, test_images, points, colors
 
 
+CHOSEN_FORM = dict(precision=1, fp32_ssim=1, exact_culling=1, sparse_adam=1, spatial_order=1, fast_blend=1, graph=1)
+
+
+def reduced_schedule(iterations):
+    """The trainer's schedule compressed to `iterations` (the reference's runs
+    30,000 with densification until 15,000): SH degree +1 every 1,000
+    iterations, position learning-rate decay over the run, density control
+    every 100 iterations from 500 to half the run, opacity reset to 0.01 at
+    a third of the run, large-Gaussian pruning after 1,000 iterations."""
+    return dict(position_lr_steps=iterations, densify_until=iterations // 2,
+                opacity_reset_interval=max(1000, iterations // 3), prune_large_after=1000)
+
+
+def psnr_gate(torch, iterations=6000, seeds=(0, 1), width=1600, height=1064, cap=1_200_000, forms=None):
+    """Held-out PSNR of the plain form against the chosen form (bf16 SH storage
+    with the fp32 SSIM gradient, exact culling, sparse Adam on the Morton order,
+    fast blend arithmetic, CUDA-graph steady state) on the synthetic ring scene
+    (1.5M-Gaussian hidden model, 180 train / 20 held-out views, 100k initial
+    points), each trained for `iterations` on the reduced schedule once per
+    density seed. Returns the per-run and mean PSNRs (FP64, held-out views) and
+    the mean difference chosen - plain."""
+    forms = forms or {"plain": {}, "chosen": CHOSEN_FORM}
+    args = argparse.Namespace(width=width, height=height, target=1_500_000, points=100_000)
+    train, test, train_images, test_images, points, colors = build_scene(args, torch)
+    runs = {k: [] for k in forms}
+    for seed in seeds:
+        for name, switches in forms.items():
+            opts = gsn.TrainingOptions.defaults(max_gaussians=cap, density_seed=seed,
+                                                **reduced_schedule(iterations), **switches)
+            trainer = gsn.Trainer()
+            assert trainer.initialize(train, train_images, points, colors, opts) == 0
+            t0 = time.time()
+            assert trainer.train(iterations) == 0
+            torch.cuda.synchronize()
+            wall = time.time() - t0
+            psnr, _ = trainer.evaluate(test, test_images)
+            runs[name].append({"seed": seed, "psnr_db": round(psnr, 4), "gaussians": trainer.state()["count"],
+                               "wall_s": round(wall, 2)})
+            trainer.close()
+    mean = {k: float(np.mean([r["psnr_db"] for r in v])) for k, v in runs.items()}
+    out = {"iterations": iterations, "views": {"train": len(train), "held_out": len(test)},
+           "resolution": [width, height], "seeds": list(seeds), "schedule": reduced_schedule(iterations),
+           "runs": runs}
+    if "plain" in mean and "chosen" in mean:
+        out.update(plain_db=round(mean["plain"], 4), chosen_db=round(mean["chosen"], 4),
+                   delta_db=round(mean["chosen"] - mean["plain"], 4))
+    return out
+
+
 def main():
     p = argparse.ArgumentParser()
     p.add_argument("--iterations", type=int, default=30000)

@@ -12,6 +12,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_PATH = os.path.join(HERE, "liboracle.so")
 REF_PATH = os.path.join(HERE, "_ref", "libgsref.so")
+REF_CPU_PATH = os.path.join(HERE, "_ref", "libgsref_cpu.so")
 
 _vp, _i32, _i64, _f32, _f64, _u64 = (ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_float,
                                      ctypes.c_double, ctypes.c_uint64)
@@ -95,6 +96,52 @@ def reference():
             pass
         _ref = L
     return _ref
+
+
+_ref_cpu = None
+
+
+def ref_cpu_available():
+    return os.path.exists(REF_CPU_PATH)
+
+
+def ref_cpu():
+    """The reference's CPU reference (test/cpu_reference.h, single-threaded as
+    written), compiled unmodified against the OpenCV shim."""
+    global _ref_cpu
+    if _ref_cpu is None:
+        if not ref_cpu_available():
+            raise RuntimeError(f"{REF_CPU_PATH} missing: run `make -C {HERE} REF=<reference tree>`")
+        L = ctypes.CDLL(REF_CPU_PATH)
+        cp = ctypes.c_void_p
+        L.ref_cpu_render.argtypes = [cp, _i32, cp, cp, _i32, cp]
+        L.ref_cpu_render.restype = _i32
+        L.ref_cpu_loss.argtypes = [cp, cp, _i32, _i32, ctypes.POINTER(_f64)]
+        L.ref_cpu_loss.restype = _i32
+        _ref_cpu = L
+    return _ref_cpu
+
+
+def ref_cpu_render(params, cam, background, sh_degree):
+    """RenderReference (cpu_reference.h:22-116): FP64 image of the 58 x n block."""
+    params = np.ascontiguousarray(params, dtype=np.float32)
+    image = np.zeros((cam.height, cam.width, 3), dtype=np.float64)
+    bg = np.ascontiguousarray(background, dtype=np.float32)
+    st = ref_cpu().ref_cpu_render(ptr(params), params.shape[1], cam_ref(cam), ptr(bg), int(sh_degree), ptr(image))
+    if st != 0:
+        raise RuntimeError("RenderReference failed")
+    return image
+
+
+def ref_cpu_loss(image, target):
+    """ComputeLoss (cpu_reference.h:118-152): 0.8 L1 + 0.2 (1 - SSIM)."""
+    image = np.ascontiguousarray(image, dtype=np.float64)
+    target = np.ascontiguousarray(target, dtype=np.uint8)
+    h, w = target.shape[:2]
+    out = _f64()
+    if ref_cpu().ref_cpu_loss(ptr(image), ptr(target), w, h, ctypes.byref(out)) != 0:
+        raise RuntimeError("ComputeLoss failed")
+    return out.value
 
 
 def ref_fn(name, args, res=ctypes.c_int):

@@ -92,4 +92,49 @@ int ref_adam(const float* gradients, float* params, float* first, float* second,
     return cudaDeviceSynchronize() == cudaSuccess ? 0 : -1;
 }
 
+// The steady-state loop of GaussianSplatting::Train (gaussian_splatting.cpp:
+// 137-187, iterations >= 15000: no density statistics, no density control, no
+// opacity reset; the per-iteration log line is not emitted) over the
+// reference's own Renderer and Solver: per step the view's target is uploaded
+// from host memory with cudaMemcpy2D as Train does (host_targets != nullptr) or
+// read from device memory (device_targets), then Render and Iterate. views[k]
+// is step k's camera index into cameras / the targets (width * height * 3
+// bytes each). The loop's device time (CUDA events on the legacy stream the
+// reference uses) is written to elapsed_ms. Timing harness only.
+int ref_train_replay(void* renderer, void* solver, float* params, int count, const CameraParams* cameras,
+                     const int* views, int steps, const uint8_t* const* host_targets, const uint8_t* device_targets,
+                     uint8_t* target_buffer, const float* background, float* image, float position_lr,
+                     int sh_degree, float* elapsed_ms) {
+    auto* r = static_cast<Renderer*>(renderer);
+    auto* s = static_cast<Solver*>(solver);
+    GaussianBuffers g;
+    g.gaussians_ = params;
+    g.gaussian_count_ = count;
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return -1;
+    int status = 0;
+    cudaEventRecord(e0, 0);
+    for (int k = 0; k < steps && status == 0; ++k) {
+        const CameraParams& cam = cameras[views[k]];
+        const size_t row = static_cast<size_t>(cam.width_) * 3;
+        const uint8_t* target = nullptr;
+        if (host_targets) {
+            if (cudaMemcpy2D(target_buffer, row, host_targets[views[k]], row, row, cam.height_,
+                             cudaMemcpyHostToDevice) != cudaSuccess)
+                status = -2;
+            target = target_buffer;
+        } else {
+            target = device_targets + static_cast<size_t>(views[k]) * row * cam.height_;
+        }
+        if (status == 0 && !r->Render(g, cam, background, image, sh_degree)) status = -3;
+        if (status == 0 && !s->Iterate(cam, *r, image, target, g, position_lr, sh_degree)) status = -4;
+    }
+    cudaEventRecord(e1, 0);
+    if (cudaEventSynchronize(e1) != cudaSuccess) status = status ? status : -5;
+    cudaEventElapsedTime(elapsed_ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return status;
+}
+
 }  // extern "C"
