@@ -98,6 +98,8 @@ def parse():
     p.add_argument("--no-multiview", action="store_true", help="skip the 32-view multi-view measurement")
     p.add_argument("--no-reference-cuda", action="store_true", help="skip the reference CUDA build's leg")
     p.add_argument("--no-psnr-gate", action="store_true", help="skip the held-out PSNR gate runs")
+    p.add_argument("--no-large-scene", action="store_true",
+                   help="skip the 3.0M-Gaussian 2048x1360 batched-form measurement")
     p.add_argument("--gate-iterations", type=int, default=6000,
                    help="iterations of each held-out PSNR gate run (reduced schedule)")
     return p.parse_args()
@@ -189,6 +191,18 @@ def algorithmic_bytes(n, records, tiles, pixels, s=16, tile_passes=2, visible=No
         "raster_backward": records * 40 + pixels * 28 + vis * 48,
         "gaussian_update": updated * row_bytes * 6 + n * (48 + 4 + 16),
     }
+
+
+# FP32 operations per (pixel, record) pair the blend takes, counting an FMA as
+# two: forward 16 (offset, two-FMA power, exp2, clamp, transmittance FMA, weight,
+# three colour FMAs); backward 46 (offset, power, exp2, clamp, weight, 1 - alpha
+# and its reciprocal, dL/dC . c, dL/dalpha, three colour-gradient FMAs, the
+# chain to the power, d(mean) and d(conic) accumulations, |d mean| sums, the
+# carried colour and transmittance). Counted from the fast form's arithmetic.
+FLOP_PER_PAIR = {"raster_forward": 16, "raster_backward": 46}
+# No FP32 figure is measured for this pool; the nominal FMA rate at the
+# maximum SM clock: 148 SMs x 128 lanes x 2 FLOP x 1.965 GHz.
+FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 
 
 def load_peaks():
@@ -313,7 +327,11 @@ def measure_reference_cuda(gsn, torch, model, train, targets, lr, args):
         assert st == 0, f"reference replay failed ({st})"
         return ms.value
 
+    # warm-up: the reference's renderer grows its buffers to the largest view
+    # it has seen, so it first sees the timed views too (no growth inside the
+    # timed loops)
     run(warm, False)
+    run(views, False)
     ms = run(views, False)
     ms_e2e = run(views, True)
     oracle.ref_fn("ref_solver_destroy", [V])(s)
@@ -376,6 +394,106 @@ def measure_multiview(gsn, torch, model, stream, sp, args, world):
             "speedup": round(ms_single / ms_multi, 3),
             "config": {"tile_w": best[0], "tile_h": best[1], "threads": best[2], "key_bits": best[3]},
             "autotune_ms": [[r["tile_w"], r["tile_h"], r["threads"], r["key_bits"], round(r["ms"], 3)] for r in rows]}
+
+
+def measure_large_scene(gsn, torch, stream, sp, args, world):
+    """The batched form at the large scene's scale: a 3.0M-Gaussian model (seed
+    12, means N(0, 4^2)) trained against targets rendered from the hidden
+    4M-Gaussian model (seed 11, means N(0, 4^2)) on 20 of the 300 two-ring
+    views (radii 8 and 12, 2048x1360, fx = fy = 1800). Iterations/s of the
+    unbatched, un-captured plain FP32 path against the chosen form (bf16 SH,
+    exact culling, sparse Adam on the Morton order, fast blend arithmetic, one
+    CUDA graph per step over a fixed record capacity), and the 32-view
+    multi-view render of the same model."""
+    import scenes
+    hidden = scenes.random_gaussians(4_000_000, 11, mean_sigma=4.0)
+    model = scenes.random_gaussians(3_000_000, 12, mean_sigma=4.0)
+    cams = scenes.two_ring_cameras()
+    views = cams[::15][:20]
+    W, H = views[0].width, views[0].height
+    centers = np.array([-np.array(list(c.R_c_w)).reshape(3, 3).T @ np.array(list(c.t_c_w)) for c in cams])
+    extent = 1.1 * float(np.linalg.norm(centers - centers.mean(0), axis=1).max())
+    lr = position_lr(15000, extent)
+    img = torch.empty((H, W, 3), device="cuda")
+    targets = torch.empty((len(views), H, W, 3), dtype=torch.uint8, device="cuda")
+    hp = torch.from_numpy(hidden).cuda()
+    maker = gsn.Renderer()
+    maker.set_stream(sp)
+    for k, c in enumerate(views):
+        assert maker.render(hp.data_ptr(), hp.shape[1], c, [0, 0, 0], img.data_ptr(), SH_DEGREE) == 0
+        targets[k] = (img * 255.0).round().clamp(0, 255).to(torch.uint8)
+    del hp, maker
+    torch.cuda.empty_cache()
+    n = model.shape[1]
+
+    def make(chosen):
+        r, s = gsn.Renderer(), gsn.Solver()
+        r.set_stream(sp)
+        s.set_stream(sp)
+        block = model
+        if chosen:
+            r.set_exact_culling(True)
+            r.set_fast_blend(True)
+            r.set_bf16_sh(True)
+            s.set_sparse_adam(True)
+            s.set_bf16_sh(True)
+            s.set_tensor_core_loss(False)
+            dev_model = torch.from_numpy(model).cuda()
+            perm = torch.empty(n, dtype=torch.int32, device="cuda")
+            gsn.spatial_permutation(dev_model.data_ptr(), n, perm.data_ptr(), sp)
+            block = dev_model[:, perm.long()].cpu().numpy()
+            del dev_model, perm
+            params = gsn.to_precision_layout(block, torch)
+        else:
+            params = torch.from_numpy(np.ascontiguousarray(block)).cuda()
+        return r, s, params
+
+    def step(r, s, params, k):
+        c = views[k % len(views)]
+        assert r.render(params.data_ptr(), n, c, [0, 0, 0], img.data_ptr(), SH_DEGREE) == 0
+        assert s.iterate(c, r, img.data_ptr(), targets[k % len(views)].data_ptr(), params.data_ptr(), n, lr,
+                         SH_DEGREE) == 0
+
+    def timed(run):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        run()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    r, s, params = make(False)
+    for k in range(args.warmup):
+        step(r, s, params, k)
+    ms_plain = timed(lambda: [step(r, s, params, args.warmup + k) for k in range(args.steps)])
+    records_plain = int(r.buffers().record_count_host)
+    del r, s, params
+    torch.cuda.empty_cache()
+    r, s, params = make(True)
+    for k in range(args.warmup):
+        step(r, s, params, k)
+    torch.cuda.synchronize()
+    records = int(r.buffers().record_count_host)
+    graph = gsn.Graph()
+    capacity = int(records * 1.5) + 65536
+    graph.capture(r, s, params.data_ptr(), n, views, targets.data_ptr(), W * H * 3, [0, 0, 0], img.data_ptr(),
+                  SH_DEGREE, capacity, sp)
+    schedule = [(args.warmup + k) % len(views) for k in range(args.steps)]
+    graph.run(schedule[:max(3, args.warmup)], [lr] * max(3, args.warmup))
+    ms_graph = timed(lambda: graph.run(schedule, [lr] * len(schedule)))
+    status = graph.check()
+    graph.close()
+    del r, s, params, targets
+    torch.cuda.empty_cache()
+    rate = lambda t: round(job_rate(world, args.steps, t), 3)  # noqa: E731
+    multiview = measure_multiview(gsn, torch, model, stream, sp, args, world)
+    return {"gaussians": n, "hidden_gaussians": hidden.shape[1], "resolution": [W, H], "views": len(views),
+            "plain_fp32_eager": {"value": rate(ms_plain), "ms_per_step": round(ms_plain / args.steps, 4),
+                                 "records_per_step": records_plain},
+            "chosen_graph": {"value": rate(ms_graph), "ms_per_step": round(ms_graph / args.steps, 4),
+                             "record_capacity": capacity, "records_per_step": records, "status": status},
+            "chosen_over_plain": round(ms_plain / ms_graph, 4), "multiview": multiview}
 
 
 def run_reference(args):
@@ -583,6 +701,17 @@ def run_gsn(args):
         gsn.profile_enable(False)
         return {k: v / args.steps for k, v in st.items() if v > 0}
 
+    def count_pairs(f):
+        """(pixel, record) pairs the blend takes per step, over the timed steps'
+        views (a counting pass after the timed regions)."""
+        counter = torch.zeros(1, dtype=torch.int64, device="cuda")
+        f.renderer.set_pair_counter(counter.data_ptr())
+        for k in range(args.steps):
+            step(f, args.warmup + k)
+        f.renderer.set_pair_counter(0)
+        torch.cuda.synchronize()
+        return float(counter.item()) / args.steps
+
     def measure(f, with_stages=True):
         """Eager timing, per-stage profile, end-to-end timing, then the graph form."""
         for k in range(args.warmup):
@@ -590,6 +719,8 @@ def run_gsn(args):
         torch.cuda.synchronize()
         ms, launches = timed(eager_steps(f, args.warmup), args.steps)
         stages = profile_stages(f) if with_stages else None
+        if stages is not None:
+            stages["pairs_per_step"] = count_pairs(f)
         f.solver.set_compute_loss(True)
         upload_view[0] = 0
         e2e_steps(f, 0)(2)
@@ -680,6 +811,9 @@ def run_gsn(args):
     psnr = plain_eager["psnr_db_last_step"]
     multiview = None if args.no_multiview else measure_multiview(gsn, torch, model, stream, sp, args, world)
     target0 = targets[0].cpu().numpy()
+    large = None
+    if not args.no_large_scene and world == 1:
+        large = measure_large_scene(gsn, torch, stream, sp, args, world)
     # baselines and the accuracy gate, after (and outside) every timed region of the forms
     ref_cuda = None
     if not args.no_reference_cuda and world == 1:
@@ -703,6 +837,8 @@ def run_gsn(args):
     peak, peak_kind = load_peaks()
     stage_table = {}
     for name, t in stages.items():
+        if name == "pairs_per_step":
+            continue
         entry = {"ms": round(t, 4)}
         if name in alg:
             gbs = alg[name] / (t / 1000.0) / 1e9
@@ -717,11 +853,33 @@ def run_gsn(args):
     valid = {k: v for k, v in forms.items() if v.get("status", 0) == 0}
     chosen = max(valid, key=lambda k: valid[k]["value"])
 
+    def stages_of(form):
+        culled_f, sparse_f, bf16_f = "culled" in form, "sparse" in form, form.startswith("precision")
+        return (prec32_stages if "fp32ssim" in form else prec_stages) if bf16_f else \
+            sparse_stages if sparse_f else culled_stages if culled_f else stages
+
+    def blend_roofline(form):
+        """FP32 roofline of the blend kernels of a form: algorithmic FLOPs (the
+        pairs the blend took this step x FLOP_PER_PAIR) over the kernel's
+        per-step device time, against the nominal FP32 rate."""
+        st = stages_of(form)
+        pairs = st.get("pairs_per_step")
+        out = {}
+        for k in ("raster_backward", "raster_forward"):
+            if k in st and pairs:
+                ach = pairs * FLOP_PER_PAIR[k] / (st[k] / 1000.0) / 1e12
+                out[k] = {"bound": "fp32", "kernel": k, "form": form, "achieved": round(ach, 3),
+                          "peak": round(FP32_NOMINAL_TFLOPS, 1), "unit": "TFLOP/s",
+                          "frac": round(ach / FP32_NOMINAL_TFLOPS, 4), "ms": round(st[k], 4),
+                          "pairs_per_step": int(pairs), "flop_per_pair": FLOP_PER_PAIR[k],
+                          "peak_source": ("nominal FP32 FMA rate, 148 SMs x 128 lanes x 2 FLOP x 1.965 GHz "
+                                          "(MEASURED_PEAKS.json holds no FP32 figure)")}
+        return out
+
     def roofline_of(form):
         """Roofline of the largest HBM-bound stage of a form, from its live stage times."""
         culled_f, sparse_f, bf16_f = "culled" in form, "sparse" in form, form.startswith("precision")
-        st = (prec32_stages if "fp32ssim" in form else prec_stages) if bf16_f else \
-            sparse_stages if sparse_f else culled_stages if culled_f else stages
+        st = stages_of(form)
         rec = culled_records if culled_f else records
         ab = algorithmic_bytes(n, rec, tiles, pixels, tile_passes=passes, visible=vis, culled=culled_f,
                                sparse=sparse_f, bf16=bf16_f)
@@ -781,8 +939,11 @@ def run_gsn(args):
         "e2e_chosen_over_reference_cuda": (round(forms[chosen]["e2e"] / ref_cuda["e2e"], 4)
                                            if ref_cuda and "e2e" in ref_cuda else None),
         "psnr_gate": gate,
+        "large_scene": large,
         "roofline": roofline,
         "roofline_plain": roofline_of("plain_fp32"),
+        "roofline_dominant": blend_roofline(chosen).get("raster_backward"),
+        "roofline_blend": {"chosen": blend_roofline(chosen), "plain": blend_roofline("plain_fp32")},
         "psnr_note": ("psnr_db_last_step is the training view's PSNR after this run's steps from the random "
                       "model; the 0.1 dB condition is checked by psnr_gate: held-out PSNR of plain and chosen "
                       "training runs on the reduced schedule, same scene, density seeds and iterations"),

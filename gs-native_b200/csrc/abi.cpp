@@ -240,6 +240,12 @@ int gsn_renderer_set_fast_blend(gsn_renderer* r, int enabled) {
     return GSN_OK;
 }
 
+int gsn_renderer_set_pair_counter(gsn_renderer* r, unsigned long long* device_counter) {
+    if (!r) return GSN_ERR_INVALID_ARGUMENT;
+    r->impl.SetPairCounter(device_counter);
+    return GSN_OK;
+}
+
 int gsn_renderer_set_record_capacity(gsn_renderer* r, int64_t records) {
     if (!r) return GSN_ERR_INVALID_ARGUMENT;
     return r->impl.SetRecordCapacity(records) ? GSN_OK : GSN_ERR_INVALID_ARGUMENT;

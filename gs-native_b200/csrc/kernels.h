@@ -151,6 +151,10 @@ struct RasterForwardArgs {
     uint32_t* record_warps;
     int64_t record_words;
     bool fast;                     // fast power / exp arithmetic (see raster_common.cuh Power)
+    // optional: adds the number of (pixel, record) pairs the blend took (the
+    // algorithmic work of the blend and of its backward) to *pair_count; the
+    // counting variant of the kernel runs only when it is set
+    unsigned long long* pair_count = nullptr;
 };
 int launch_raster_forward(const RasterForwardArgs& a, cudaStream_t stream);
 

@@ -3,33 +3,39 @@
 // One 64-thread CTA per 16x16 tile, four pixels per thread (raster_common.cuh),
 // replaying the tile's records front to back against each pixel's final colour
 // like the reference (solver.cu:325-466), with these changes:
-//   * a thread first sums the contributions of its four pixels in registers, so
-//     one warp reduction serves 128 pixel-record pairs;
-//   * the replay of a tile stops at the largest per-pixel contributor count the
-//     forward pass recorded, and a pixel stops at its own count, so records
-//     behind the saturation point are never re-evaluated;
+//   * the take set is the forward pass's: records [0, limit) of a tile hold
+//     every record a pixel took (limit = the per-pixel contributor count the
+//     forward records), so a pixel takes record idx when idx < limit and the
+//     per-pixel alpha test passes; the transmittance stop needs no replay, and
+//     a warp stops at its pixels' largest limit, the CTA at its own;
+//   * a thread sums the contributions of its four pixels in registers, so one
+//     warp reduction serves 128 pixel-record pairs; the four pixels are
+//     evaluated branch-free (a pixel that does not take a record gets
+//     alpha = 0, which zeroes its terms), so their dependency chains interleave;
 //   * the 11 per-pair values of a warp are combined with a butterfly
 //     reduce-scatter (13 shuffles instead of 55): after five halving steps lane
 //     pairs hold the warp sum of one value each;
 //   * warp sums are accumulated per batch in shared memory (shared-memory
-//     float atomics) and flushed with one global atomic per (Gaussian, value)
-//     and tile, instead of one per warp;
+//     float atomics) and flushed with one 16-byte vector reduction per four
+//     values of a Gaussian and tile (three per Gaussian) when grad_out is
+//     16-byte aligned;
 //   * each warp walks only the records that some pixel of its 16x8 strip took
 //     in the forward pass (per-record strip flags the forward writes) and whose
-//     conservative alpha >= 1/255 box reaches the strip, powers below a
-//     record's alpha floor skip expf, and the three divisions by (1 - alpha)
-//     share one reciprocal (the hardware approximation in the fast form);
-//   * the 12 per-Gaussian sums of a batch are flushed with 16-byte vector
-//     reductions (three per Gaussian) when grad_out is 16-byte aligned;
+//     conservative alpha >= 1/255 box reaches the strip;
 //   * the colour term of dL/dalpha is carried per pixel as two scalars (the
 //     gradient-weighted final colour and the gradient-weighted colour in front
 //     of the record) instead of three channel sums; the fast form carries their
 //     difference as one value;
-//   * d(cov a) and d(cov c) are accumulated without the power's factor 1/2,
-//     which is applied once per record before the warp reduction;
-//   * at most 80 registers (12 CTAs, 24 warps per SM): measured 0.81 ms against
-//     0.88 ms at the unconstrained 122 registers (the exact form uses 80, the
-//     fast form 69).
+//   * per-record factors leave the per-pixel loop: d(cov a) and d(cov c) are
+//     accumulated without the power's factor 1/2 and d(opacity logit) without
+//     the sigmoid's (1 - o), applied once per record before the reduction;
+//   * the fast form evaluates alpha as ex2 of the power in log2 units with the
+//     opacity folded in (two FMAs, one MUFU per pixel; raster_common.cuh
+//     fast_record), takes a pixel on one compare and divides by (1 - alpha)
+//     through the hardware reciprocal; the exact form keeps the reference's
+//     power expression, expf and the correctly rounded reciprocal;
+//   * at most 80 registers (12 CTAs, 24 warps per SM): the exact form uses 80,
+//     the fast form 66.
 // Per-Gaussian output (12 floats, Gaussian-major): d(u, v), d(cov a, b, c),
 // d(opacity logit), d(r, g, b), sum|du|, sum|dv|, 0.
 #include "raster_common.cuh"
@@ -56,9 +62,10 @@ __global__ void __launch_bounds__(kRasterThreads, 12) raster_backward_kernel(Ras
     __shared__ uint32_t s_id[kRasterBatch];
     __shared__ float2 s_mean[kRasterBatch];
     __shared__ float4 s_conic[kRasterBatch];
+    __shared__ float4 s_fast[kRasterBatch];   // fast form: fast_record terms
     __shared__ float3 s_color[kRasterBatch];
     __shared__ float4 s_box[kRasterBatch];
-    __shared__ float s_floor[kRasterBatch];
+    __shared__ float s_floor[kRasterBatch];   // exact form: alpha floor
     __shared__ uint16_t s_warps[kRasterBatch];
     __shared__ __align__(16) float s_acc[kRasterBatch * kVals];
     __shared__ int s_bound;
@@ -73,10 +80,13 @@ __global__ void __launch_bounds__(kRasterThreads, 12) raster_backward_kernel(Ras
 
     float fy[kPixPerThread], T[kPixPerThread];
     // per pixel: dL/dcolour, S = dL/dcolour . final colour and P = dL/dcolour .
-    // colour accumulated in front of the current record
+    // colour accumulated in front of the current record (the fast form carries
+    // P - S in P)
     float gI[kPixPerThread][3], S[kPixPerThread], P[kPixPerThread];
+    // records [0, limit) of the tile hold every record the pixel took in the
+    // forward pass; past it the pixel took nothing (its transmittance stop, or
+    // the end of the list), so limit alone replays the forward's stop
     int limit[kPixPerThread];
-    bool done[kPixPerThread];
     int my_bound = 0;
 #pragma unroll
     for (int p = 0; p < kPixPerThread; ++p) {
@@ -94,19 +104,16 @@ __global__ void __launch_bounds__(kRasterThreads, 12) raster_backward_kernel(Ras
                 gI[p][c] = a.image_grad[pix * 3 + c];
                 S[p] += gI[p][c] * a.image[pix * 3 + c];
             }
-            limit[p] = a.contributors ? a.contributors[pix] : static_cast<int>(end_all - begin);
+            limit[p] = a.contributors[pix];
         }
-        done[p] = limit[p] == 0;
         my_bound = max(my_bound, limit[p]);
-        // the fast form carries P - S in P (one add less per pixel and record)
         if (kFast) P[p] = -S[p];
     }
+    // the warp's replay ends at its pixels' largest bound, the CTA's at its own
+    const int warp_bound = __reduce_max_sync(0xffffffffu, my_bound);
     if (t == 0) s_bound = 0;
     __syncthreads();
-    {
-        int wmax = __reduce_max_sync(0xffffffffu, my_bound);
-        if (lane == 0 && wmax > 0) atomicMax(&s_bound, wmax);
-    }
+    if (lane == 0 && warp_bound > 0) atomicMax(&s_bound, warp_bound);
     __syncthreads();
     const int64_t end = begin + min(static_cast<int64_t>(s_bound), end_all - begin);
 
@@ -127,7 +134,8 @@ __global__ void __launch_bounds__(kRasterThreads, 12) raster_backward_kernel(Ras
                 // with the forward's take bits the box test is implied (a record
                 // some strip pixel took reaches that strip); without them it runs
                 if (!a.record_warps) s_box[slot] = alpha_box(mean, q);
-                s_floor[slot] = alpha_floor(q.w);
+                if (kFast) s_fast[slot] = fast_record(q);
+                else s_floor[slot] = alpha_floor(q.w);
                 uint16_t flags = 0x0101;
                 if (a.record_warps) {
                     const int64_t r = base + slot;
@@ -141,111 +149,132 @@ __global__ void __launch_bounds__(kRasterThreads, 12) raster_backward_kernel(Ras
         for (int k = t; k < kRasterBatch * kVals; k += kRasterThreads) s_acc[k] = 0.0f;
         __syncthreads();
         const int rel = static_cast<int>(base - begin);
+        // this warp's records of the batch: those before its bound
+        const int wend = min(batch, warp_bound - rel);
 #pragma unroll 1
-        for (int k = 0; k < kRasterBatch / 32; ++k) {
+        for (int k = 0; k * 32 < wend; ++k) {
             const int jl = k * 32 + lane;
             // records the forward pass took somewhere in this warp's strip (every
             // other record leaves the strip's pixels unchanged)
-            uint32_t m = __ballot_sync(0xffffffffu, jl < batch && ((s_warps[jl] >> warp_shift) & 1u) &&
+            uint32_t m = __ballot_sync(0xffffffffu, jl < wend && ((s_warps[jl] >> warp_shift) & 1u) &&
                                                         (a.record_warps ||
                                                          box_hits(s_box[jl], g.sx0, g.sx1, g.sy0, g.sy1)));
             while (m) {
-                if (__all_sync(0xffffffffu, done[0] && done[1] && done[2] && done[3])) break;
                 const int j = k * 32 + __ffs(m) - 1;
                 m &= m - 1;
+                const int idx = rel + j;
                 const float2 mu = s_mean[j];
                 const float4 q = s_conic[j];
-                const float lim = s_floor[j];
                 const float3 col = s_color[j];
                 const float cc[3] = {col.x, col.y, col.z};
                 const float dx = mu.x - fx;
-                const Power<kFast> power(q, dx);
+                const float qxdx = q.x * dx, qydx = q.y * dx;
                 float v[kVals];
 #pragma unroll
                 for (int i = 0; i < kVals; ++i) v[i] = 0.0f;
                 // four pixels evaluated without branches (selects only) so their
-                // dependency chains interleave
-                float pw[kPixPerThread], dyv[kPixPerThread];
-                bool act[kPixPerThread];
-                bool any = false;
-#pragma unroll
-                for (int p = 0; p < kPixPerThread; ++p) {
-                    done[p] = done[p] || rel + j >= limit[p];
-                    dyv[p] = mu.y - fy[p];
-                    pw[p] = power.at(dyv[p]);
-                    act[p] = !done[p] && !(pw[p] > 0.0f) && !(pw[p] < lim);
-                    any |= act[p];
-                }
-                bool has = false;
-                if (any) {
+                // dependency chains interleave; a pixel that does not take the
+                // record gets alpha = 0, which zeroes its contributions
+                if constexpr (kFast) {
+                    const float4 kf = s_fast[j];
+                    const float Ax = fmaf(kf.x * dx, dx, kf.w), Bx = kf.y * dx;
 #pragma unroll
                     for (int p = 0; p < kPixPerThread; ++p) {
-                        const float dy = dyv[p];
-                        float raw = gaussian_weight<kFast>(q.w, pw[p]);
-                        float alpha = fminf(kAlphaMax, raw);
-                        bool take = act[p] && !(alpha < kAlphaMin);
-                        float nextT = T[p] * (1.0f - alpha);
-                        bool stop = take && nextT < kTransmittanceMin;
-                        done[p] = done[p] || stop;
-                        take = take && !stop;
-                        has |= take;
-                        float w = alpha * T[p];
-                        float inv = one_over<kFast>(1.0f - alpha);
-                        // dL/dalpha = (dL/dC . (colour in front + T c - final)) / (1 - alpha)
+                        const float dy = mu.y - fy[p];
+                        const float pw2 = fmaf(fmaf(kf.z, dy, Bx), dy, Ax);
+                        const bool take = idx < limit[p] && pw2 >= kLog2AlphaMin;
+                        const float raw = ex2_approx(pw2);
+                        const float alpha = take ? fminf(kAlphaMax, raw) : 0.0f;
+                        // d alpha / d power: raw below the clamp, 0 when clamped or not taken
+                        const float r = alpha < kAlphaMax ? alpha : 0.0f;
+                        const float w = alpha * T[p];
+                        const float inv = one_over<true>(1.0f - alpha);
                         const float G = gI[p][0] * cc[0] + gI[p][1] * cc[1] + gI[p][2] * cc[2];
-                        float dalpha = (kFast ? fmaf(T[p], G, P[p]) : P[p] + T[p] * G - S[p]) * inv;
-                        const float wt = take ? w : 0.0f;
+                        // dL/dalpha = (dL/dC . (colour in front + T c - final)) / (1 - alpha)
+                        const float dalpha = fmaf(T[p], G, P[p]) * inv;
 #pragma unroll
-                        for (int c = 0; c < 3; ++c) v[6 + c] += wt * gI[p][c];
-                        float common = (take && raw < kAlphaMax) ? dalpha * raw : 0.0f;
-                        float qx = q.x * dx + q.y * dy;
-                        float qy = q.y * dx + q.z * dy;
+                        for (int c = 0; c < 3; ++c) v[6 + c] = fmaf(w, gI[p][c], v[6 + c]);
+                        const float common = dalpha * r;
+                        const float qx = fmaf(q.y, dy, qxdx);
+                        const float qy = fmaf(q.z, dy, qydx);
                         const float cqx = common * qx, cqy = common * qy;
                         v[0] -= cqx;
                         v[1] -= cqy;
-                        v[2] += cqx * qx;  // halved once per record below
-                        v[3] += cqx * qy;
-                        v[4] += cqy * qy;  // halved once per record below
-                        v[5] += common * (1.0f - q.w);
+                        v[2] = fmaf(cqx, qx, v[2]);  // halved once per record below
+                        v[3] = fmaf(cqx, qy, v[3]);
+                        v[4] = fmaf(cqy, qy, v[4]);  // halved once per record below
+                        v[5] += common;             // times (1 - o) once per record below
                         v[9] += fabsf(cqx);
                         v[10] += fabsf(cqy);
-                        P[p] += wt * G;
-                        T[p] = take ? nextT : T[p];
+                        P[p] = fmaf(w, G, P[p]);
+                        T[p] = fmaf(-T[p], alpha, T[p]);
+                    }
+                } else {
+                    const Power<false> power(q, dx);
+                    const float lim = s_floor[j];
+#pragma unroll
+                    for (int p = 0; p < kPixPerThread; ++p) {
+                        const float dy = mu.y - fy[p];
+                        const float pw = power.at(dy);
+                        const bool act = idx < limit[p] && !(pw > 0.0f) && !(pw < lim);
+                        const float raw = gaussian_weight<false>(q.w, pw);
+                        const bool take = act && !(raw < kAlphaMin);
+                        const float alpha = take ? fminf(kAlphaMax, raw) : 0.0f;
+                        const float r = alpha < kAlphaMax ? alpha : 0.0f;
+                        const float w = alpha * T[p];
+                        const float inv = one_over<false>(1.0f - alpha);
+                        const float G = gI[p][0] * cc[0] + gI[p][1] * cc[1] + gI[p][2] * cc[2];
+                        const float dalpha = (P[p] + T[p] * G - S[p]) * inv;
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) v[6 + c] += w * gI[p][c];
+                        const float common = dalpha * r;
+                        const float qx = fmaf(q.y, dy, qxdx);
+                        const float qy = fmaf(q.z, dy, qydx);
+                        const float cqx = common * qx, cqy = common * qy;
+                        v[0] -= cqx;
+                        v[1] -= cqy;
+                        v[2] += cqx * qx;
+                        v[3] += cqx * qy;
+                        v[4] += cqy * qy;
+                        v[5] += common;
+                        v[9] += fabsf(cqx);
+                        v[10] += fabsf(cqy);
+                        P[p] += w * G;
+                        T[p] = take ? T[p] * (1.0f - alpha) : T[p];
                     }
                 }
-                if (__any_sync(0xffffffffu, has)) {
-                    // d(cov a) and d(cov c) carry the factor 1/2 of the power (exact)
-                    v[2] *= 0.5f;
-                    v[4] *= 0.5f;
-                    // butterfly reduce-scatter of the 12 slots (slot 11 is padding)
-                    const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4, b1 = lane & 2;
-                    float k6[6];
+                // d(cov a) and d(cov c) carry the factor 1/2 of the power, the
+                // opacity logit the sigmoid's derivative o (1 - o) / o (exact)
+                v[2] *= 0.5f;
+                v[4] *= 0.5f;
+                v[5] *= 1.0f - q.w;
+                // butterfly reduce-scatter of the 12 slots (slot 11 is padding)
+                const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4, b1 = lane & 2;
+                float k6[6];
 #pragma unroll
-                    for (int i = 0; i < 6; ++i) {
-                        float send = sel(b4, v[i], v[6 + i]);
-                        k6[i] = sel(b4, v[6 + i], v[i]) + __shfl_xor_sync(0xffffffffu, send, 16);
-                    }
-                    float k3[3];
-#pragma unroll
-                    for (int i = 0; i < 3; ++i) {
-                        float send = sel(b3, k6[i], k6[3 + i]);
-                        k3[i] = sel(b3, k6[3 + i], k6[i]) + __shfl_xor_sync(0xffffffffu, send, 8);
-                    }
-                    float k4[4] = {k3[0], k3[1], k3[2], 0.0f};
-                    float k2[2];
-#pragma unroll
-                    for (int i = 0; i < 2; ++i) {
-                        float send = sel(b2, k4[i], k4[2 + i]);
-                        k2[i] = sel(b2, k4[2 + i], k4[i]) + __shfl_xor_sync(0xffffffffu, send, 4);
-                    }
-                    float send = sel(b1, k2[0], k2[1]);
-                    float k1 = sel(b1, k2[1], k2[0]) + __shfl_xor_sync(0xffffffffu, send, 2);
-                    k1 += __shfl_xor_sync(0xffffffffu, k1, 1);
-                    const int low = (b2 ? 2 : 0) + (b1 ? 1 : 0);
-                    const int field = (b4 ? 6 : 0) + (b3 ? 3 : 0) + low;
-                    if ((lane & 1) == 0 && low < 3 && field < 11 && k1 != 0.0f)
-                        atomicAdd(&s_acc[j * kVals + field], k1);
+                for (int i = 0; i < 6; ++i) {
+                    float send = sel(b4, v[i], v[6 + i]);
+                    k6[i] = sel(b4, v[6 + i], v[i]) + __shfl_xor_sync(0xffffffffu, send, 16);
                 }
+                float k3[3];
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    float send = sel(b3, k6[i], k6[3 + i]);
+                    k3[i] = sel(b3, k6[3 + i], k6[i]) + __shfl_xor_sync(0xffffffffu, send, 8);
+                }
+                float k4[4] = {k3[0], k3[1], k3[2], 0.0f};
+                float k2[2];
+#pragma unroll
+                for (int i = 0; i < 2; ++i) {
+                    float send = sel(b2, k4[i], k4[2 + i]);
+                    k2[i] = sel(b2, k4[2 + i], k4[i]) + __shfl_xor_sync(0xffffffffu, send, 4);
+                }
+                float send = sel(b1, k2[0], k2[1]);
+                float k1 = sel(b1, k2[1], k2[0]) + __shfl_xor_sync(0xffffffffu, send, 2);
+                k1 += __shfl_xor_sync(0xffffffffu, k1, 1);
+                const int low = (b2 ? 2 : 0) + (b1 ? 1 : 0);
+                const int field = (b4 ? 6 : 0) + (b3 ? 3 : 0) + low;
+                if ((lane & 1) == 0 && low < 3 && field < 11 && k1 != 0.0f) atomicAdd(&s_acc[j * kVals + field], k1);
             }
         }
         __syncthreads();
@@ -273,6 +302,7 @@ __global__ void __launch_bounds__(kRasterThreads, 12) raster_backward_kernel(Ras
 int launch_raster_backward(const RasterBackwardArgs& a, cudaStream_t stream) {
     int64_t tiles = static_cast<int64_t>(a.cam.tile_count_x) * a.cam.tile_count_y;
     if (tiles <= 0) return GSN_OK;
+    if (!a.contributors) return GSN_ERR_INVALID_ARGUMENT;
     if (a.fast) raster_backward_kernel<true><<<static_cast<unsigned>(tiles), kRasterThreads, 0, stream>>>(a);
     else raster_backward_kernel<false><<<static_cast<unsigned>(tiles), kRasterThreads, 0, stream>>>(a);
     return launched(1);

@@ -117,6 +117,33 @@ __device__ __forceinline__ float one_over(float x) {
     return r;
 }
 
+// Fast-form record terms. The fast forms evaluate a record's alpha as
+// ex2(pw2) with pw2 = log2(o) + log2(e) * power, the Gaussian power in log2
+// units with the opacity folded in: per record k = (-log2(e) A / 2,
+// -log2(e) B, -log2(e) C / 2, log2(o)), per (thread, record) the column terms
+// Ax = k.x dx^2 + k.w and Bx = k.y dx, per pixel two FMAs
+// pw2 = (k.z dy + Bx) dy + Ax and one MUFU ex2. A pixel takes the record when
+// alpha >= 1/255, i.e. pw2 >= log2(1/255) (one compare; false for NaN; a
+// record with o < 1/255 never passes since pw2 <= log2(o)). The reference's
+// second test, power > 0, only catches rounding: projected conics are
+// positive definite (the 2D covariance carries +0.3 on its diagonal and
+// det <= 0 is culled), so the true power is never positive; the fast forms
+// drop it, as evaluating it against log2(o) would reject pixels within an ulp
+// of a Gaussian's centre. The forward and backward fast kernels share these
+// expressions, so their take decisions agree.
+constexpr float kLog2e = 1.4426950408889634f;
+constexpr float kLog2AlphaMin = -7.9943534368588578f;  // log2(1/255)
+
+__device__ __forceinline__ float4 fast_record(float4 q) {
+    return make_float4(-0.5f * kLog2e * q.x, -kLog2e * q.y, -0.5f * kLog2e * q.z, log2f(q.w));
+}
+
+__device__ __forceinline__ float ex2_approx(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 // Does the box of a record overlap the pixel rectangle [x0, x1] x [y0, y1]?
 __device__ __forceinline__ bool box_hits(float4 b, float x0, float x1, float y0, float y1) {
     return b.x <= x1 && b.y >= x0 && b.z <= y1 && b.w >= y0;

@@ -14,12 +14,16 @@
 // so the result is unchanged. A CTA stops as soon as all of its pixels are
 // saturated.
 //
-// The per-pixel arithmetic (power, alpha clamp at 0.99, the 1/255 skip and the
-// 1e-4 transmittance stop) is evaluated exactly as the reference does
-// (renderer.cu:273-338), so images are bit-identical for identical inputs.
-// Besides the image the kernel records, per pixel, how many records were
-// consumed up to its last contribution; the backward pass bounds its replay
-// with it.
+// The exact form evaluates the per-pixel arithmetic (power, alpha clamp at
+// 0.99, the 1/255 skip and the 1e-4 transmittance stop) exactly as the
+// reference does (renderer.cu:273-338), so images are bit-identical for
+// identical inputs. The fast form takes alpha as ex2 of the power in log2
+// units with the opacity folded in (raster_common.cuh fast_record: two FMAs and
+// one MUFU per pixel, one compare for the 1/255 test) and updates the
+// transmittance with one FMA; every pixel is evaluated branch-free. Besides the
+// image the kernel records, per pixel, how many records were consumed up to its
+// last contribution; the backward pass takes its replay's take set from it.
+// A counting variant (RasterForwardArgs::pair_count) also sums the pairs taken.
 #include "raster_common.cuh"
 #include "kernels.h"
 
@@ -49,10 +53,10 @@ __device__ __forceinline__ Staged fetch(const RasterForwardArgs& a, int64_t r, i
     return s;
 }
 
-template <bool kFast>
+template <bool kFast, bool kCount>
 __global__ void __launch_bounds__(kRasterThreads) raster_forward_kernel(RasterForwardArgs a) {
     __shared__ float2 s_mean[kRasterBatch];
-    __shared__ float4 s_conic[kRasterBatch];
+    __shared__ float4 s_conic[kRasterBatch];  // exact form: conic + opacity; fast form: fast_record terms
     __shared__ float3 s_color[kRasterBatch];
     __shared__ float4 s_box[kRasterBatch];
     __shared__ float s_floor[kRasterBatch];
@@ -67,6 +71,7 @@ __global__ void __launch_bounds__(kRasterThreads) raster_forward_kernel(RasterFo
     float T[kPixPerThread];
     float3 C[kPixPerThread];
     int consumed[kPixPerThread];
+    unsigned int pairs = 0;  // kCount: pairs this thread's pixels took
 #pragma unroll
     for (int p = 0; p < kPixPerThread; ++p) {
         fy[p] = static_cast<float>(g.py[p]);
@@ -85,19 +90,20 @@ __global__ void __launch_bounds__(kRasterThreads) raster_forward_kernel(RasterFo
         const bool mine = done[0] && done[1] && done[2] && done[3];
         if (__syncthreads_and(mine)) break;
         s_mean[t] = n0.mean;
-        s_conic[t] = n0.conic;
+        s_conic[t] = kFast ? fast_record(n0.conic) : n0.conic;
         s_color[t] = n0.color;
         s_box[t] = alpha_box(n0.mean, n0.conic);
-        s_floor[t] = alpha_floor(n0.conic.w);
+        if (!kFast) s_floor[t] = alpha_floor(n0.conic.w);
         s_mean[t + kRasterThreads] = n1.mean;
-        s_conic[t + kRasterThreads] = n1.conic;
+        s_conic[t + kRasterThreads] = kFast ? fast_record(n1.conic) : n1.conic;
         s_color[t + kRasterThreads] = n1.color;
         s_box[t + kRasterThreads] = alpha_box(n1.mean, n1.conic);
-        s_floor[t + kRasterThreads] = alpha_floor(n1.conic.w);
+        if (!kFast) s_floor[t + kRasterThreads] = alpha_floor(n1.conic.w);
         __syncthreads();
         n0 = fetch(a, base + kRasterBatch + t, end);
         n1 = fetch(a, base + kRasterBatch + kRasterThreads + t, end);
         const int batch = static_cast<int>(min(static_cast<int64_t>(kRasterBatch), end - base));
+        const int rel = static_cast<int>(base - begin);
         uint32_t* plane = a.record_warps ? a.record_warps + warp * a.record_words : nullptr;
 #pragma unroll 1
         for (int k = 0; k < kRasterBatch / 32; ++k) {
@@ -109,39 +115,70 @@ __global__ void __launch_bounds__(kRasterThreads) raster_forward_kernel(RasterFo
                 m &= m - 1;
                 const float2 mu = s_mean[j];
                 const float4 q = s_conic[j];
-                const float lim = s_floor[j];
                 const float3 c = s_color[j];
                 const float dx = mu.x - fx;
-                const Power<kFast> power(q, dx);
-                // the four pixels are evaluated without branches (selects only),
-                // so their dependency chains interleave; values of a pixel that
-                // does not take the record are computed but discarded
-                float pw[kPixPerThread];
-                bool act[kPixPerThread];
-                bool any = false;
+                if constexpr (kFast) {
+                    // fast_record terms (raster_common.cuh), the same expressions as
+                    // the fast backward; every pixel evaluated branch-free, a pixel
+                    // that does not take the record gets alpha = 0
+                    const float Ax = fmaf(q.x * dx, dx, q.w), Bx = q.y * dx;
+                    bool any = false;
 #pragma unroll
-                for (int p = 0; p < kPixPerThread; ++p) {
-                    float dy = mu.y - fy[p];
-                    pw[p] = power.at(dy);
-                    act[p] = !done[p] && !(pw[p] > 0.0f) && !(pw[p] < lim);
-                    any |= act[p];
-                }
-                if (!any) continue;
+                    for (int p = 0; p < kPixPerThread; ++p) {
+                        const float dy = mu.y - fy[p];
+                        const float pw2 = fmaf(fmaf(q.z, dy, Bx), dy, Ax);
+                        const bool take = !done[p] && pw2 >= kLog2AlphaMin;
+                        float alpha = take ? fminf(kAlphaMax, ex2_approx(pw2)) : 0.0f;
+                        const float nextT = fmaf(-T[p], alpha, T[p]);
+                        // a live pixel's T stays >= 1e-4, so only a taken record can stop it
+                        const bool stop = nextT < kTransmittanceMin;
+                        done[p] = done[p] || stop;
+                        alpha = stop ? 0.0f : alpha;
+                        const float w = alpha * T[p];
+                        C[p].x = fmaf(c.x, w, C[p].x);
+                        C[p].y = fmaf(c.y, w, C[p].y);
+                        C[p].z = fmaf(c.z, w, C[p].z);
+                        T[p] = stop ? T[p] : nextT;
+                        const bool took_p = alpha > 0.0f;
+                        consumed[p] = took_p ? rel + j + 1 : consumed[p];
+                        any |= took_p;
+                        if (kCount) pairs += took_p ? 1u : 0u;
+                    }
+                    took |= any ? 1u << (j & 31) : 0u;
+                } else {
+                    const float lim = s_floor[j];
+                    const Power<false> power(q, dx);
+                    // the four pixels are evaluated without branches (selects only),
+                    // so their dependency chains interleave; values of a pixel that
+                    // does not take the record are computed but discarded
+                    float pw[kPixPerThread];
+                    bool act[kPixPerThread];
+                    bool any = false;
 #pragma unroll
-                for (int p = 0; p < kPixPerThread; ++p) {
-                    float alpha = fminf(kAlphaMax, gaussian_weight<kFast>(q.w, pw[p]));
-                    bool take = act[p] && !(alpha < kAlphaMin);
-                    float nextT = T[p] * (1.0f - alpha);
-                    bool stop = take && nextT < kTransmittanceMin;
-                    done[p] = done[p] || stop;
-                    take = take && !stop;
-                    float w = alpha * T[p];
-                    C[p].x = take ? C[p].x + c.x * w : C[p].x;
-                    C[p].y = take ? C[p].y + c.y * w : C[p].y;
-                    C[p].z = take ? C[p].z + c.z * w : C[p].z;
-                    T[p] = take ? nextT : T[p];
-                    consumed[p] = take ? static_cast<int>(base - begin) + j + 1 : consumed[p];
-                    took |= take ? 1u << (j & 31) : 0u;
+                    for (int p = 0; p < kPixPerThread; ++p) {
+                        float dy = mu.y - fy[p];
+                        pw[p] = power.at(dy);
+                        act[p] = !done[p] && !(pw[p] > 0.0f) && !(pw[p] < lim);
+                        any |= act[p];
+                    }
+                    if (!any) continue;
+#pragma unroll
+                    for (int p = 0; p < kPixPerThread; ++p) {
+                        float alpha = fminf(kAlphaMax, gaussian_weight<false>(q.w, pw[p]));
+                        bool take = act[p] && !(alpha < kAlphaMin);
+                        float nextT = T[p] * (1.0f - alpha);
+                        bool stop = take && nextT < kTransmittanceMin;
+                        done[p] = done[p] || stop;
+                        take = take && !stop;
+                        float w = alpha * T[p];
+                        C[p].x = take ? C[p].x + c.x * w : C[p].x;
+                        C[p].y = take ? C[p].y + c.y * w : C[p].y;
+                        C[p].z = take ? C[p].z + c.z * w : C[p].z;
+                        T[p] = take ? nextT : T[p];
+                        consumed[p] = take ? rel + j + 1 : consumed[p];
+                        took |= take ? 1u << (j & 31) : 0u;
+                        if (kCount) pairs += take ? 1u : 0u;
+                    }
                 }
             }
             if (plane) {
@@ -157,6 +194,10 @@ __global__ void __launch_bounds__(kRasterThreads) raster_forward_kernel(RasterFo
                 }
             }
         }
+    }
+    if (kCount) {
+        const unsigned long long warp_pairs = __reduce_add_sync(0xffffffffu, pairs);
+        if (lane == 0 && warp_pairs) atomicAdd(a.pair_count, warp_pairs);
     }
 #pragma unroll
     for (int p = 0; p < kPixPerThread; ++p) {
@@ -176,8 +217,15 @@ __global__ void __launch_bounds__(kRasterThreads) raster_forward_kernel(RasterFo
 int launch_raster_forward(const RasterForwardArgs& a, cudaStream_t stream) {
     int64_t tiles = static_cast<int64_t>(a.cam.tile_count_x) * a.cam.tile_count_y;
     if (tiles <= 0) return GSN_OK;
-    if (a.fast) raster_forward_kernel<true><<<static_cast<unsigned>(tiles), kRasterThreads, 0, stream>>>(a);
-    else raster_forward_kernel<false><<<static_cast<unsigned>(tiles), kRasterThreads, 0, stream>>>(a);
+    const unsigned grid = static_cast<unsigned>(tiles);
+    if (a.pair_count) {
+        if (a.fast) raster_forward_kernel<true, true><<<grid, kRasterThreads, 0, stream>>>(a);
+        else raster_forward_kernel<false, true><<<grid, kRasterThreads, 0, stream>>>(a);
+    } else if (a.fast) {
+        raster_forward_kernel<true, false><<<grid, kRasterThreads, 0, stream>>>(a);
+    } else {
+        raster_forward_kernel<false, false><<<grid, kRasterThreads, 0, stream>>>(a);
+    }
     return launched(1);
 }
 

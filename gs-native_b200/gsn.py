@@ -183,6 +183,11 @@ class Renderer:
         fn = declare("gsn_renderer_set_fast_blend", [ctypes.c_void_p, ctypes.c_int])
         _check(fn(self.handle, int(bool(enabled))), "set_fast_blend")
 
+    def set_pair_counter(self, device_ptr):
+        fn = declare("gsn_renderer_set_pair_counter", [ctypes.c_void_p, ctypes.c_void_p])
+        _check(fn(self.handle, ctypes.c_void_p(device_ptr or None)), "set_pair_counter")
+
+
 
 def launch_count():
     return int(lib().gsn_kernel_launch_count())

@@ -158,6 +158,15 @@ def training_scene_cameras(count=200, held_out_every=10):
     return train, test
 
 
+def two_ring_cameras(count=300, radii=(8.0, 12.0), width=2048, height=1360, focal=1800.0):
+    """The large scene's cameras: `count` views split over two rings of radii
+    8 and 12 around the origin at elevation +/-15 deg, 2048x1360, fx = fy =
+    1800."""
+    half = count // 2
+    return (ring_cameras(half, radii[0], 15.0, width, height, focal, focal) +
+            ring_cameras(count - half, radii[1], 15.0, width, height, focal, focal))
+
+
 def initial_points(target_params, count, seed, jitter=0.05):
     """`count` target means jittered by N(0, jitter^2) with the target's SH-DC colour."""
     rng = np.random.default_rng(seed)

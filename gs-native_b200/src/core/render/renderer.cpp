@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <cstdint>
 
 #include "kernels.h"
 #include "profile.h"
@@ -107,8 +108,6 @@ bool Renderer::Render(const GaussianBuffers& gaussians, const CameraParams& came
     last_count_ = count;
     const gsn_camera& cam = AsGsnCamera(camera);
     cudaStream_t s = stream_;
-    int* record_count = counters_.get();
-    int* overflow = counters_.get() + 1;
     if (cudaMemsetAsync(counters_.get(), 0, 2 * sizeof(int), s) != cudaSuccess) return false;
 
     int64_t records = 0;
@@ -133,6 +132,28 @@ bool Renderer::Render(const GaussianBuffers& gaussians, const CameraParams& came
                                             scratch, &in_alt, visible, s) != GSN_OK)
             return false;
         const uint32_t* by_depth = depth_ids_[in_alt ? 1 : 0].get();
+        if (!OrderBySort(by_depth, visible, count, camera, tile_count, &records)) return false;
+    } else {
+        last_records_ = 0;
+        sorted_ids_ = record_ids_[0].get();
+        if (cudaMemsetAsync(tile_offsets_.get(), 0, (static_cast<size_t>(tile_count) + 1) * sizeof(int64_t), s) !=
+            cudaSuccess)
+            return false;
+    }
+    return Blend(cam, background, image);
+}
+
+// Per-tile lists by emitting the records in depth order and stable-sorting
+// them by tile over all records (record scan, emission, radix sort, ranges).
+bool Renderer::OrderBySort(const uint32_t* by_depth, const int* visible, int count, const CameraParams& camera,
+                           int tile_count, int64_t* records_out) {
+    cudaStream_t s = stream_;
+    int* record_count = counters_.get();
+    int* overflow = counters_.get() + 1;
+    int64_t records = 0;
+    gsn::RadixSortScratch scratch;
+    bool in_alt = false;
+    {
         gsn::stage_mark(s, gsn::kStageRecordScan);
         if (gsn::launch_exclusive_scan(exact_culling_ ? cull_counts_.get() : tile_counts_.get(), by_depth,
                                        record_start_.get(), count, scan_scratch_.get(), s, visible) != GSN_OK)
@@ -181,13 +202,14 @@ bool Renderer::Render(const GaussianBuffers& gaussians, const CameraParams& came
         if (gsn::launch_tile_ranges(tile_keys_[in_alt ? 1 : 0].get(), record_count, std::max(max_records, 1),
                                     tile_count, tile_offsets_.get(), s) != GSN_OK)
             return false;
-    } else {
-        last_records_ = 0;
-        sorted_ids_ = record_ids_[0].get();
-        if (cudaMemsetAsync(tile_offsets_.get(), 0, (static_cast<size_t>(tile_count) + 1) * sizeof(int64_t), s) !=
-            cudaSuccess)
-            return false;
     }
+    *records_out = records;
+    return true;
+}
+
+// The per-tile blend of the ordered records.
+bool Renderer::Blend(const gsn_camera& cam, const float* background, float* image) {
+    cudaStream_t s = stream_;
     gsn::RasterForwardArgs ra;
     ra.tile_ids = sorted_ids_;
     ra.tile_offsets = tile_offsets_.get();
@@ -202,6 +224,7 @@ bool Renderer::Render(const GaussianBuffers& gaussians, const CameraParams& came
     ra.record_warps = record_warps_.get();
     ra.record_words = record_words_;
     ra.fast = fast_blend_;
+    ra.pair_count = pair_counter_;
     if (record_warps_.get() &&
         cudaMemsetAsync(record_warps_.get(), 0, 2 * static_cast<size_t>(record_words_) * sizeof(uint32_t), s) !=
             cudaSuccess)

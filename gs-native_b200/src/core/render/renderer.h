@@ -73,6 +73,10 @@ public:
     // 24-bit keys (three radix passes instead of four).
     void SetFastBlend(bool enabled) { fast_blend_ = enabled; }
     bool GetFastBlend() const { return fast_blend_; }
+    // Measurement: while set, every Render adds the number of (pixel, record)
+    // pairs its blend took to this device counter (a counting variant of the
+    // blend kernel; nullptr, the default, runs the plain one).
+    void SetPairCounter(unsigned long long* device_counter) { pair_counter_ = device_counter; }
     bool GetExactCulling() const { return exact_culling_; }
     bool GetBf16Sh() const { return bf16_sh_; }
     const int* GetTileCounts() const { return tile_counts_.get(); }
@@ -101,11 +105,16 @@ private:
     size_t gaussian_capacity_ = 0;
     size_t tile_capacity_ = 0;
     int64_t record_capacity_ = 0;
+    bool OrderBySort(const uint32_t* by_depth, const int* visible, int count, const CameraParams& camera,
+                     int tile_count, int64_t* records_out);
+    bool Blend(const gsn_camera& cam, const float* background, float* image);
+
     bool fixed_capacity_ = false;
     const gsn_camera* device_camera_ = nullptr;
     bool bf16_sh_ = false;
     bool exact_culling_ = false;
     bool fast_blend_ = false;
+    unsigned long long* pair_counter_ = nullptr;
     int64_t last_records_ = 0;
     int last_count_ = 0;
 

@@ -55,6 +55,9 @@ def build_scene(args, torch):
 
 
 CHOSEN_FORM = dict(precision=1, fp32_ssim=1, exact_culling=1, sparse_adam=1, spatial_order=1, fast_blend=1, graph=1)
+# the precision form as specified: bf16 SH storage, tensor-core SSIM, FP64
+# near-singular conics, nothing else changed
+PRECISION_FORM = dict(precision=1)
 
 
 def reduced_schedule(iterations):
@@ -70,12 +73,13 @@ def reduced_schedule(iterations):
 def psnr_gate(torch, iterations=6000, seeds=(0, 1), width=1600, height=1064, cap=1_200_000, forms=None):
     """Held-out PSNR of the plain form against the chosen form (bf16 SH storage
     with the fp32 SSIM gradient, exact culling, sparse Adam on the Morton order,
-    fast blend arithmetic, CUDA-graph steady state) on the synthetic ring scene
+    fast blend arithmetic, CUDA-graph steady state) and the precision form (bf16
+    SH storage, tensor-core SSIM) on the synthetic ring scene
     (1.5M-Gaussian hidden model, 180 train / 20 held-out views, 100k initial
     points), each trained for `iterations` on the reduced schedule once per
     density seed. Returns the per-run and mean PSNRs (FP64, held-out views) and
-    the mean difference chosen - plain."""
-    forms = forms or {"plain": {}, "chosen": CHOSEN_FORM}
+    the mean differences chosen - plain and precision - plain."""
+    forms = forms or {"plain": {}, "chosen": CHOSEN_FORM, "precision": PRECISION_FORM}
     args = argparse.Namespace(width=width, height=height, target=1_500_000, points=100_000)
     train, test, train_images, test_images, points, colors = build_scene(args, torch)
     runs = {k: [] for k in forms}
@@ -100,6 +104,9 @@ def psnr_gate(torch, iterations=6000, seeds=(0, 1), width=1600, height=1064, cap
     if "plain" in mean and "chosen" in mean:
         out.update(plain_db=round(mean["plain"], 4), chosen_db=round(mean["chosen"], 4),
                    delta_db=round(mean["chosen"] - mean["plain"], 4))
+    if "plain" in mean and "precision" in mean:
+        out.update(precision_db=round(mean["precision"], 4),
+                   precision_delta_db=round(mean["precision"] - mean["plain"], 4))
     return out
 
 

@@ -174,6 +174,10 @@ int gsn_renderer_set_exact_culling(gsn_renderer* r, int enabled);
  * approximation, instead of the expression and expf of renderer.cu:300-305.
  * Images move by a few ulps; the solver's backward pass follows the setting. */
 int gsn_renderer_set_fast_blend(gsn_renderer* r, int enabled);
+/* Measurement hook (gs-native extension, no reference counterpart): while
+ * device_counter (device unsigned long long) is set, each render adds the
+ * number of (pixel, record) pairs its blend took to it; NULL turns it off. */
+int gsn_renderer_set_pair_counter(gsn_renderer* r, unsigned long long* device_counter);
 
 
 /* ------------------------------------------------------------------ solver
