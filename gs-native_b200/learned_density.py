@@ -129,17 +129,20 @@ def train_run(scene, options, iterations, mlp_weights=None, confidence=0.9):
     assert tr.initialize(scene.train_cams, scene.train_images, scene.points, scene.colors, opts) == 0
     if learned:
         tr.set_density_mlp(mlp_weights)
+    import time
     load = 0
     done = 0
+    t0 = time.time()
     while done < iterations:
         k = min(100, iterations - done)
         assert tr.train(k) == 0
         done += k
-        load += tr.state()["count"] * k
+        load += tr.state()["count"] * k  # state() waits for the chunk
+    seconds = time.time() - t0
     psnr, loss = tr.evaluate(scene.test_cams, scene.test_images)
     count = tr.state()["count"]
     tr.close()
-    return dict(psnr=psnr, loss=loss, count=count, gaussian_iterations=load)
+    return dict(psnr=psnr, loss=loss, count=count, gaussian_iterations=load, iters_per_s=iterations / seconds)
 
 
 def judge(scene, options, iterations, mlp_weights, confidence=0.9, tolerance_db=0.1, repeats=3):
@@ -157,10 +160,110 @@ def judge(scene, options, iterations, mlp_weights, confidence=0.9, tolerance_db=
     delta = float(diffs.mean())
     mean = lambda runs, key: float(np.mean([x[key] for x in runs]))  # noqa: E731
     return dict(plain=dict(psnr=mean(plain, "psnr"), count=mean(plain, "count"),
-                           gaussian_iterations=mean(plain, "gaussian_iterations")),
+                           gaussian_iterations=mean(plain, "gaussian_iterations"),
+                           iters_per_s=mean(plain, "iters_per_s")),
                 learned=dict(psnr=mean(learned, "psnr"), count=mean(learned, "count"),
-                             gaussian_iterations=mean(learned, "gaussian_iterations")),
+                             gaussian_iterations=mean(learned, "gaussian_iterations"),
+                             iters_per_s=mean(learned, "iters_per_s")),
                 runs=dict(plain=[x["psnr"] for x in plain], learned=[x["psnr"] for x in learned]),
                 accepted=bool(delta >= -tolerance_db), delta_db=delta,
                 delta_std_db=float(diffs.std(ddof=1)) if repeats > 1 else 0.0,
                 load_ratio=mean(learned, "gaussian_iterations") / max(mean(plain, "gaussian_iterations"), 1.0))
+
+
+def large_scene(seed, points=100_000, width=2048, height=1360, held_out_every=10, torch=None):
+    """One seeded training setup of the large scene: a 4M-Gaussian hidden model
+    (means N(0, 4^2)) seen by 300 cameras on two rings of radii 8 and 12 at
+    2048x1360 (fx = fy = 1800), every tenth camera held out; `points` target
+    means jittered by N(0, 0.05^2) with the target's DC colours start the
+    training. Targets are rendered on the GPU from the hidden model."""
+    import scenes
+    if torch is None:
+        import torch
+    hidden = scenes.random_gaussians(4_000_000, seed, mean_sigma=4.0)
+    cams = scenes.two_ring_cameras(300, width=width, height=height, focal=1800.0 * width / 2048.0)
+    train = [c for k, c in enumerate(cams) if k % held_out_every != held_out_every - 1]
+    test = [c for k, c in enumerate(cams) if k % held_out_every == held_out_every - 1]
+    r = gsn.Renderer()
+    hp = torch.from_numpy(hidden).cuda()
+    img = torch.empty((height, width, 3), device="cuda")
+
+    def render(cs):
+        out = []
+        for c in cs:
+            assert r.render(hp.data_ptr(), hp.shape[1], c, [0, 0, 0], img.data_ptr(), 3) == 0
+            out.append((img * 255.0).round().clamp(0, 255).to(torch.uint8).cpu().numpy())
+        return out
+
+    train_images, test_images = render(train), render(test)
+    pts, cols = scenes.initial_points(hidden, points, seed + 1000)
+    del hp
+    r.close()
+    return Scene(train, train_images, test, test_images, pts, cols)
+
+
+def main():
+    """The learned-density protocol on the large scene: plain-rule runs with the
+    density log on five seeded training scenes (seeds 12-16), the MLP fitted
+    on the GPU, then the judge on the unseen target scene (seed 11): paired
+    plain / learned runs over density seeds, held-out PSNR, final Gaussian
+    count and iterations/s. Each stage's result is appended to --out as one
+    JSON line as soon as it is known.
+
+        python learned_density.py [--iterations 30000] [--cap 3000000] [--repeats 2] --out results.jsonl
+    """
+    import argparse
+    import json
+    import time
+
+    import torch
+
+    p = argparse.ArgumentParser()
+    p.add_argument("--iterations", type=int, default=30000)
+    p.add_argument("--cap", type=int, default=3_000_000)
+    p.add_argument("--repeats", type=int, default=2)
+    p.add_argument("--train-seeds", default="12,13,14,15,16")
+    p.add_argument("--eval-seed", type=int, default=11)
+    p.add_argument("--width", type=int, default=2048)
+    p.add_argument("--height", type=int, default=1360)
+    p.add_argument("--out", required=True)
+    args = p.parse_args()
+    gsn.lib()
+    options = dict(max_gaussians=args.cap)
+    if args.iterations != 30000:
+        import synthetic_run
+        options.update(synthetic_run.reduced_schedule(args.iterations))
+
+    def emit(record):
+        with open(args.out, "a") as f:
+            f.write(json.dumps(record) + "\n")
+
+    parts = []
+    for seed in [int(s) for s in args.train_seeds.split(",")]:
+        t0 = time.time()
+        sc = large_scene(seed, width=args.width, height=args.height, torch=torch)
+        f, l, w, info = collect(sc, options, args.iterations, seed=seed)
+        parts.append((f, l, w, info))
+        emit({"stage": "collect", "seed": seed, "samples": int(len(l)), "steps": info["steps"],
+              "relabelled": info["relabelled"], "labels": np.bincount(l, minlength=4).tolist(),
+              "wall_s": round(time.time() - t0, 1)})
+        del sc
+    feats = np.concatenate([x[0] for x in parts])
+    labels = np.concatenate([x[1] for x in parts])
+    weights = np.concatenate([x[2] for x in parts])
+    t0 = time.time()
+    mlp_weights, loss = fit(feats, labels, weights)
+    np.save(args.out + ".weights.npy", mlp_weights)
+    emit({"stage": "fit", "samples": int(len(labels)), "loss": float(loss), "wall_s": round(time.time() - t0, 1)})
+    sc = large_scene(args.eval_seed, width=args.width, height=args.height, torch=torch)
+    t0 = time.time()
+    verdict = judge(sc, options, args.iterations, mlp_weights, repeats=args.repeats)
+    verdict["wall_s"] = round(time.time() - t0, 1)
+    verdict["iterations"] = args.iterations
+    verdict["stage"] = "judge"
+    emit(verdict)
+    print(json.dumps(verdict), flush=True)
+
+
+if __name__ == "__main__":
+    main()

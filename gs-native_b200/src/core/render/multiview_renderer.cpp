@@ -38,6 +38,26 @@ MultiViewRenderer::MultiViewRenderer() = default;
 
 MultiViewRenderer::~MultiViewRenderer() {
     if (host_totals_) cudaFreeHost(host_totals_);
+    for (cudaEvent_t e : joins_) cudaEventDestroy(e);
+    if (fork_) cudaEventDestroy(fork_);
+    for (cudaStream_t st : side_) cudaStreamDestroy(st);
+}
+
+bool MultiViewRenderer::EnsureSideStreams() {
+    if (!side_.empty()) return true;
+    if (cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming) != cudaSuccess) {
+        fork_ = nullptr;
+        return false;
+    }
+    for (int k = 0; k < kSideStreams; ++k) {
+        cudaStream_t st = nullptr;
+        cudaEvent_t e = nullptr;
+        if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return false;
+        side_.push_back(st);
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return false;
+        joins_.push_back(e);
+    }
+    return true;
 }
 
 bool MultiViewRenderer::ConfigValid(const MultiViewConfig& c) {
@@ -70,7 +90,8 @@ bool SortScratch(DeviceArray<unsigned char>& scratch, size_t& have, int64_t need
 
 }  // namespace
 
-bool MultiViewRenderer::Prepare(View& v, const GaussianBuffers& g, const CameraParams& camera, int sh_degree) {
+bool MultiViewRenderer::Prepare(View& v, const GaussianBuffers& g, const CameraParams& camera, int sh_degree,
+                                cudaStream_t stream) {
     const int n = g.gaussian_count_;
     v.cam = AsGsnCamera(camera);
     v.cam.tile_count_x = (camera.width_ + config_.tile_w - 1) / config_.tile_w;
@@ -92,25 +113,25 @@ bool MultiViewRenderer::Prepare(View& v, const GaussianBuffers& g, const CameraP
     if (!SortScratch(v.sort_scratch, v.sort_scratch_count, n)) return false;
     gsn::ProjectOutputs po{v.means.get(), v.conic.get(), v.colors.get(), v.depths.get(),
                            v.rects.get(), v.tile_counts.get(), v.depth_keys[0].get(), nullptr, nullptr, 0};
-    if (gsn::launch_project_tiled(g.gaussians_, n, v.cam, config_.tile_w, config_.tile_h, sh_degree, po, stream_) !=
+    if (gsn::launch_project_tiled(g.gaussians_, n, v.cam, config_.tile_w, config_.tile_h, sh_degree, po, stream) !=
         GSN_OK)
         return false;
     if (config_.key_bits == 32) {
         gsn::RadixSortScratch scratch = gsn::radix_sort_scratch(v.sort_scratch.get(), static_cast<int>(v.sort_scratch_count));
         bool alt = false;
         if (gsn::launch_radix_sort(v.depth_keys[0].get(), v.depth_ids[0].get(), v.depth_keys[1].get(),
-                                   v.depth_ids[1].get(), true, n, nullptr, 0, 32, scratch, &alt, stream_) != GSN_OK)
+                                   v.depth_ids[1].get(), true, n, nullptr, 0, 32, scratch, &alt, stream) != GSN_OK)
             return false;
         v.by_depth = v.depth_ids[alt ? 1 : 0].get();
         return gsn::launch_exclusive_scan(v.tile_counts.get(), v.by_depth, v.record_start.get(), n,
-                                          v.scan_scratch.get(), stream_) == GSN_OK;
+                                          v.scan_scratch.get(), stream) == GSN_OK;
     }
     v.by_depth = nullptr;
     return gsn::launch_exclusive_scan(v.tile_counts.get(), nullptr, v.record_start.get(), n, v.scan_scratch.get(),
-                                      stream_) == GSN_OK;
+                                      stream) == GSN_OK;
 }
 
-bool MultiViewRenderer::Order(View& v, int n) {
+bool MultiViewRenderer::Order(View& v, int n, cudaStream_t stream) {
     const int64_t r = v.records;
     if (r > v.record_capacity) {
         const int64_t grow = std::min<int64_t>(std::max<int64_t>(r, v.record_capacity + v.record_capacity / 2), INT_MAX);
@@ -126,19 +147,19 @@ bool MultiViewRenderer::Order(View& v, int n) {
     if (config_.key_bits == 32) {
         if (gsn::launch_emit_records(v.by_depth, v.record_start.get(), v.rects.get(), n, v.cam.tile_count_x,
                                      v.tile_keys[0].get(), v.record_ids[0].get(), v.record_capacity, nullptr,
-                                     stream_) != GSN_OK)
+                                     stream) != GSN_OK)
             return false;
         if (records > 0 &&
             gsn::launch_radix_sort(v.tile_keys[0].get(), v.record_ids[0].get(), v.tile_keys[1].get(),
                                    v.record_ids[1].get(), false, records, nullptr, 0, Bits(v.tiles), scratch, &alt,
-                                   stream_) != GSN_OK)
+                                   stream) != GSN_OK)
             return false;
     } else {
         // records in id order with their depth key; stable sort on depth (the
         // values are record indices), gather, stable sort on the tile key
         if (gsn::launch_emit_keyed(v.record_start.get(), v.rects.get(), v.tile_counts.get(), v.depth_keys[0].get(),
                                    n, v.cam.tile_count_x, v.record_capacity, v.tile_keys[0].get(),
-                                   v.record_depth.get(), v.record_ids[0].get(), stream_) != GSN_OK)
+                                   v.record_depth.get(), v.record_ids[0].get(), stream) != GSN_OK)
             return false;
         if (records > 0) {
             bool depth_alt = false;
@@ -149,31 +170,31 @@ bool MultiViewRenderer::Order(View& v, int n) {
             uint32_t* order_alt = v.depth_ids[1].Reserve(static_cast<size_t>(records)) ? v.depth_ids[1].get() : nullptr;
             if (!order_alt ||
                 gsn::launch_radix_sort(keys, order, keys_alt, order_alt, true, records, nullptr, 0, 32, scratch,
-                                       &depth_alt, stream_) != GSN_OK)
+                                       &depth_alt, stream) != GSN_OK)
                 return false;
             const uint32_t* sorted_order = depth_alt ? order_alt : order;
             // gathered (tile, id) pairs into record_depth / tile_keys[1]
             if (gsn::launch_gather_records(sorted_order, v.tile_keys[0].get(), v.record_ids[0].get(), records,
-                                           v.record_depth.get(), v.tile_keys[1].get(), stream_) != GSN_OK)
+                                           v.record_depth.get(), v.tile_keys[1].get(), stream) != GSN_OK)
                 return false;
             const int bits = config_.key_bits == 48 ? Bits(v.tiles) : 32;
             bool tile_alt = false;
             if (gsn::launch_radix_sort(v.record_depth.get(), v.tile_keys[1].get(), v.tile_keys[0].get(),
                                        v.record_ids[0].get(), false, records, nullptr, 0, bits, scratch, &tile_alt,
-                                       stream_) != GSN_OK)
+                                       stream) != GSN_OK)
                 return false;
             v.sorted_ids = tile_alt ? v.record_ids[0].get() : v.tile_keys[1].get();
             const uint32_t* sorted_tiles = tile_alt ? v.tile_keys[0].get() : v.record_depth.get();
             return gsn::launch_tile_ranges(sorted_tiles, v.record_start.get() + n, std::max(records, 1), v.tiles,
-                                           v.tile_offsets.get(), stream_) == GSN_OK;
+                                           v.tile_offsets.get(), stream) == GSN_OK;
         }
     }
     v.sorted_ids = v.record_ids[alt ? 1 : 0].get();
     if (records == 0)
         return cudaMemsetAsync(v.tile_offsets.get(), 0, (static_cast<size_t>(v.tiles) + 1) * sizeof(int64_t),
-                               stream_) == cudaSuccess;
+                               stream) == cudaSuccess;
     return gsn::launch_tile_ranges(v.tile_keys[alt ? 1 : 0].get(), v.record_start.get() + n, records, v.tiles,
-                                   v.tile_offsets.get(), stream_) == GSN_OK;
+                                   v.tile_offsets.get(), stream) == GSN_OK;
 }
 
 bool MultiViewRenderer::Render(const GaussianBuffers& g, const std::vector<CameraParams>& cameras,
@@ -194,22 +215,34 @@ bool MultiViewRenderer::Render(const GaussianBuffers& g, const std::vector<Camer
         host_totals_count_ = count;
     }
     sh_degree = std::clamp(sh_degree, 0, 3);
+    if (!EnsureSideStreams()) return false;
+    // the views' preprocessing runs on side streams, view k on side stream
+    // k % kSideStreams, after the work already queued on the caller's stream
+    if (cudaEventRecord(fork_, stream_) != cudaSuccess) return false;
+    for (cudaStream_t side : side_)
+        if (cudaStreamWaitEvent(side, fork_, 0) != cudaSuccess) return false;
+    auto side_of = [&](size_t k) { return side_[k % side_.size()]; };
     // phase 1: projection and record counts of every view, one readback
     for (size_t k = 0; k < count; ++k) {
-        if (!Prepare(*views_[k], g, cameras[k], sh_degree) ||
+        if (!Prepare(*views_[k], g, cameras[k], sh_degree, side_of(k)) ||
             cudaMemcpyAsync(host_totals_ + k, views_[k]->record_start.get() + n, sizeof(int), cudaMemcpyDeviceToHost,
-                            stream_) != cudaSuccess)
+                            side_of(k)) != cudaSuccess)
             return false;
     }
-    if (cudaStreamSynchronize(stream_) != cudaSuccess) return false;
-    // phase 2: record ordering and ranges of every view
+    for (cudaStream_t side : side_)
+        if (cudaStreamSynchronize(side) != cudaSuccess) return false;
+    // phase 2: record ordering and ranges of every view, then the caller's
+    // stream waits for all of them
     last_records_ = 0;
     for (size_t k = 0; k < count; ++k) {
         if (host_totals_[k] < 0) return false;
         views_[k]->records = host_totals_[k];
         last_records_ += host_totals_[k];
-        if (!Order(*views_[k], n)) return false;
+        if (!Order(*views_[k], n, side_of(k))) return false;
     }
+    for (size_t j = 0; j < side_.size(); ++j)
+        if (cudaEventRecord(joins_[j], side_[j]) != cudaSuccess || cudaStreamWaitEvent(stream_, joins_[j], 0) != cudaSuccess)
+            return false;
     // one persistent blend over all (view, tile) work items
     std::vector<gsn::MultiView> table(count);
     std::vector<int> prefix(count + 1, 0);

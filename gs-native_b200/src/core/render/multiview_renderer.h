@@ -5,7 +5,8 @@
 // width.
 //
 // Per view the preprocessing is the single-view renderer's (projection, record
-// ordering, per-tile ranges) into buffers of its own; all views' record totals
+// ordering, per-tile ranges) into buffers of its own, the views spread over
+// eight side streams so their small launches overlap; all views' record totals
 // are read back with one synchronisation, and one persistent kernel then blends
 // every (view, tile) work item. Sort key width: 32 = a stable sort of the N
 // depth keys, records emitted in depth order, then a stable sort on the tile
@@ -63,9 +64,17 @@ public:
 
 private:
     struct View;
-    bool Prepare(View& v, const GaussianBuffers& g, const CameraParams& cam, int sh_degree);
-    bool Order(View& v, int count);
+    bool Prepare(View& v, const GaussianBuffers& g, const CameraParams& cam, int sh_degree, cudaStream_t stream);
+    bool Order(View& v, int count, cudaStream_t stream);
+    bool EnsureSideStreams();
 
+    // The views' projection and record ordering (small, latency-bound
+    // launches) run concurrently on kSideStreams streams of the renderer's
+    // own; the persistent blend runs on the caller's stream after all of them.
+    static constexpr int kSideStreams = 8;
+    std::vector<cudaStream_t> side_;
+    std::vector<cudaEvent_t> joins_;
+    cudaEvent_t fork_ = nullptr;
     cudaStream_t stream_ = nullptr;
     MultiViewConfig config_;
     std::vector<std::unique_ptr<View>> views_;
