@@ -58,6 +58,12 @@ CHOSEN_FORM = dict(precision=1, fp32_ssim=1, exact_culling=1, sparse_adam=1, spa
 # the precision form as specified: bf16 SH storage, tensor-core SSIM, FP64
 # near-singular conics, nothing else changed
 PRECISION_FORM = dict(precision=1)
+# the chosen form with the learned density policy proposing the density-control
+# actions (the threshold rule stays the fallback below the policy's confidence)
+CHOSEN_LEARNED_FORM = dict(CHOSEN_FORM, learned_density=1)
+# weights of the density policy trained on the large scene's five seeded
+# training scenes (learned_density.py main) and accepted there by its judge
+POLICY_WEIGHTS = os.path.join(HERE, "policies", "density_mlp_large_scene.npy")
 
 
 def reduced_schedule(iterations):
@@ -73,13 +79,15 @@ def reduced_schedule(iterations):
 def psnr_gate(torch, iterations=6000, seeds=(0, 1), width=1600, height=1064, cap=1_200_000, forms=None):
     """Held-out PSNR of the plain form against the chosen form (bf16 SH storage
     with the fp32 SSIM gradient, exact culling, sparse Adam on the Morton order,
-    fast blend arithmetic, CUDA-graph steady state) and the precision form (bf16
-    SH storage, tensor-core SSIM) on the synthetic ring scene
+    fast blend arithmetic, CUDA-graph steady state), the chosen form with the
+    learned density policy and the precision form (bf16 SH storage, tensor-core
+    SSIM) on the synthetic ring scene
     (1.5M-Gaussian hidden model, 180 train / 20 held-out views, 100k initial
     points), each trained for `iterations` on the reduced schedule once per
     density seed. Returns the per-run and mean PSNRs (FP64, held-out views) and
-    the mean differences chosen - plain and precision - plain."""
-    forms = forms or {"plain": {}, "chosen": CHOSEN_FORM, "precision": PRECISION_FORM}
+    the mean differences of the other forms against plain."""
+    forms = forms or {"plain": {}, "chosen": CHOSEN_FORM, "precision": PRECISION_FORM,
+                      "chosen_learned": CHOSEN_LEARNED_FORM}
     args = argparse.Namespace(width=width, height=height, target=1_500_000, points=100_000)
     train, test, train_images, test_images, points, colors = build_scene(args, torch)
     runs = {k: [] for k in forms}
@@ -89,6 +97,8 @@ def psnr_gate(torch, iterations=6000, seeds=(0, 1), width=1600, height=1064, cap
                                                 **reduced_schedule(iterations), **switches)
             trainer = gsn.Trainer()
             assert trainer.initialize(train, train_images, points, colors, opts) == 0
+            if switches.get("learned_density"):
+                trainer.set_density_mlp(np.load(POLICY_WEIGHTS))
             t0 = time.time()
             assert trainer.train(iterations) == 0
             torch.cuda.synchronize()
@@ -107,6 +117,9 @@ def psnr_gate(torch, iterations=6000, seeds=(0, 1), width=1600, height=1064, cap
     if "plain" in mean and "precision" in mean:
         out.update(precision_db=round(mean["precision"], 4),
                    precision_delta_db=round(mean["precision"] - mean["plain"], 4))
+    if "plain" in mean and "chosen_learned" in mean:
+        out.update(chosen_learned_db=round(mean["chosen_learned"], 4),
+                   chosen_learned_delta_db=round(mean["chosen_learned"] - mean["plain"], 4))
     return out
 
 
