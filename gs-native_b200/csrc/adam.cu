@@ -24,11 +24,11 @@ namespace gsn {
 namespace {
 
 constexpr int kUpdateThreads = 256;
-// Staged precision-form update: a CTA's 48 bf16 SH rows of p, m and v in
-// shared memory (48 x 256 x 2 bytes per array).
+// Staged precision-form update: a CTA's 48 bf16 SH rows of m and v in shared
+// memory (48 x 256 x 2 bytes per array).
 constexpr uint32_t kStageRowBytes = kUpdateThreads * 2;
 constexpr uint32_t kStageArrayBytes = kShRows * kStageRowBytes;  // 24,576
-constexpr uint32_t kStageBytes = 3 * kStageArrayBytes;           // 73,728
+constexpr uint32_t kStageBytes = 2 * kStageArrayBytes;           // 49,152
 constexpr long long kStageWaitCycles = 2000000000LL;             // about a second
 
 // One arrival on the mbarrier that also announces `bytes` of bulk-copy traffic.
@@ -336,18 +336,17 @@ __device__ __forceinline__ void adam_rows_bf16(__nv_bfloat16* __restrict__ P, __
 }
 
 // kStaged (precision layout with Adam only; the host checks the alignment):
-// a full CTA with any Gaussian to update has thread 0 issue bulk copies of the
-// CTA's 48 SH rows of p (completing on bar[0]) and of m and v (bar[1]) into
-// shared memory at its start. The chain rule reads its SH coefficients from
-// the staged p rows, the SH Adam step reads all three staged arrays; the
-// geometry rows keep their per-thread loads. Every thread of a staged CTA waits
-// for both barriers (bounded) before any of them may return, so no copy is in
-// flight when the CTA ends; a wait that gives up sets the status and that CTA
-// falls back to the per-thread global loads.
+// a full CTA with any Gaussian to update has warp 0 issue bulk copies of the
+// CTA's 48 SH rows of m and v into shared memory at its start, completing on
+// one mbarrier; they land while the chain rule runs (the parameters keep their
+// per-thread loads). The SH Adam step reads the staged moments. Every thread
+// of a staged CTA waits for the barrier (bounded) before any of them may
+// return, so no copy is in flight when the CTA ends; a wait that gives up sets
+// the status and that CTA falls back to the per-thread global loads.
 template <int D, bool kBf16, bool kStaged>
 __global__ void __launch_bounds__(kUpdateThreads, 2) gaussian_update_kernel(GaussianUpdateArgs a) {
     extern __shared__ __align__(128) uint8_t stage[];
-    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ __align__(8) uint64_t bar[1];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n) return;
     const int64_t N = a.n;
@@ -358,7 +357,7 @@ __global__ void __launch_bounds__(kUpdateThreads, 2) gaussian_update_kernel(Gaus
     const bool visible = a.tile_counts[i] > 0;
     const gsn_camera cam = a.frame ? a.frame->cam : a.cam;
 
-    bool staged = false, p_ready = false, mv_ready = false;
+    bool staged = false, mv_ready = false;
     if constexpr (kStaged) {
         // a full CTA: no thread left at the count check above, so all reach the barriers
         if (static_cast<int64_t>(blockIdx.x + 1) * kUpdateThreads <= N) {
@@ -366,23 +365,18 @@ __global__ void __launch_bounds__(kUpdateThreads, 2) gaussian_update_kernel(Gaus
             if (staged) {
                 if (threadIdx.x == 0) {
                     tc::mbar_init(&bar[0], 1);
-                    tc::mbar_init(&bar[1], 1);
+                    mbar_expect_tx(&bar[0], kStageBytes);  // the one arrival, with all the bytes
                 }
                 __syncthreads();
-                if (threadIdx.x == 0) {
+                if (threadIdx.x < 32) {
+                    // warp 0: three rows per lane (lane l: rows l and l + 32 < 48 of m, of v)
                     const int64_t col = static_cast<int64_t>(blockIdx.x) * kUpdateThreads;
-                    const auto* sp = reinterpret_cast<const __nv_bfloat16*>(a.params + kGeometryRows * N) + col;
                     const auto* sm = reinterpret_cast<const __nv_bfloat16*>(a.m + kGeometryRows * N) + col;
                     const auto* sv = reinterpret_cast<const __nv_bfloat16*>(a.v + kGeometryRows * N) + col;
-                    mbar_expect_tx(&bar[0], kStageArrayBytes);
-                    for (int r = 0; r < kShRows; ++r)
-                        bulk_copy_to_smem(stage + r * kStageRowBytes, sp + r * N, kStageRowBytes, &bar[0]);
-                    mbar_expect_tx(&bar[1], 2 * kStageArrayBytes);
-                    for (int r = 0; r < kShRows; ++r) {
-                        bulk_copy_to_smem(stage + kStageArrayBytes + r * kStageRowBytes, sm + r * N, kStageRowBytes,
-                                          &bar[1]);
-                        bulk_copy_to_smem(stage + 2 * kStageArrayBytes + r * kStageRowBytes, sv + r * N,
-                                          kStageRowBytes, &bar[1]);
+                    for (int r = threadIdx.x; r < kShRows; r += 32) {
+                        bulk_copy_to_smem(stage + r * kStageRowBytes, sm + r * N, kStageRowBytes, &bar[0]);
+                        bulk_copy_to_smem(stage + kStageArrayBytes + r * kStageRowBytes, sv + r * N,
+                                          kStageRowBytes, &bar[0]);
                     }
                 }
             }
@@ -415,10 +409,6 @@ __global__ void __launch_bounds__(kUpdateThreads, 2) gaussian_update_kernel(Gaus
 #pragma unroll
     for (int k = 0; k < 9; ++k) active = active || in[k] != 0.0f;
     const __nv_bfloat16* sh_stage = nullptr;
-    if (kStaged && staged) {
-        p_ready = tc::mbar_wait(&bar[0], 0, kStageWaitCycles);
-        if (p_ready) sh_stage = reinterpret_cast<const __nv_bfloat16*>(stage);
-    }
     Chain ch;
     if (active) {
         chain_rule<D, kBf16>(a.params, N, i, cam, in, ch, sh_stage, threadIdx.x);
@@ -458,11 +448,10 @@ __global__ void __launch_bounds__(kUpdateThreads, 2) gaussian_update_kernel(Gaus
     }
     if (kStaged && staged) {
         // every thread waits for the copies before any may leave the CTA
-        mv_ready = tc::mbar_wait(&bar[1], 0, kStageWaitCycles);
-        if (!p_ready || !mv_ready) {
+        mv_ready = tc::mbar_wait(&bar[0], 0, kStageWaitCycles);
+        if (!mv_ready) {
             if (a.status) atomicExch(a.status, GSN_ERR_TIMEOUT);
-            if (!p_ready) tc::mbar_wait(&bar[0], 0, kStageWaitCycles);
-            if (!mv_ready) tc::mbar_wait(&bar[1], 0, kStageWaitCycles);
+            tc::mbar_wait(&bar[0], 0, kStageWaitCycles);
         }
     }
     // visibility-masked (sparse) Adam: a Gaussian outside the view keeps its
@@ -484,12 +473,12 @@ __global__ void __launch_bounds__(kUpdateThreads, 2) gaussian_update_kernel(Gaus
         const uint32_t seed = a.frame ? a.frame->seed : a.seed;
         rng = fmix32(static_cast<uint32_t>(i) * 0x9E3779B9u ^ fmix32(seed)) | 1u;
     }
-    if (kStaged && staged && p_ready && mv_ready) {
-        // SH rows from the staged copies; the same arithmetic and the same
-        // stochastic-rounding sequence as the per-thread path below
-        const auto* st_p = reinterpret_cast<const __nv_bfloat16*>(stage);
-        const auto* st_m = reinterpret_cast<const __nv_bfloat16*>(stage + kStageArrayBytes);
-        const auto* st_v = reinterpret_cast<const __nv_bfloat16*>(stage + 2 * kStageArrayBytes);
+    if (kStaged && staged && mv_ready) {
+        // SH moments from the staged copies, the parameters from global memory
+        // (cached: the chain rule has just read them); the same arithmetic and
+        // the same stochastic-rounding sequence as the per-thread path below
+        const auto* st_m = reinterpret_cast<const __nv_bfloat16*>(stage);
+        const auto* st_v = reinterpret_cast<const __nv_bfloat16*>(stage + kStageArrayBytes);
         auto* Pb = reinterpret_cast<__nv_bfloat16*>(P + kGeometryRows * N);
         auto* Mb = reinterpret_cast<__nv_bfloat16*>(M + kGeometryRows * N);
         auto* Vb = reinterpret_cast<__nv_bfloat16*>(V + kGeometryRows * N);
@@ -503,9 +492,9 @@ __global__ void __launch_bounds__(kUpdateThreads, 2) gaussian_update_kernel(Gaus
                 const int li = r * kUpdateThreads + threadIdx.x;
                 const float first = 0.9f * __bfloat162float(st_m[li]) + 0.1f * g;
                 const float second = 0.999f * __bfloat162float(st_v[li]) + 0.001f * g * g;
-                const float pn =
-                    __bfloat162float(st_p[li]) - __fdividef(lr * (first * c1), sqrt_approx(second * c2) + 1e-15f);
                 const int64_t idx = static_cast<int64_t>(r) * N + i;
+                const float pn =
+                    __bfloat162float(Pb[idx]) - __fdividef(lr * (first * c1), sqrt_approx(second * c2) + 1e-15f);
                 const uint32_t r1 = xorshift32(rng), r2 = xorshift32(rng);
                 Pb[idx] = bf16_stochastic(pn, r1);
                 Mb[idx] = bf16_stochastic(first, r1 >> 16);

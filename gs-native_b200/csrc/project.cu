@@ -147,9 +147,12 @@ __global__ void __launch_bounds__(256) emit_records_culled(const uint32_t* __res
         count = record_start[p + 1] - begin;
         id = sorted_ids[p];
         active = count > 0;
+        // past the capacity the overflow flag is set and the records that still
+        // fit are written (below), so every slot below min(total, capacity) -
+        // all the sort and the blend read - holds a record
         if (active && begin + static_cast<int64_t>(count) > capacity) {
             if (sub == 0 && overflow) atomicExch(overflow, 1);
-            active = false;
+            active = begin < capacity;
         }
     }
     int4 r = make_int4(0, 0, 0, 0);
@@ -175,7 +178,7 @@ __global__ void __launch_bounds__(256) emit_records_culled(const uint32_t* __res
         }
         const int group_total = __shfl_sync(0xffffffffu, incl, 3, 4);
         const int at = k + incl - w;
-        for (int j = 0; j < w && at + j < count; ++j) {
+        for (int j = 0; j < w && at + j < count && begin + at + j < capacity; ++j) {
             tile_keys[begin + at + j] = static_cast<uint32_t>(ty * tile_count_x + span.x + j);
             record_ids[begin + at + j] = id;
         }

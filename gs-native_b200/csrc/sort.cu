@@ -381,12 +381,16 @@ __global__ void __launch_bounds__(256) emit_records(const uint32_t* __restrict__
     if (count <= 0) return;
     if (begin + static_cast<int64_t>(count) > capacity) {
         if (sub == 0 && overflow) atomicExch(overflow, 1);
-        return;
+        if (begin >= capacity) return;
     }
     const uint32_t id = sorted_ids[p];
     const int4 r = rects[id];
     const int width = r.z - r.x;
-    for (int k = sub; k < count; k += 4) {
+    // past the capacity the overflow flag is set and the records that still fit
+    // are written, so every slot below min(total, capacity) - all the sort and
+    // the blend read - holds a record
+    const int fit = static_cast<int>(min(static_cast<int64_t>(count), capacity - begin));
+    for (int k = sub; k < fit; k += 4) {
         int ty = r.y + k / width;
         int tx = r.x + k % width;
         tile_keys[begin + k] = static_cast<uint32_t>(ty * tile_count_x + tx);

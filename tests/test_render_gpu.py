@@ -194,11 +194,27 @@ def test_fixed_record_capacity_and_overflow_flag():
     sync()
     assert t.equal(img_a, img_b)
     assert host(fixed.buffers().overflow, np.int32, 1)[0] == 0
-    small = gsn.Renderer()
-    assert small.set_record_capacity(records // 2) == 0
-    assert small.render(p.data_ptr(), n, cam, [1, 1, 1], img_b.data_ptr(), 3) == 0
-    sync()
-    assert host(small.buffers().overflow, np.int32, 1)[0] == 1
+    for culled in (False, True):
+        sizing = gsn.Renderer()
+        sizing.set_exact_culling(culled)
+        assert sizing.render(p.data_ptr(), n, cam, [1, 1, 1], img_b.data_ptr(), 3) == 0
+        sync()
+        total = sizing.buffers().record_count_host
+        small = gsn.Renderer()
+        small.set_exact_culling(culled)
+        assert small.set_record_capacity(total // 2) == 0
+        # a larger model first fills every record slot with ids up to 8,191 (its
+        # own render overflows too); the overflowing render of the 4,096 model
+        # must then rewrite every slot the lists read: a slot left unwritten
+        # below the capacity would keep an id of the first model
+        big = dev(scenes.random_gaussians(8192, 3))
+        assert small.render(big.data_ptr(), 8192, cam, [1, 1, 1], img_b.data_ptr(), 3) == 0
+        assert small.render(p.data_ptr(), n, cam, [1, 1, 1], img_b.data_ptr(), 3) == 0
+        sync()
+        assert host(small.buffers().overflow, np.int32, 1)[0] == 1
+        ids, offsets = gsn_sorted_lists(small, cam)
+        assert 0 < offsets[-1] <= total // 2
+        assert ids.max() < n
 
 
 def test_invalid_arguments_are_rejected():
