@@ -13,38 +13,12 @@
 // expression for expression, so for identical screen-space input the mapped
 // gradients are bit-identical to the reference's; Adam follows
 // UpdateGaussiansKernel (solver.cu:651-689).
-#include <mutex>
-
 #include "common.cuh"
 #include "kernels.h"
-#include "tcgen05.cuh"
 
 namespace gsn {
 
 namespace {
-
-constexpr int kUpdateThreads = 256;
-// Staged precision-form update: a CTA's 48 bf16 SH rows of m and v in shared
-// memory (48 x 256 x 2 bytes per array).
-constexpr uint32_t kStageRowBytes = kUpdateThreads * 2;
-constexpr uint32_t kStageArrayBytes = kShRows * kStageRowBytes;  // 24,576
-constexpr uint32_t kStageBytes = 2 * kStageArrayBytes;           // 49,152
-constexpr long long kStageWaitCycles = 2000000000LL;             // about a second
-
-// One arrival on the mbarrier that also announces `bytes` of bulk-copy traffic.
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc::smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-
-// 1-D bulk copy global -> this CTA's shared memory (no multicast), completing
-// its bytes on the mbarrier. Both addresses 16-byte aligned, bytes a multiple of 16.
-__device__ __forceinline__ void bulk_copy_to_smem(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     tc::smem_u32(dst)),
-                 "l"(src), "r"(bytes), "r"(tc::smem_u32(bar))
-                 : "memory");
-}
 
 struct Chain {
     float g[10];      // position 0-2, log-scale 3-5, axis-angle 6-8, opacity 9
@@ -54,8 +28,7 @@ struct Chain {
 
 template <int D, bool kBf16>
 __device__ __forceinline__ void sh_with_derivatives(const float* __restrict__ p, int64_t N, int i, const gsn_camera& cam,
-                                                    float* basis, float* color, float* dcol,
-                                                    const __nv_bfloat16* sh_stage, int li) {
+                                                    float* basis, float* color, float* dcol) {
     constexpr int s = (D + 1) * (D + 1);
     float dir[3];
 #pragma unroll
@@ -132,9 +105,7 @@ __device__ __forceinline__ void sh_with_derivatives(const float* __restrict__ p,
         float dv[3] = {0.0f, 0.0f, 0.0f};
 #pragma unroll
         for (int j = 0; j < s; ++j) {
-            // SH coefficient: from the CTA's staged rows when they are there
-            float coef = sh_stage ? __bfloat162float(sh_stage[(ch * kShStride + j) * kUpdateThreads + li])
-                                  : load_sh<kBf16>(p, N, ch * kShStride + j, i);
+            float coef = load_sh<kBf16>(p, N, ch * kShStride + j, i);
             value += coef * basis[j];
 #pragma unroll
             for (int a2 = 0; a2 < 3; ++a2) dv[a2] += coef * der[j * 3 + a2];
@@ -150,7 +121,7 @@ __device__ __forceinline__ void sh_with_derivatives(const float* __restrict__ p,
 // Chain rule of solver.cu:512-622 for one Gaussian with screen gradients in[0..8].
 template <int D, bool kBf16>
 __device__ __forceinline__ void chain_rule(const float* __restrict__ p, int64_t N, int i, const gsn_camera& cam,
-                                           const float in[9], Chain& out, const __nv_bfloat16* sh_stage, int li) {
+                                           const float in[9], Chain& out) {
     float rot[9], crot[9], cov[9], pos[3], s2[3];
     axis_angle_to_matrix(p[(GSN_ROTATION_INDEX + 0) * N + i], p[(GSN_ROTATION_INDEX + 1) * N + i],
                          p[(GSN_ROTATION_INDEX + 2) * N + i], rot);
@@ -192,7 +163,7 @@ __device__ __forceinline__ void chain_rule(const float* __restrict__ p, int64_t 
                 LP[r * 3 + c] += P[r * 3 + j] * crot[j * 3 + c];
             }
     float color[3], dcol[9];
-    sh_with_derivatives<D, kBf16>(p, N, i, cam, out.basis, color, dcol, sh_stage, li);
+    sh_with_derivatives<D, kBf16>(p, N, i, cam, out.basis, color, dcol);
     float right[3];
 #pragma unroll
     for (int axis = 0; axis < 3; ++axis) {
@@ -335,18 +306,8 @@ __device__ __forceinline__ void adam_rows_bf16(__nv_bfloat16* __restrict__ P, __
     }
 }
 
-// kStaged (precision layout with Adam only; the host checks the alignment):
-// a full CTA with any Gaussian to update has warp 0 issue bulk copies of the
-// CTA's 48 SH rows of m and v into shared memory at its start, completing on
-// one mbarrier; they land while the chain rule runs (the parameters keep their
-// per-thread loads). The SH Adam step reads the staged moments. Every thread
-// of a staged CTA waits for the barrier (bounded) before any of them may
-// return, so no copy is in flight when the CTA ends; a wait that gives up sets
-// the status and that CTA falls back to the per-thread global loads.
-template <int D, bool kBf16, bool kStaged>
-__global__ void __launch_bounds__(kUpdateThreads, 2) gaussian_update_kernel(GaussianUpdateArgs a) {
-    extern __shared__ __align__(128) uint8_t stage[];
-    __shared__ __align__(8) uint64_t bar[1];
+template <int D, bool kBf16>
+__global__ void __launch_bounds__(256, 2) gaussian_update_kernel(GaussianUpdateArgs a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n) return;
     const int64_t N = a.n;
@@ -356,32 +317,6 @@ __global__ void __launch_bounds__(kUpdateThreads, 2) gaussian_update_kernel(Gaus
     float adu = s2.y, adv = s2.z;
     const bool visible = a.tile_counts[i] > 0;
     const gsn_camera cam = a.frame ? a.frame->cam : a.cam;
-
-    bool staged = false, mv_ready = false;
-    if constexpr (kStaged) {
-        // a full CTA: no thread left at the count check above, so all reach the barriers
-        if (static_cast<int64_t>(blockIdx.x + 1) * kUpdateThreads <= N) {
-            staged = __syncthreads_or(!a.sparse || visible);
-            if (staged) {
-                if (threadIdx.x == 0) {
-                    tc::mbar_init(&bar[0], 1);
-                    mbar_expect_tx(&bar[0], kStageBytes);  // the one arrival, with all the bytes
-                }
-                __syncthreads();
-                if (threadIdx.x < 32) {
-                    // warp 0: three rows per lane (lane l: rows l and l + 32 < 48 of m, of v)
-                    const int64_t col = static_cast<int64_t>(blockIdx.x) * kUpdateThreads;
-                    const auto* sm = reinterpret_cast<const __nv_bfloat16*>(a.m + kGeometryRows * N) + col;
-                    const auto* sv = reinterpret_cast<const __nv_bfloat16*>(a.v + kGeometryRows * N) + col;
-                    for (int r = threadIdx.x; r < kShRows; r += 32) {
-                        bulk_copy_to_smem(stage + r * kStageRowBytes, sm + r * N, kStageRowBytes, &bar[0]);
-                        bulk_copy_to_smem(stage + kStageArrayBytes + r * kStageRowBytes, sv + r * N,
-                                          kStageRowBytes, &bar[0]);
-                    }
-                }
-            }
-        }
-    }
 
     // view-space statistics (solver.cu:468-490) and round accumulation
     // (density_controller.cu:280-295)
@@ -408,10 +343,9 @@ __global__ void __launch_bounds__(kUpdateThreads, 2) gaussian_update_kernel(Gaus
     bool active = false;
 #pragma unroll
     for (int k = 0; k < 9; ++k) active = active || in[k] != 0.0f;
-    const __nv_bfloat16* sh_stage = nullptr;
     Chain ch;
     if (active) {
-        chain_rule<D, kBf16>(a.params, N, i, cam, in, ch, sh_stage, threadIdx.x);
+        chain_rule<D, kBf16>(a.params, N, i, cam, in, ch);
     } else {
 #pragma unroll
         for (int k = 0; k < 10; ++k) ch.g[k] = 0.0f;
@@ -446,14 +380,6 @@ __global__ void __launch_bounds__(kUpdateThreads, 2) gaussian_update_kernel(Gaus
             for (int k = 0; k < kShStride; ++k)
                 a.grads_out[(GSN_SH_INDEX + c * kShStride + k) * N + i] = k < K ? ch.grgb[c] * ch.basis[k] : 0.0f;
     }
-    if (kStaged && staged) {
-        // every thread waits for the copies before any may leave the CTA
-        mv_ready = tc::mbar_wait(&bar[0], 0, kStageWaitCycles);
-        if (!mv_ready) {
-            if (a.status) atomicExch(a.status, GSN_ERR_TIMEOUT);
-            tc::mbar_wait(&bar[0], 0, kStageWaitCycles);
-        }
-    }
     // visibility-masked (sparse) Adam: a Gaussian outside the view keeps its
     // parameters and moments (no momentum step, no moment decay)
     if (!a.m || (a.sparse && !visible)) return;
@@ -472,36 +398,6 @@ __global__ void __launch_bounds__(kUpdateThreads, 2) gaussian_update_kernel(Gaus
     if constexpr (kBf16) {
         const uint32_t seed = a.frame ? a.frame->seed : a.seed;
         rng = fmix32(static_cast<uint32_t>(i) * 0x9E3779B9u ^ fmix32(seed)) | 1u;
-    }
-    if (kStaged && staged && mv_ready) {
-        // SH moments from the staged copies, the parameters from global memory
-        // (cached: the chain rule has just read them); the same arithmetic and
-        // the same stochastic-rounding sequence as the per-thread path below
-        const auto* st_m = reinterpret_cast<const __nv_bfloat16*>(stage);
-        const auto* st_v = reinterpret_cast<const __nv_bfloat16*>(stage + kStageArrayBytes);
-        auto* Pb = reinterpret_cast<__nv_bfloat16*>(P + kGeometryRows * N);
-        auto* Mb = reinterpret_cast<__nv_bfloat16*>(M + kGeometryRows * N);
-        auto* Vb = reinterpret_cast<__nv_bfloat16*>(V + kGeometryRows * N);
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-#pragma unroll
-            for (int k = 0; k < kShStride; ++k) {
-                const int r = c * kShStride + k;
-                const float g = k < K ? ch.grgb[c] * ch.basis[k] : 0.0f;
-                const float lr = k == 0 ? a.lr[4] : a.lr[5];
-                const int li = r * kUpdateThreads + threadIdx.x;
-                const float first = 0.9f * __bfloat162float(st_m[li]) + 0.1f * g;
-                const float second = 0.999f * __bfloat162float(st_v[li]) + 0.001f * g * g;
-                const int64_t idx = static_cast<int64_t>(r) * N + i;
-                const float pn =
-                    __bfloat162float(Pb[idx]) - __fdividef(lr * (first * c1), sqrt_approx(second * c2) + 1e-15f);
-                const uint32_t r1 = xorshift32(rng), r2 = xorshift32(rng);
-                Pb[idx] = bf16_stochastic(pn, r1);
-                Mb[idx] = bf16_stochastic(first, r1 >> 16);
-                Vb[idx] = bf16_stochastic(second, r2);
-            }
-        }
-        return;
     }
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -557,58 +453,23 @@ __global__ void remap_moments_kernel(const int* __restrict__ parents, const floa
 
 }  // namespace
 
-// Opt-in to the staged kernels' shared memory, once per device.
-static bool configure_staged_update() {
-    static std::mutex mutex;
-    static bool configured[64] = {};
-    int device = 0;
-    if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= 64) return false;
-    std::lock_guard<std::mutex> lock(mutex);
-    if (configured[device]) return true;
-    const int bytes = static_cast<int>(kStageBytes);
-    if (cudaFuncSetAttribute(gaussian_update_kernel<0, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             bytes) != cudaSuccess ||
-        cudaFuncSetAttribute(gaussian_update_kernel<1, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             bytes) != cudaSuccess ||
-        cudaFuncSetAttribute(gaussian_update_kernel<2, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             bytes) != cudaSuccess ||
-        cudaFuncSetAttribute(gaussian_update_kernel<3, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             bytes) != cudaSuccess)
-        return false;
-    configured[device] = true;
-    return true;
-}
-
 int launch_gaussian_update(const GaussianUpdateArgs& a, int sh_degree, cudaStream_t stream) {
     if (a.n <= 0) return GSN_OK;
-    dim3 grid(ceil_div(a.n, kUpdateThreads));
+    dim3 grid(ceil_div(a.n, 256));
     const int d = sh_degree < 0 ? 0 : (sh_degree > 3 ? 3 : sh_degree);
-    auto aligned16 = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
-    // staged: the SH rows' byte offsets (40 N + 2 N r) and the CTA's 512-byte
-    // slices are 16-byte aligned when N is a multiple of 8
-    const bool staged = a.bf16_sh && a.m && a.v && a.n % 8 == 0 && aligned16(a.params) && aligned16(a.m) &&
-                        aligned16(a.v);
-    if (staged) {
-        if (!configure_staged_update()) return GSN_ERR_CUDA;
+    if (a.bf16_sh) {
         switch (d) {
-            case 0: gaussian_update_kernel<0, true, true><<<grid, kUpdateThreads, kStageBytes, stream>>>(a); break;
-            case 1: gaussian_update_kernel<1, true, true><<<grid, kUpdateThreads, kStageBytes, stream>>>(a); break;
-            case 2: gaussian_update_kernel<2, true, true><<<grid, kUpdateThreads, kStageBytes, stream>>>(a); break;
-            default: gaussian_update_kernel<3, true, true><<<grid, kUpdateThreads, kStageBytes, stream>>>(a); break;
-        }
-    } else if (a.bf16_sh) {
-        switch (d) {
-            case 0: gaussian_update_kernel<0, true, false><<<grid, kUpdateThreads, 0, stream>>>(a); break;
-            case 1: gaussian_update_kernel<1, true, false><<<grid, kUpdateThreads, 0, stream>>>(a); break;
-            case 2: gaussian_update_kernel<2, true, false><<<grid, kUpdateThreads, 0, stream>>>(a); break;
-            default: gaussian_update_kernel<3, true, false><<<grid, kUpdateThreads, 0, stream>>>(a); break;
+            case 0: gaussian_update_kernel<0, true><<<grid, 256, 0, stream>>>(a); break;
+            case 1: gaussian_update_kernel<1, true><<<grid, 256, 0, stream>>>(a); break;
+            case 2: gaussian_update_kernel<2, true><<<grid, 256, 0, stream>>>(a); break;
+            default: gaussian_update_kernel<3, true><<<grid, 256, 0, stream>>>(a); break;
         }
     } else {
         switch (d) {
-            case 0: gaussian_update_kernel<0, false, false><<<grid, kUpdateThreads, 0, stream>>>(a); break;
-            case 1: gaussian_update_kernel<1, false, false><<<grid, kUpdateThreads, 0, stream>>>(a); break;
-            case 2: gaussian_update_kernel<2, false, false><<<grid, kUpdateThreads, 0, stream>>>(a); break;
-            default: gaussian_update_kernel<3, false, false><<<grid, kUpdateThreads, 0, stream>>>(a); break;
+            case 0: gaussian_update_kernel<0, false><<<grid, 256, 0, stream>>>(a); break;
+            case 1: gaussian_update_kernel<1, false><<<grid, 256, 0, stream>>>(a); break;
+            case 2: gaussian_update_kernel<2, false><<<grid, 256, 0, stream>>>(a); break;
+            default: gaussian_update_kernel<3, false><<<grid, 256, 0, stream>>>(a); break;
         }
     }
     return launched(1);

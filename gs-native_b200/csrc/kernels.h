@@ -231,12 +231,7 @@ struct GaussianUpdateArgs {
     float* depth_sum;
     float* depth_sq;
     float4* last_grad;
-    int* status;              // optional: set to GSN_ERR_TIMEOUT if a staging wait gave up
 };
-// Precision layout with Adam, N a multiple of 8 and 16-byte aligned blocks:
-// each full CTA stages its Gaussians' SH rows of p, m and v into shared memory
-// with 1-D bulk copies issued at its start (no registers held while they are in
-// flight); every other case takes the per-thread loads.
 int launch_gaussian_update(const GaussianUpdateArgs& a, int sh_degree, cudaStream_t stream);
 
 // Adam history gather after densification: row r of the new moments takes the

@@ -182,13 +182,6 @@ bool Solver::UpdateGaussians(const CameraParams& camera, const Renderer& rendere
     a.frame = frame_;
     a.bf16_sh = bf16_sh_;
     a.sparse = sparse_adam_;
-    if (bf16_sh_ && adam) {
-        // the staged precision-form update reports a staging wait that gave up here
-        if (!status_.get() &&
-            (!status_.Reserve(1) || cudaMemsetAsync(status_.get(), 0, sizeof(int), stream_) != cudaSuccess))
-            return false;
-        a.status = status_.get();
-    }
     a.seed = static_cast<uint32_t>(iteration);
     gsn::stage_mark(stream_, gsn::kStageGaussianUpdate);
     if (gsn::launch_gaussian_update(a, std::clamp(sh_degree, 0, 3), stream_) != GSN_OK) return false;

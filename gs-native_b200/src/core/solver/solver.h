@@ -107,8 +107,7 @@ public:
     void SetSparseAdam(bool enabled) { sparse_adam_ = enabled; }
     bool GetSparseAdam() const { return sparse_adam_; }
     bool GetTensorCoreLoss() const { return tensor_core_loss_; }
-    // Device status word of the tensor-core passes and of the staged
-    // precision-form update: 0, or GSN_ERR_TIMEOUT.
+    // Device status word of the tensor-core passes: 0, or GSN_ERR_TIMEOUT.
     const int* GetStatusDevice() const { return status_.get(); }
     void SetIteration(uint64_t iteration) { iteration_ = iteration; }
 
