@@ -103,9 +103,11 @@ __device__ __forceinline__ void sh_with_derivatives(const float* __restrict__ p,
     for (int ch = 0; ch < 3; ++ch) {
         float value = 0.0f;
         float dv[3] = {0.0f, 0.0f, 0.0f};
+        float coefs[s];
+        load_sh_coefs<kBf16, s>(p, N, ch * kShStride, i, coefs);
 #pragma unroll
         for (int j = 0; j < s; ++j) {
-            float coef = load_sh<kBf16>(p, N, ch * kShStride + j, i);
+            const float coef = coefs[j];
             value += coef * basis[j];
 #pragma unroll
             for (int a2 = 0; a2 < 3; ++a2) dv[a2] += coef * der[j * 3 + a2];
@@ -274,35 +276,46 @@ __device__ __forceinline__ void adam_rows(float* __restrict__ P, float* __restri
     }
 }
 
-// Precision form: the same step on bf16 rows (SH parameters and their
-// moments), computed in fp32 and written back with stochastic rounding.
-template <int CNT>
-__device__ __forceinline__ void adam_rows_bf16(__nv_bfloat16* __restrict__ P, __nv_bfloat16* __restrict__ M,
-                                               __nv_bfloat16* __restrict__ V, int64_t N, int i, int row0,
-                                               const float* g, const float* lr, float c1, float c2, uint32_t& rng) {
-    float p[CNT], m[CNT], v[CNT];
+// Precision form: the same step on bf16 SH pair rows (two coefficients of a
+// Gaussian per 32-bit word, the parameters and both moments), computed in fp32
+// and written back with stochastic rounding; coefficient by coefficient the
+// noise stream is the one a row-by-row pass draws.
+template <int PAIRS>
+__device__ __forceinline__ void adam_pairs_bf16(uint32_t* __restrict__ P, uint32_t* __restrict__ M,
+                                                uint32_t* __restrict__ V, int64_t N, int i, int pair0,
+                                                const float* g, const float* lr, float c1, float c2, uint32_t& rng) {
+    // all of the group's words first (three per pair), so they are in flight
+    // together; then pair by pair: widen, step, round, narrow, store
+    uint32_t pw[PAIRS], mw[PAIRS], vw[PAIRS];
 #pragma unroll
-    for (int r = 0; r < CNT; ++r) {
-        const int64_t idx = static_cast<int64_t>(row0 + r) * N + i;
-        p[r] = __bfloat162float(P[idx]);
-        m[r] = __bfloat162float(M[idx]);
-        v[r] = __bfloat162float(V[idx]);
+    for (int q = 0; q < PAIRS; ++q) {
+        const int64_t idx = static_cast<int64_t>(pair0 + q) * N + i;
+        pw[q] = P[idx];
+        mw[q] = M[idx];
+        vw[q] = V[idx];
     }
 #pragma unroll
-    for (int r = 0; r < CNT; ++r) {
-        float first = 0.9f * m[r] + 0.1f * g[r];
-        float second = 0.999f * v[r] + 0.001f * g[r] * g[r];
-        m[r] = first;
-        v[r] = second;
-        p[r] -= __fdividef(lr[r] * (first * c1), sqrt_approx(second * c2) + 1e-15f);
-    }
+    for (int q = 0; q < PAIRS; ++q) {
+        uint32_t bits[3] = {0u, 0u, 0u};
 #pragma unroll
-    for (int r = 0; r < CNT; ++r) {
-        const int64_t idx = static_cast<int64_t>(row0 + r) * N + i;
-        const uint32_t r1 = xorshift32(rng), r2 = xorshift32(rng);
-        P[idx] = bf16_stochastic(p[r], r1);
-        M[idx] = bf16_stochastic(m[r], r1 >> 16);
-        V[idx] = bf16_stochastic(v[r], r2);
+        for (int h = 0; h < 2; ++h) {
+            const int r = 2 * q + h;
+            float p = h ? bf16_hi(pw[q]) : bf16_lo(pw[q]);
+            const float m = h ? bf16_hi(mw[q]) : bf16_lo(mw[q]);
+            const float v = h ? bf16_hi(vw[q]) : bf16_lo(vw[q]);
+            const float first = 0.9f * m + 0.1f * g[r];
+            const float second = 0.999f * v + 0.001f * g[r] * g[r];
+            p -= __fdividef(lr[r] * (first * c1), sqrt_approx(second * c2) + 1e-15f);
+            const uint32_t r1 = xorshift32(rng), r2 = xorshift32(rng);
+            const int shift = 16 * h;
+            bits[0] |= static_cast<uint32_t>(__bfloat16_as_ushort(bf16_stochastic(p, r1))) << shift;
+            bits[1] |= static_cast<uint32_t>(__bfloat16_as_ushort(bf16_stochastic(first, r1 >> 16))) << shift;
+            bits[2] |= static_cast<uint32_t>(__bfloat16_as_ushort(bf16_stochastic(second, r2))) << shift;
+        }
+        const int64_t idx = static_cast<int64_t>(pair0 + q) * N + i;
+        P[idx] = bits[0];
+        M[idx] = bits[1];
+        V[idx] = bits[2];
     }
 }
 
@@ -391,55 +404,51 @@ __global__ void __launch_bounds__(256, 2) gaussian_update_kernel(GaussianUpdateA
     const float c2 = a.frame ? a.frame->c2 : a.c2;
     const float lr_geo[10] = {lr0, lr0, lr0, a.lr[1], a.lr[1], a.lr[1], a.lr[2], a.lr[2], a.lr[2], a.lr[3]};
     adam_rows<10>(P, M, V, N, i, 0, ch.g, lr_geo, c1, c2);
-    float lr_sh[8];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) lr_sh[k] = a.lr[5];
-    uint32_t rng = 0;
     if constexpr (kBf16) {
+        // one group per colour channel: its 16 coefficients are 8 pair words
+        // per array, the bytes in flight of the fp32 form's 8-row groups
         const uint32_t seed = a.frame ? a.frame->seed : a.seed;
-        rng = fmix32(static_cast<uint32_t>(i) * 0x9E3779B9u ^ fmix32(seed)) | 1u;
-    }
+        uint32_t rng = fmix32(static_cast<uint32_t>(i) * 0x9E3779B9u ^ fmix32(seed)) | 1u;
+        float lr_sh[kShStride];
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
+        for (int k = 0; k < kShStride; ++k) lr_sh[k] = k == 0 ? a.lr[4] : a.lr[5];
 #pragma unroll
-        for (int half = 0; half < 2; ++half) {
-            float g8[8];
+        for (int c = 0; c < 3; ++c) {
+            float g16[kShStride];
 #pragma unroll
-            for (int k = 0; k < 8; ++k) g8[k] = half * 8 + k < K ? ch.grgb[c] * ch.basis[half * 8 + k] : 0.0f;
-            lr_sh[0] = half == 0 ? a.lr[4] : a.lr[5];
-            if constexpr (kBf16) {
-                auto* Pb = reinterpret_cast<__nv_bfloat16*>(P + kGeometryRows * N);
-                auto* Mb = reinterpret_cast<__nv_bfloat16*>(M + kGeometryRows * N);
-                auto* Vb = reinterpret_cast<__nv_bfloat16*>(V + kGeometryRows * N);
-                adam_rows_bf16<8>(Pb, Mb, Vb, N, i, c * kShStride + half * 8, g8, lr_sh, c1, c2, rng);
-            } else {
+            for (int k = 0; k < kShStride; ++k) g16[k] = k < K ? ch.grgb[c] * ch.basis[k] : 0.0f;
+            adam_pairs_bf16<kShStride / 2>(reinterpret_cast<uint32_t*>(P), reinterpret_cast<uint32_t*>(M),
+                                           reinterpret_cast<uint32_t*>(V), N, i,
+                                           kGeometryRows + c * (kShStride / 2), g16, lr_sh, c1, c2, rng);
+        }
+    } else {
+        float lr_sh[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) lr_sh[k] = a.lr[5];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+#pragma unroll
+            for (int half = 0; half < 2; ++half) {
+                float g8[8];
+#pragma unroll
+                for (int k = 0; k < 8; ++k) g8[k] = half * 8 + k < K ? ch.grgb[c] * ch.basis[half * 8 + k] : 0.0f;
+                lr_sh[0] = half == 0 ? a.lr[4] : a.lr[5];
                 adam_rows<8>(P, M, V, N, i, GSN_SH_INDEX + c * kShStride + half * 8, g8, lr_sh, c1, c2);
             }
         }
     }
 }
 
-template <bool kBf16>
+// One 32-bit word per (physical row, Gaussian): an fp32 value, or a pair of
+// bf16 SH moments in the precision layout (zero bits are two bf16 zeros).
 __global__ void remap_moments_kernel(const int* __restrict__ parents, const float* __restrict__ prev_m,
                                      const float* __restrict__ prev_v, float* __restrict__ m, float* __restrict__ v,
                                      int prev_count, int count) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
-    const int row = blockIdx.y;  // logical row 0..57
+    const int row = blockIdx.y;  // physical row
     const int parent = parents ? parents[i] : -1;
     const bool take = parent >= 0 && parent < prev_count;
-    if (kBf16 && row >= kGeometryRows) {
-        const int k = row - kGeometryRows;
-        const auto* pm = reinterpret_cast<const __nv_bfloat16*>(prev_m + kGeometryRows * static_cast<int64_t>(prev_count));
-        const auto* pv = reinterpret_cast<const __nv_bfloat16*>(prev_v + kGeometryRows * static_cast<int64_t>(prev_count));
-        auto* dm = reinterpret_cast<__nv_bfloat16*>(m + kGeometryRows * static_cast<int64_t>(count));
-        auto* dv = reinterpret_cast<__nv_bfloat16*>(v + kGeometryRows * static_cast<int64_t>(count));
-        const int64_t dst = static_cast<int64_t>(k) * count + i;
-        const int64_t src = static_cast<int64_t>(k) * prev_count + parent;
-        dm[dst] = take ? pm[src] : __float2bfloat16_rn(0.0f);
-        dv[dst] = take ? pv[src] : __float2bfloat16_rn(0.0f);
-        return;
-    }
     const int64_t dst = static_cast<int64_t>(row) * count + i;
     if (take) {
         const int64_t src = static_cast<int64_t>(row) * prev_count + parent;
@@ -478,9 +487,8 @@ int launch_gaussian_update(const GaussianUpdateArgs& a, int sh_degree, cudaStrea
 int launch_remap_moments(const int* parents, const float* prev_m, const float* prev_v, float* m, float* v,
                          int prev_count, int count, bool bf16_sh, cudaStream_t stream) {
     if (count <= 0) return GSN_OK;
-    dim3 grid(ceil_div(count, 256), kParams);
-    if (bf16_sh) remap_moments_kernel<true><<<grid, 256, 0, stream>>>(parents, prev_m, prev_v, m, v, prev_count, count);
-    else remap_moments_kernel<false><<<grid, 256, 0, stream>>>(parents, prev_m, prev_v, m, v, prev_count, count);
+    dim3 grid(ceil_div(count, 256), bf16_sh ? kPrecisionPhysicalRows : kParams);
+    remap_moments_kernel<<<grid, 256, 0, stream>>>(parents, prev_m, prev_v, m, v, prev_count, count);
     return launched(1);
 }
 

@@ -52,23 +52,50 @@ inline int launched(int kernels) {
 // ---------------------------------------------------------------- layouts
 // Parameter block layouts. The plain form uses the reference's 58 fp32 rows of
 // stride N. The precision form keeps the 10 geometry rows (position, log-scale,
-// axis-angle, opacity logit) in fp32 and stores the 48 SH rows as bf16 rows of
-// stride N right after them, so its block is 10 + 24 = 34 float rows. Adam's
-// moments use the same layout as the parameters.
+// axis-angle, opacity logit) in fp32 and stores the 48 SH coefficients in bf16
+// as 24 pair rows right after them: pair row r holds coefficients 2r (low 16
+// bits) and 2r + 1 (high 16 bits) of Gaussian i in the 32-bit word r * N + i,
+// so its block is 10 + 24 = 34 rows of 32-bit words of stride N, and every SH
+// load or store moves 4 bytes per Gaussian like an fp32 row. Adam's moments use
+// the same layout as the parameters.
 constexpr int kGeometryRows = GSN_SH_INDEX;  // 10
 constexpr int kShRows = 3 * kShStride;       // 48
-constexpr int kPrecisionPhysicalRows = kGeometryRows + kShRows / 2;  // 34
+constexpr int kShPairRows = kShRows / 2;     // 24
+constexpr int kPrecisionPhysicalRows = kGeometryRows + kShPairRows;  // 34
 
 template <bool kBf16>
 __host__ __device__ constexpr int physical_rows() { return kBf16 ? kPrecisionPhysicalRows : kParams; }
 
+// bf16 bits <-> fp32 (bf16 is the upper half of an fp32: exact widening).
+__device__ __forceinline__ float bf16_lo(uint32_t w) { return __uint_as_float(w << 16); }
+__device__ __forceinline__ float bf16_hi(uint32_t w) { return __uint_as_float(w & 0xffff0000u); }
+
+// SH coefficient k (0..47, channel-major) of Gaussian i.
 template <bool kBf16>
 __device__ __forceinline__ float load_sh(const float* block, int64_t n, int k, int64_t i) {
     if constexpr (kBf16) {
-        const __nv_bfloat16* sh = reinterpret_cast<const __nv_bfloat16*>(block + kGeometryRows * n);
-        return __bfloat162float(sh[k * n + i]);
+        const uint32_t w = reinterpret_cast<const uint32_t*>(block)[(kGeometryRows + (k >> 1)) * n + i];
+        return (k & 1) ? bf16_hi(w) : bf16_lo(w);
     } else {
         return block[(kGeometryRows + k) * n + i];
+    }
+}
+
+// The K coefficients k0 .. k0 + K - 1 (k0 even) of Gaussian i, one 32-bit load
+// per pair in the precision layout.
+template <bool kBf16, int K>
+__device__ __forceinline__ void load_sh_coefs(const float* block, int64_t n, int k0, int64_t i, float* out) {
+    if constexpr (kBf16) {
+        const uint32_t* words = reinterpret_cast<const uint32_t*>(block);
+#pragma unroll
+        for (int q = 0; 2 * q < K; ++q) {
+            const uint32_t w = words[(kGeometryRows + (k0 >> 1) + q) * n + i];
+            out[2 * q] = bf16_lo(w);
+            if (2 * q + 1 < K) out[2 * q + 1] = bf16_hi(w);
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < K; ++k) out[k] = block[(kGeometryRows + k0 + k) * n + i];
     }
 }
 

@@ -337,7 +337,7 @@ __global__ void samples_kernel(const int* __restrict__ control, float* __restric
 
 // density_controller.cu:168-243 (children) and 245-278 (parent ids, new flags,
 // statistics reset), fused: one thread per source Gaussian. kBf16: precision-form
-// layout (the 48 SH rows are bf16 and are copied bit for bit).
+// layout (34 physical rows).
 template <bool kBf16>
 __global__ void write_kernel(const float* __restrict__ params, const int4* __restrict__ counts,
                              const int4* __restrict__ offsets, const int* __restrict__ control,
@@ -389,13 +389,9 @@ __global__ void write_kernel(const float* __restrict__ params, const int4* __res
             atomicExch(const_cast<int*>(control) + 2, 1);
             return;
         }
-        if constexpr (kBf16) {
-            const auto* in_sh = reinterpret_cast<const __nv_bfloat16*>(params + kGeometryRows * N);
-            auto* out_sh = reinterpret_cast<__nv_bfloat16*>(out + kGeometryRows * static_cast<int64_t>(out_stride));
-            for (int k = 0; k < kShRows; ++k)
-                out_sh[static_cast<int64_t>(k) * out_stride + dst] = in_sh[static_cast<int64_t>(k) * N + id];
-        }
-        for (int p = 0; p < (kBf16 ? kGeometryRows : kParams); ++p) {
+        // every physical row is one 32-bit word per Gaussian; the SH rows (bf16
+        // pairs in the precision layout) are copied bit for bit
+        for (int p = 0; p < physical_rows<kBf16>(); ++p) {
             float value = params[static_cast<int64_t>(p) * N + id];
             if (split && p < GSN_POSITION_INDEX + 3) {
                 float delta = 0;

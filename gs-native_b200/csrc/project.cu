@@ -307,9 +307,11 @@ __global__ void __launch_bounds__(256) project_kernel(const float* __restrict__ 
     float rgb[3];
 #pragma unroll
     for (int ch = 0; ch < 3; ++ch) {
+        float coef[K];
+        load_sh_coefs<kBf16, K>(params, N, ch * kShStride, i, coef);
         float value = 0.0f;
 #pragma unroll
-        for (int k = 0; k < K; ++k) value += basis[k] * load_sh<kBf16>(params, N, ch * kShStride + k, i);
+        for (int k = 0; k < K; ++k) value += basis[k] * coef[k];
         rgb[ch] = fmaxf(value + 0.5f, 0.0f);
     }
     out.colors[i] = make_float3(rgb[0], rgb[1], rgb[2]);

@@ -34,8 +34,13 @@
 //     fast_record), takes a pixel on one compare and divides by (1 - alpha)
 //     through the hardware reciprocal; the exact form keeps the reference's
 //     power expression, expf and the correctly rounded reciprocal;
+//   * the fast form runs the four pixels as two pairs in packed FP32x2
+//     arithmetic (raster_common.cuh fma2/mul2/add2, one instruction per two
+//     operations), since the loop is bound by instruction issue (the alpha
+//     test, clamp and MUFU operations stay per pixel); its transmittance
+//     update T - alpha T is the fast forward's expression;
 //   * at most 80 registers (12 CTAs, 24 warps per SM): the exact form uses 80,
-//     the fast form 66.
+//     the fast form 67.
 // Per-Gaussian output (12 floats, Gaussian-major): d(u, v), d(cov a, b, c),
 // d(opacity logit), d(r, g, b), sum|du|, sum|dv|, 0.
 #include "raster_common.cuh"
@@ -109,6 +114,16 @@ __global__ void __launch_bounds__(kRasterThreads, 12) raster_backward_kernel(Ras
         my_bound = max(my_bound, limit[p]);
         if (kFast) P[p] = -S[p];
     }
+    // fast form: the pixels as two packed pairs (2h, 2h + 1)
+    float2 nfy2[2], T2[2], P2[2], gI2[2][3];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        nfy2[h] = make_float2(-fy[2 * h], -fy[2 * h + 1]);
+        T2[h] = pk(1.0f);
+        P2[h] = make_float2(P[2 * h], P[2 * h + 1]);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) gI2[h][c] = make_float2(gI[2 * h][c], gI[2 * h + 1][c]);
+    }
     // the warp's replay ends at its pixels' largest bound, the CTA's at its own
     const int warp_bound = __reduce_max_sync(0xffffffffu, my_bound);
     if (t == 0) s_bound = 0;
@@ -176,39 +191,54 @@ __global__ void __launch_bounds__(kRasterThreads, 12) raster_backward_kernel(Ras
                 // dependency chains interleave; a pixel that does not take the
                 // record gets alpha = 0, which zeroes its contributions
                 if constexpr (kFast) {
+                    // the two pixel pairs in packed FP32x2 arithmetic; the alpha
+                    // test, clamp and the MUFU operations stay per pixel
                     const float4 kf = s_fast[j];
                     const float Ax = fmaf(kf.x * dx, dx, kf.w), Bx = kf.y * dx;
+                    const float2 m1 = pk(-1.0f), one = pk(1.0f);
+                    float2 acc[9];
 #pragma unroll
-                    for (int p = 0; p < kPixPerThread; ++p) {
-                        const float dy = mu.y - fy[p];
-                        const float pw2 = fmaf(fmaf(kf.z, dy, Bx), dy, Ax);
-                        const bool take = idx < limit[p] && pw2 >= kLog2AlphaMin;
-                        const float raw = ex2_approx(pw2);
-                        const float alpha = take ? fminf(kAlphaMax, raw) : 0.0f;
+                    for (int i = 0; i < 9; ++i) acc[i] = pk(0.0f);
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const float2 dy = add2(pk(mu.y), nfy2[h]);
+                        const float2 pw2 = fma2(fma2(pk(kf.z), dy, pk(Bx)), dy, pk(Ax));
+                        const bool take0 = idx < limit[2 * h] && pw2.x >= kLog2AlphaMin;
+                        const bool take1 = idx < limit[2 * h + 1] && pw2.y >= kLog2AlphaMin;
+                        float2 alpha;
+                        alpha.x = take0 ? fminf(kAlphaMax, ex2_approx(pw2.x)) : 0.0f;
+                        alpha.y = take1 ? fminf(kAlphaMax, ex2_approx(pw2.y)) : 0.0f;
                         // d alpha / d power: raw below the clamp, 0 when clamped or not taken
-                        const float r = alpha < kAlphaMax ? alpha : 0.0f;
-                        const float w = alpha * T[p];
-                        const float inv = one_over<true>(1.0f - alpha);
-                        const float G = gI[p][0] * cc[0] + gI[p][1] * cc[1] + gI[p][2] * cc[2];
+                        const float2 r = make_float2(alpha.x < kAlphaMax ? alpha.x : 0.0f,
+                                                     alpha.y < kAlphaMax ? alpha.y : 0.0f);
+                        const float2 w = mul2(alpha, T2[h]);
+                        const float2 om = fma2(alpha, m1, one);  // 1 - alpha
+                        const float2 inv = make_float2(one_over<true>(om.x), one_over<true>(om.y));
+                        float2 G = mul2(gI2[h][0], pk(cc[0]));
+                        G = fma2(gI2[h][1], pk(cc[1]), G);
+                        G = fma2(gI2[h][2], pk(cc[2]), G);
                         // dL/dalpha = (dL/dC . (colour in front + T c - final)) / (1 - alpha)
-                        const float dalpha = fmaf(T[p], G, P[p]) * inv;
+                        const float2 dalpha = mul2(fma2(T2[h], G, P2[h]), inv);
 #pragma unroll
-                        for (int c = 0; c < 3; ++c) v[6 + c] = fmaf(w, gI[p][c], v[6 + c]);
-                        const float common = dalpha * r;
-                        const float qx = fmaf(q.y, dy, qxdx);
-                        const float qy = fmaf(q.z, dy, qydx);
-                        const float cqx = common * qx, cqy = common * qy;
-                        v[0] -= cqx;
-                        v[1] -= cqy;
-                        v[2] = fmaf(cqx, qx, v[2]);  // halved once per record below
-                        v[3] = fmaf(cqx, qy, v[3]);
-                        v[4] = fmaf(cqy, qy, v[4]);  // halved once per record below
-                        v[5] += common;             // times (1 - o) once per record below
-                        v[9] += fabsf(cqx);
-                        v[10] += fabsf(cqy);
-                        P[p] = fmaf(w, G, P[p]);
-                        T[p] = fmaf(-T[p], alpha, T[p]);
+                        for (int c = 0; c < 3; ++c) acc[6 + c] = fma2(w, gI2[h][c], acc[6 + c]);
+                        const float2 common = mul2(dalpha, r);
+                        const float2 qx = fma2(pk(q.y), dy, pk(qxdx));
+                        const float2 qy = fma2(pk(q.z), dy, pk(qydx));
+                        const float2 cqx = mul2(common, qx), cqy = mul2(common, qy);
+                        acc[0] = fma2(cqx, m1, acc[0]);
+                        acc[1] = fma2(cqy, m1, acc[1]);
+                        acc[2] = fma2(cqx, qx, acc[2]);  // halved once per record below
+                        acc[3] = fma2(cqx, qy, acc[3]);
+                        acc[4] = fma2(cqy, qy, acc[4]);  // halved once per record below
+                        acc[5] = add2(acc[5], common);   // times (1 - o) once per record below
+                        v[9] += fabsf(cqx.x) + fabsf(cqx.y);
+                        v[10] += fabsf(cqy.x) + fabsf(cqy.y);
+                        P2[h] = fma2(w, G, P2[h]);
+                        // T (1 - alpha) as T - alpha T, the forward's expression
+                        T2[h] = fma2(w, m1, T2[h]);
                     }
+#pragma unroll
+                    for (int i = 0; i < 9; ++i) v[i] = acc[i].x + acc[i].y;
                 } else {
                     const Power<false> power(q, dx);
                     const float lim = s_floor[j];

@@ -144,6 +144,15 @@ __device__ __forceinline__ float ex2_approx(float x) {
     return y;
 }
 
+// Packed FP32x2 arithmetic (sm_100: one instruction performs two IEEE
+// round-to-nearest operations, each rounded as its scalar form). The fast forms
+// evaluate a thread's four pixels as two pairs (pixels 2h and 2h + 1) with
+// these, which halves the issue slots of their per-pixel arithmetic.
+__device__ __forceinline__ float2 pk(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+
 // Does the box of a record overlap the pixel rectangle [x0, x1] x [y0, y1]?
 __device__ __forceinline__ bool box_hits(float4 b, float x0, float x1, float y0, float y1) {
     return b.x <= x1 && b.y >= x0 && b.z <= y1 && b.w >= y0;

@@ -20,7 +20,7 @@
 // identical inputs. The fast form takes alpha as ex2 of the power in log2
 // units with the opacity folded in (raster_common.cuh fast_record: two FMAs and
 // one MUFU per pixel, one compare for the 1/255 test) and updates the
-// transmittance with one FMA; every pixel is evaluated branch-free. Besides the
+// transmittance as T - alpha T; every pixel is evaluated branch-free. Besides the
 // image the kernel records, per pixel, how many records were consumed up to its
 // last contribution; the backward pass takes its replay's take set from it.
 // A counting variant (RasterForwardArgs::pair_count) also sums the pairs taken.
@@ -120,27 +120,31 @@ __global__ void __launch_bounds__(kRasterThreads) raster_forward_kernel(RasterFo
                 if constexpr (kFast) {
                     // fast_record terms (raster_common.cuh), the same expressions as
                     // the fast backward; every pixel evaluated branch-free, a pixel
-                    // that does not take the record gets alpha = 0
+                    // that does not take the record gets alpha = 0. Scalar
+                    // arithmetic: this loop is bound by the ALU pipe, which the
+                    // register moves of packed pairs would load further.
                     const float Ax = fmaf(q.x * dx, dx, q.w), Bx = q.y * dx;
+                    const int consumed_if = rel + j + 1;
                     bool any = false;
 #pragma unroll
                     for (int p = 0; p < kPixPerThread; ++p) {
                         const float dy = mu.y - fy[p];
                         const float pw2 = fmaf(fmaf(q.z, dy, Bx), dy, Ax);
                         const bool take = !done[p] && pw2 >= kLog2AlphaMin;
-                        float alpha = take ? fminf(kAlphaMax, ex2_approx(pw2)) : 0.0f;
-                        const float nextT = fmaf(-T[p], alpha, T[p]);
+                        const float alpha = take ? fminf(kAlphaMax, ex2_approx(pw2)) : 0.0f;
+                        float w = alpha * T[p];
+                        const float nextT = T[p] - w;  // T (1 - alpha) as T - alpha T
                         // a live pixel's T stays >= 1e-4, so only a taken record can stop it
                         const bool stop = nextT < kTransmittanceMin;
                         done[p] = done[p] || stop;
-                        alpha = stop ? 0.0f : alpha;
-                        const float w = alpha * T[p];
+                        w = stop ? 0.0f : w;
                         C[p].x = fmaf(c.x, w, C[p].x);
                         C[p].y = fmaf(c.y, w, C[p].y);
                         C[p].z = fmaf(c.z, w, C[p].z);
                         T[p] = stop ? T[p] : nextT;
-                        const bool took_p = alpha > 0.0f;
-                        consumed[p] = took_p ? rel + j + 1 : consumed[p];
+                        // alpha >= 1/255 and T >= 1e-4 make a taken record's w > 0
+                        const bool took_p = w > 0.0f;
+                        consumed[p] = took_p ? consumed_if : consumed[p];
                         any |= took_p;
                         if (kCount) pairs += took_p ? 1u : 0u;
                     }

@@ -121,15 +121,9 @@ int launch_gather_gaussians(const float* src, float* dst, const uint32_t* perm, 
     if (n <= 0) return GSN_OK;
     if (!src || !dst || !perm) return GSN_ERR_INVALID_ARGUMENT;
     const unsigned blocks = static_cast<unsigned>(ceil_div(n, 256));
-    if (!bf16_sh) {
-        gather_rows<float><<<dim3(blocks, kParams), 256, 0, stream>>>(src, dst, perm, n);
-        return launched(1);
-    }
-    gather_rows<float><<<dim3(blocks, kGeometryRows), 256, 0, stream>>>(src, dst, perm, n);
-    const int64_t off = static_cast<int64_t>(kGeometryRows) * n;
-    gather_rows<__nv_bfloat16><<<dim3(blocks, kShRows), 256, 0, stream>>>(
-        reinterpret_cast<const __nv_bfloat16*>(src + off), reinterpret_cast<__nv_bfloat16*>(dst + off), perm, n);
-    return launched(2);
+    // one 32-bit word per (physical row, Gaussian) in both layouts
+    gather_rows<float><<<dim3(blocks, bf16_sh ? kPrecisionPhysicalRows : kParams), 256, 0, stream>>>(src, dst, perm, n);
+    return launched(1);
 }
 
 int launch_compose_parents(const int* parents, const uint32_t* perm, int n, int* out, cudaStream_t stream) {

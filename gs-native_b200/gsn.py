@@ -651,12 +651,15 @@ class Graph:
 
 def to_precision_layout(params, torch):
     """58 x N fp32 parameter block (numpy or torch) -> the precision-form device
-    block: 10 fp32 geometry rows, then the 48 SH rows as bf16 (34 float rows)."""
+    block: 10 fp32 geometry rows, then the 48 SH coefficients in bf16 as 24 rows
+    of pairs (34 float rows; coefficient 2r in the low half of word r * N + i
+    of the SH block, 2r + 1 in its high half)."""
     p = torch.as_tensor(params).cuda().float()
     n = p.shape[1]
     block = torch.empty(34 * n, dtype=torch.float32, device="cuda")
     block[:10 * n] = p[:10].reshape(-1)
-    block[10 * n:].view(torch.bfloat16)[:] = p[10:].reshape(-1).to(torch.bfloat16)
+    pairs = p[10:].reshape(24, 2, n).transpose(1, 2).to(torch.bfloat16)
+    block[10 * n:].view(torch.bfloat16)[:] = pairs.reshape(-1)
     return block
 
 
@@ -664,7 +667,7 @@ def from_precision_layout(block, n, torch):
     """Inverse of to_precision_layout: a 58 x N fp32 tensor (SH widened)."""
     out = torch.empty((58, n), dtype=torch.float32, device=block.device)
     out[:10] = block[:10 * n].reshape(10, n)
-    out[10:] = block[10 * n:34 * n].view(torch.bfloat16).reshape(48, n).float()
+    out[10:] = block[10 * n:34 * n].view(torch.bfloat16).reshape(24, n, 2).transpose(1, 2).reshape(48, n).float()
     return out
 
 

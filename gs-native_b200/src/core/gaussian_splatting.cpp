@@ -143,7 +143,11 @@ float FromBf16(uint16_t b) {
     return x;
 }
 
-constexpr size_t kGeometryRows = kShIndex;  // 10 fp32 rows, then 48 bf16 SH rows
+// The precision layout: 10 fp32 rows, then the 48 SH coefficients as 24 rows
+// of bf16 pairs (coefficient 2r in the low half of the 32-bit word r * N + i of
+// the SH block, 2r + 1 in its high half).
+constexpr size_t kGeometryRows = kShIndex;
+size_t ShPairIndex(size_t k, size_t N, size_t i) { return ((k >> 1) * N + i) * 2 + (k & 1); }
 
 }  // namespace
 
@@ -156,7 +160,7 @@ bool GaussianSplatting::SetParameters(const float* host_params, int count) {
         std::memcpy(block.data(), host_params, kGeometryRows * N * sizeof(float));
         auto* sh = reinterpret_cast<uint16_t*>(block.data() + kGeometryRows * N);
         for (size_t k = 0; k < kMaxParamCount - kGeometryRows; ++k)
-            for (size_t i = 0; i < N; ++i) sh[k * N + i] = ToBf16(host_params[(kGeometryRows + k) * N + i]);
+            for (size_t i = 0; i < N; ++i) sh[ShPairIndex(k, N, i)] = ToBf16(host_params[(kGeometryRows + k) * N + i]);
     } else {
         std::memcpy(block.data(), host_params, block.size() * sizeof(float));
     }
@@ -207,7 +211,7 @@ bool GaussianSplatting::GetParameters(std::vector<float>& out) const {
     std::memcpy(out.data(), block.data(), kGeometryRows * N * sizeof(float));
     const auto* sh = reinterpret_cast<const uint16_t*>(block.data() + kGeometryRows * N);
     for (size_t k = 0; k < kMaxParamCount - kGeometryRows; ++k)
-        for (size_t i = 0; i < N; ++i) out[(kGeometryRows + k) * N + i] = FromBf16(sh[k * N + i]);
+        for (size_t i = 0; i < N; ++i) out[(kGeometryRows + k) * N + i] = FromBf16(sh[ShPairIndex(k, N, i)]);
     return true;
 }
 
@@ -446,7 +450,8 @@ bool GaussianSplatting::Load(const std::string& path) {
 namespace {
 
 constexpr char kCheckpointMagic[8] = {'G', 'S', 'N', 'C', 'K', 'P', 'T', '1'};
-constexpr uint32_t kCheckpointVersion = 2;
+// version 3: the precision layout's SH block holds bf16 pair rows
+constexpr uint32_t kCheckpointVersion = 3;
 
 struct CheckpointHeader {
     char magic[8];

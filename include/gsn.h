@@ -157,8 +157,10 @@ int gsn_renderer_record_offsets(gsn_renderer* r, const int** out);
 /* Fixed record capacity (0 = grow on demand, the reference behaviour). */
 int gsn_renderer_set_record_capacity(gsn_renderer* r, int64_t records);
 /* Precision form (gs-native extension): `enabled` selects the parameter layout
- * of 10 fp32 geometry rows followed by the 48 SH rows in bf16 (34 float rows
- * of stride count). The same switch exists on the solver (parameters and Adam
+ * of 10 fp32 geometry rows followed by the 48 SH coefficients in bf16 as 24
+ * rows of pairs (34 rows of 32-bit words of stride count; SH coefficient 2r of
+ * Gaussian i in the low 16 bits of word r * count + i of the SH rows, 2r + 1 in
+ * the high 16 bits). The same switch exists on the solver (parameters and Adam
  * moments; SH updates use stochastic rounding; switching drops the history)
  * and on the density controller. */
 int gsn_renderer_set_bf16_sh(gsn_renderer* r, int enabled);
