@@ -59,7 +59,7 @@ struct ProjectOutputs {
     int depth_key_shift;     // depth key = float bits >> shift (0: exact order; 8: 24-bit keys, fast forms)
 };
 // cam_dev (optional): device camera read instead of `cam` (batched form).
-// bf16_sh: precision-form parameter layout (10 fp32 rows + 48 bf16 SH rows).
+// bf16_sh: precision-form parameter layout (10 fp32 rows + 24 rows of bf16 SH pairs).
 int launch_project(const float* params, int n, const gsn_camera& cam, const gsn_camera* cam_dev, int sh_degree,
                    bool bf16_sh, const ProjectOutputs& out, cudaStream_t stream);
 
