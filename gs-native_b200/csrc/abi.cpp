@@ -139,6 +139,19 @@ int gsn_sort_pairs(uint32_t* keys, uint32_t* values, uint32_t* keys_alt, uint32_
     return status;
 }
 
+int gsn_exclusive_scan_workspace(int max_count, size_t* bytes) {
+    if (!bytes || max_count < 0) return GSN_ERR_INVALID_ARGUMENT;
+    *bytes = gsn::scan_scratch_bytes(max_count);
+    return GSN_OK;
+}
+
+int gsn_exclusive_scan(const int* in, const uint32_t* gather, int* out, int count, const int* valid,
+                       void* workspace, size_t workspace_bytes, void* stream) {
+    if (count < 0 || !out || (count > 0 && (!in || !workspace || workspace_bytes < gsn::scan_scratch_bytes(count))))
+        return GSN_ERR_INVALID_ARGUMENT;
+    return gsn::launch_exclusive_scan(in, gather, out, count, workspace, AsStream(stream), valid);
+}
+
 int gsn_sort_pairs_noalloc(uint32_t* keys, uint32_t* values, uint32_t* keys_alt, uint32_t* values_alt, int count,
                            int begin_bit, int end_bit, int* result_in_alt, void* stream) {
     if (!result_in_alt || count < 0 || begin_bit < 0 || end_bit > 32 || end_bit < begin_bit) return GSN_ERR_INVALID_ARGUMENT;

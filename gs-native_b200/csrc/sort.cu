@@ -291,76 +291,123 @@ __device__ __forceinline__ int block_exclusive_scan(int x, int* warp_sums, int* 
     return prefix + inc - x;
 }
 
-__global__ void __launch_bounds__(kScanThreads) scan_reduce(const int* __restrict__ in,
-                                                            const uint32_t* __restrict__ gather, int n,
-                                                            const int* __restrict__ valid_dev,
-                                                            int* __restrict__ block_sums) {
-    __shared__ int warp_sums[kScanThreads / 32];
-    const int64_t start = static_cast<int64_t>(blockIdx.x) * kScanChunk;
-    const int valid = valid_dev ? min(*valid_dev, n) : n;
-    int s = 0;
+// Single-pass exclusive scan with decoupled look-back (Merrill and Garland
+// 2016). A CTA takes the next chunk index from a ticket counter (so every chunk
+// it waits on belongs to a CTA that has already started), scans its chunk in
+// shared memory, publishes the chunk total (aggregate; chunk 0 publishes its
+// inclusive prefix at once) and lets warp 0 read the 32 preceding chunks' status
+// words at a time: it adds aggregates up to the nearest inclusive prefix and
+// publishes its own. Status words hold the flag in the top two bits and the
+// value below. A word that stays unpublished for kScanPolls polls sets *error
+// and ends the walk; offsets then come out too small but never negative, and
+// every write stays inside the n + 1 outputs.
+constexpr uint64_t kScanAggregate = 1ull << 62;
+constexpr uint64_t kScanInclusive = 2ull << 62;
+constexpr uint64_t kScanValue = (1ull << 62) - 1;
+constexpr int kScanPolls = 1 << 20;
+
+__device__ __forceinline__ void store_scan_status(unsigned long long* address, unsigned long long value) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(address), "l"(value) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long load_scan_status(const unsigned long long* address) {
+    unsigned long long value;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(value) : "l"(address) : "memory");
+    return value;
+}
+
+__device__ __forceinline__ long long warp_sum64(long long v) {
 #pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-        int64_t i = start + k * kScanThreads + threadIdx.x;
-        if (i < valid) s += gather ? in[gather[i]] : in[i];
-    }
-    int total;
-    block_exclusive_scan(s, warp_sums, &total);
-    if (threadIdx.x == 0) block_sums[blockIdx.x] = total;
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
 }
 
-__global__ void __launch_bounds__(kScanThreads) scan_block_sums(int* __restrict__ block_sums, int blocks,
-                                                                int* __restrict__ total_out) {
-    __shared__ int warp_sums[kScanThreads / 32];
-    int carry = 0;
-    for (int base = 0; base < blocks; base += kScanThreads) {
-        int i = base + threadIdx.x;
-        int x = i < blocks ? block_sums[i] : 0;
-        int total;
-        int ex = block_exclusive_scan(x, warp_sums, &total);
-        if (i < blocks) block_sums[i] = carry + ex;
-        carry += total;
-    }
-    if (threadIdx.x == 0) *total_out = carry;
-}
-
-__global__ void __launch_bounds__(kScanThreads) scan_downsweep(const int* in, const uint32_t* __restrict__ gather,
-                                                               int n, const int* __restrict__ valid_dev,
-                                                               const int* __restrict__ block_sums, int* out) {
+__global__ void __launch_bounds__(kScanThreads) scan_onepass(const int* in, const uint32_t* __restrict__ gather,
+                                                             int n, const int* __restrict__ valid_dev, int* out,
+                                                             unsigned long long* __restrict__ status,
+                                                             int* __restrict__ ticket, int* __restrict__ error) {
     __shared__ int warp_sums[kScanThreads / 32];
     __shared__ int tile[kScanChunk];
-    const int64_t start = static_cast<int64_t>(blockIdx.x) * kScanChunk;
+    __shared__ int s_chunk;
+    __shared__ long long s_excl;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) s_chunk = atomicAdd(ticket, 1);
+    __syncthreads();
+    const int chunk = s_chunk;
+    const int64_t start = static_cast<int64_t>(chunk) * kScanChunk;
     const int valid = valid_dev ? min(*valid_dev, n) : n;
     // striped coalesced load -> blocked per-thread sequences via shared memory;
     // entries from `valid` on count as zero
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
-        int j = k * kScanThreads + threadIdx.x;
-        int64_t i = start + j;
+        const int j = k * kScanThreads + threadIdx.x;
+        const int64_t i = start + j;
         tile[j] = i < valid ? (gather ? in[gather[i]] : in[i]) : 0;
     }
     __syncthreads();
     int v[kScanItems];
-    int s = 0;
+    int sum = 0;
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
         v[k] = tile[threadIdx.x * kScanItems + k];
-        s += v[k];
+        sum += v[k];
     }
     int total;
-    int run = block_exclusive_scan(s, warp_sums, &total) + block_sums[blockIdx.x];
+    int run = block_exclusive_scan(sum, warp_sums, &total);
+    if (threadIdx.x == 0) {
+        store_scan_status(status + chunk, (chunk == 0 ? kScanInclusive : kScanAggregate) |
+                                              static_cast<unsigned long long>(total));
+        if (chunk == 0) s_excl = 0;
+    }
+    if (chunk > 0 && warp == 0) {
+        long long excl = 0;
+        int c = chunk - 1;  // the nearest chunk not yet added
+        for (int polls = 0;;) {
+            const int idx = c - lane;
+            // lanes past chunk 0 read a virtual inclusive zero (chunk 0 is
+            // inclusive, so the walk never needs them)
+            const unsigned long long w = idx >= 0 ? load_scan_status(status + idx) : kScanInclusive;
+            const uint32_t pending = __ballot_sync(0xffffffffu, (w >> 62) == 0);
+            const uint32_t inclusive = __ballot_sync(0xffffffffu, (w >> 62) == 2);
+            const int first_pending = pending ? __ffs(pending) - 1 : 32;
+            const int first_inclusive = inclusive ? __ffs(inclusive) - 1 : 32;
+            if (first_inclusive < first_pending) {
+                excl += warp_sum64(lane <= first_inclusive ? static_cast<long long>(w & kScanValue) : 0);
+                break;
+            }
+            // lanes before the first pending word are aggregates: add them and
+            // continue from the pending one
+            excl += warp_sum64(lane < first_pending ? static_cast<long long>(w & kScanValue) : 0);
+            c -= first_pending;
+            if (first_pending < 32) {
+                if (++polls >= kScanPolls) {
+                    if (lane == 0) atomicExch(error, 1);
+                    break;
+                }
+                if (polls >= 32) __nanosleep(64);
+            }
+        }
+        if (lane == 0) {
+            store_scan_status(status + chunk, kScanInclusive | static_cast<unsigned long long>(excl + total));
+            s_excl = excl;
+        }
+    }
+    __syncthreads();
+    const long long base = s_excl;
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
-        tile[threadIdx.x * kScanItems + k] = run;
+        tile[threadIdx.x * kScanItems + k] = static_cast<int>(base + run);
         run += v[k];
     }
     __syncthreads();
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
-        int j = k * kScanThreads + threadIdx.x;
-        int64_t i = start + j;
+        const int j = k * kScanThreads + threadIdx.x;
+        const int64_t i = start + j;
         if (i < n) out[i] = tile[j];
     }
+    // the chunk holding element n - 1 also writes the total
+    if (threadIdx.x == 0 && start + kScanChunk >= n) out[n] = static_cast<int>(base + total);
 }
 
 // ---------------------------------------------------------------- records
@@ -568,20 +615,22 @@ int launch_radix_sort_noalloc(uint32_t* keys, uint32_t* values, uint32_t* keys_a
                              result_in_alt, stream);
 }
 
+// Scan scratch: the ticket counter and the error word (16 bytes), then one
+// 64-bit look-back status word per 2048-element chunk.
 size_t scan_scratch_bytes(int n) {
-    return static_cast<size_t>(ceil_div(n > 0 ? n : 1, kScanChunk) + 1) * sizeof(int);
+    return 16 + static_cast<size_t>(ceil_div(n > 0 ? n : 1, kScanChunk)) * sizeof(unsigned long long);
 }
 
 int launch_exclusive_scan(const int* in, const uint32_t* gather, int* out, int n, void* scratch,
                           cudaStream_t stream, const int* valid_device) {
     if (n < 0) return GSN_ERR_INVALID_ARGUMENT;
-    int* block_sums = static_cast<int*>(scratch);
-    int blocks = ceil_div(n > 0 ? n : 1, kScanChunk);
-    if (n > 0) scan_reduce<<<blocks, kScanThreads, 0, stream>>>(in, gather, n, valid_device, block_sums);
-    else cudaMemsetAsync(block_sums, 0, sizeof(int), stream);
-    scan_block_sums<<<1, kScanThreads, 0, stream>>>(block_sums, n > 0 ? blocks : 0, out + n);
-    if (n > 0) scan_downsweep<<<blocks, kScanThreads, 0, stream>>>(in, gather, n, valid_device, block_sums, out);
-    return launched(n > 0 ? 3 : 1);
+    if (n == 0) return cudaMemsetAsync(out, 0, sizeof(int), stream) == cudaSuccess ? GSN_OK : GSN_ERR_CUDA;
+    const int blocks = ceil_div(n, kScanChunk);
+    int* ticket = static_cast<int*>(scratch);
+    auto* status = reinterpret_cast<unsigned long long*>(static_cast<char*>(scratch) + 16);
+    if (cudaMemsetAsync(scratch, 0, scan_scratch_bytes(n), stream) != cudaSuccess) return GSN_ERR_CUDA;
+    scan_onepass<<<blocks, kScanThreads, 0, stream>>>(in, gather, n, valid_device, out, status, ticket, ticket + 1);
+    return launched(1);
 }
 
 int launch_emit_records(const uint32_t* sorted_ids, const int* record_start, const int4* rects, int n,

@@ -87,6 +87,8 @@ def lib():
         "gsn_stage_count": ([], i32),
         "gsn_sort_pairs_workspace": ([i32, P(ctypes.c_size_t)], i32),
         "gsn_sort_pairs": ([vp, vp, vp, vp, i32, i32, i32, vp, ctypes.c_size_t, P(i32), vp], i32),
+        "gsn_exclusive_scan_workspace": ([i32, P(ctypes.c_size_t)], i32),
+        "gsn_exclusive_scan": ([vp, vp, vp, i32, vp, vp, ctypes.c_size_t, vp], i32),
         "gsn_renderer_create": ([P(vp)], i32),
         "gsn_renderer_destroy": ([vp], i32),
         "gsn_renderer_set_stream": ([vp, vp], i32),
@@ -219,6 +221,19 @@ def sort_pairs(keys, values, keys_alt, values_alt, count, begin_bit, end_bit, wo
                               ctypes.c_void_p(workspace), ctypes.c_size_t(workspace_bytes), ctypes.byref(alt),
                               ctypes.c_void_p(stream))
     return st, alt.value
+
+
+def exclusive_scan_workspace(max_count):
+    b = ctypes.c_size_t()
+    _check(lib().gsn_exclusive_scan_workspace(int(max_count), ctypes.byref(b)), "exclusive_scan_workspace")
+    return b.value
+
+
+def exclusive_scan(inp, gather, out, count, valid, workspace, workspace_bytes, stream=0):
+    """Device pointers (gather and valid may be 0). Returns the status."""
+    return lib().gsn_exclusive_scan(ctypes.c_void_p(inp), ctypes.c_void_p(gather), ctypes.c_void_p(out), int(count),
+                                    ctypes.c_void_p(valid), ctypes.c_void_p(workspace),
+                                    ctypes.c_size_t(workspace_bytes), ctypes.c_void_p(stream))
 
 
 def device_alloc(nbytes):

@@ -100,6 +100,18 @@ int gsn_sort_pairs(uint32_t* keys, uint32_t* values, uint32_t* keys_alt, uint32_
 int gsn_sort_pairs_noalloc(uint32_t* keys, uint32_t* values, uint32_t* keys_alt, uint32_t* values_alt, int count,
                            int begin_bit, int end_bit, int* result_in_alt, void* stream);
 
+/* Exclusive prefix sum of `count` device ints, the record scan of the ordering
+ * (gs-native extension; the reference's Render runs cub::DeviceScan::
+ * ExclusiveSum in place over its tile counts, renderer.cu:465-483): out[i] = the sum of
+ * the entries before i, out[count] = the total, where entry j is
+ * in[gather ? gather[j] : j] for j < *valid (device int; all `count` when
+ * valid is null) and zero from there on. `out` holds count + 1 ints; in == out
+ * is allowed without `gather`. One pass with decoupled look-back. Device
+ * workspace: gsn_exclusive_scan_workspace bytes. */
+int gsn_exclusive_scan_workspace(int max_count, size_t* bytes);
+int gsn_exclusive_scan(const int* in, const uint32_t* gather, int* out, int count, const int* valid,
+                       void* workspace, size_t workspace_bytes, void* stream);
+
 /* ------------------------------------------------------------------ 3-NN
  * LBVH 3-nearest-neighbour search (replaces ComputeMeanDist2Cuda, reference
  * src/core/knn/knn.h:9 and knn.cu:180-255). points: device float[3 * count]

@@ -81,3 +81,57 @@ def test_sort_pairs_many_chunks_tile_bits():
     k, v = run_sort(keys, values, 0, 13)
     ek, ev = expected(keys, values, 0, 13)
     assert np.array_equal(k, ek) and np.array_equal(v, ev)
+
+
+def run_scan(values, gather=None, valid=None, in_place=False):
+    t = torch()
+    n = len(values)
+    if in_place:
+        inp = out = dev(np.concatenate([values, [0]]).astype(np.int32))
+    else:
+        inp, out = dev(values.astype(np.int32)), empty((n + 1,), t.int32)
+    g = dev(gather.astype(np.int32)) if gather is not None else None
+    vd = dev(np.array([valid], dtype=np.int32)) if valid is not None else None
+    ws_bytes = gsn.exclusive_scan_workspace(n)
+    ws = empty((max(ws_bytes, 1),), t.uint8)
+    st = gsn.exclusive_scan(inp.data_ptr(), g.data_ptr() if g is not None else 0, out.data_ptr(), n,
+                            vd.data_ptr() if vd is not None else 0, ws.data_ptr(), ws_bytes)
+    assert st == 0
+    sync()
+    return out.cpu().numpy()[:n + 1].astype(np.int64)
+
+
+def expected_scan(values, gather=None, valid=None):
+    entries = values[gather] if gather is not None else values.copy()
+    if valid is not None:
+        entries[valid:] = 0
+    return np.concatenate([[0], np.cumsum(entries.astype(np.int64))])
+
+
+@pytest.mark.parametrize("n", [1, 2047, 2048, 2049, 100_000, 1_200_000, 5_000_001])
+def test_exclusive_scan_matches_cumulative_sum(n):
+    """The one-pass scan (decoupled look-back over 2,048-entry chunks) against
+    numpy's cumulative sum: plain, gathered through a permutation with a device
+    valid count (the renderer's record scan in depth order), and in place (the
+    density controller's use)."""
+    rng = np.random.default_rng(n)
+    values = rng.integers(0, 40, n).astype(np.int32)
+    assert np.array_equal(run_scan(values), expected_scan(values))
+    perm = rng.permutation(n).astype(np.int64)
+    valid = int(n * 0.6)
+    assert np.array_equal(run_scan(values, perm, valid), expected_scan(values, perm, valid))
+    assert np.array_equal(run_scan(values, in_place=True), expected_scan(values))
+
+
+def test_exclusive_scan_edge_cases():
+    t = torch()
+    out = dev(np.array([7], dtype=np.int32))
+    ws = empty((gsn.exclusive_scan_workspace(0) or 1,), t.uint8)
+    assert gsn.exclusive_scan(0, 0, out.data_ptr(), 0, 0, ws.data_ptr(), 16) == 0
+    sync()
+    assert out.cpu().numpy()[0] == 0
+    values = np.zeros(3000, dtype=np.int32)
+    assert np.array_equal(run_scan(values, valid=0), np.zeros(3001))
+    # a workspace smaller than the count needs is rejected without launching
+    buf = dev(np.ones(5000, dtype=np.int32))
+    assert gsn.exclusive_scan(buf.data_ptr(), 0, buf.data_ptr(), 4999, 0, ws.data_ptr(), 16) != 0
