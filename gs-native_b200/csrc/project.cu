@@ -124,7 +124,8 @@ __device__ __forceinline__ int cull_count(float2 mean, float4 q, int4 rect) {
 // Records of the culled counts in depth order. Four lanes serve a Gaussian and
 // take its rows four at a time, one row each: a lane finds its row's column
 // interval, the group's exclusive prefix of the interval widths (shuffles
-// within the four lanes) places the row, and the lane writes the row's records.
+// within the four lanes) places the row, and the four lanes write the group's
+// records interleaved (consecutive lanes, consecutive slots).
 // The loop runs the warp's largest number of row groups so every shuffle sees
 // all 32 lanes.
 __global__ void __launch_bounds__(256) emit_records_culled(const uint32_t* __restrict__ sorted_ids,
@@ -177,10 +178,18 @@ __global__ void __launch_bounds__(256) emit_records_culled(const uint32_t* __res
             if (sub >= o) incl += y;
         }
         const int group_total = __shfl_sync(0xffffffffu, incl, 3, 4);
-        const int at = k + incl - w;
-        for (int j = 0; j < w && at + j < count && begin + at + j < capacity; ++j) {
-            tile_keys[begin + at + j] = static_cast<uint32_t>(ty * tile_count_x + span.x + j);
-            record_ids[begin + at + j] = id;
+        // the group's four rows are one contiguous run of records; a record at
+        // run position q of row i has tile q + base_i. The four lanes write the
+        // run interleaved, so consecutive lanes write consecutive slots.
+        const int base = ty * tile_count_x + span.x - (incl - w);
+        const int e0 = __shfl_sync(0xffffffffu, incl, 0, 4), e1 = __shfl_sync(0xffffffffu, incl, 1, 4);
+        const int e2 = __shfl_sync(0xffffffffu, incl, 2, 4);
+        const int b0 = __shfl_sync(0xffffffffu, base, 0, 4), b1 = __shfl_sync(0xffffffffu, base, 1, 4);
+        const int b2 = __shfl_sync(0xffffffffu, base, 2, 4), b3 = __shfl_sync(0xffffffffu, base, 3, 4);
+        for (int q = sub; q < group_total && k + q < count && begin + k + q < capacity; q += 4) {
+            const int row_base = q < e0 ? b0 : q < e1 ? b1 : q < e2 ? b2 : b3;
+            tile_keys[begin + k + q] = static_cast<uint32_t>(row_base + q);
+            record_ids[begin + k + q] = id;
         }
         k += group_total;
     }

@@ -133,15 +133,15 @@ __global__ void __launch_bounds__(kRasterThreads) raster_forward_kernel(RasterFo
                         const bool take = !done[p] && pw2 >= kLog2AlphaMin;
                         const float alpha = take ? fminf(kAlphaMax, ex2_approx(pw2)) : 0.0f;
                         float w = alpha * T[p];
-                        const float nextT = T[p] - w;  // T (1 - alpha) as T - alpha T
-                        // a live pixel's T stays >= 1e-4, so only a taken record can stop it
-                        const bool stop = nextT < kTransmittanceMin;
-                        done[p] = done[p] || stop;
-                        w = stop ? 0.0f : w;
+                        // a live pixel's T stays >= 1e-4, so only a taken record can
+                        // stop it, and a pixel that was already done has w = 0: the
+                        // updated done flag alone decides whether w counts
+                        done[p] = done[p] || T[p] - w < kTransmittanceMin;
+                        w = done[p] ? 0.0f : w;
                         C[p].x = fmaf(c.x, w, C[p].x);
                         C[p].y = fmaf(c.y, w, C[p].y);
                         C[p].z = fmaf(c.z, w, C[p].z);
-                        T[p] = stop ? T[p] : nextT;
+                        T[p] -= w;  // T (1 - alpha) as T - alpha T; unchanged at the stop
                         // alpha >= 1/255 and T >= 1e-4 make a taken record's w > 0
                         const bool took_p = w > 0.0f;
                         consumed[p] = took_p ? consumed_if : consumed[p];
