@@ -152,7 +152,7 @@ template <bool kIdentityValues, bool kDrop>
 __global__ void __launch_bounds__(kSortThreads) radix_downsweep(
     const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ values_in,
     uint32_t* __restrict__ keys_out, uint32_t* __restrict__ values_out, const int* n_dev, int n_host,
-    int bit, uint32_t mask, const uint32_t* __restrict__ block_hist, size_t hist_stride) {
+    int bit, uint32_t mask, int digit_bits, const uint32_t* __restrict__ block_hist, size_t hist_stride) {
     __shared__ uint32_t counts[kSortWarps][kBins];
     __shared__ uint32_t global_base[kBins];
     __shared__ uint32_t local_base[kBins];
@@ -186,10 +186,12 @@ __global__ void __launch_bounds__(kSortThreads) radix_downsweep(
         bool valid = slice + s * 32 + lane < end;
         if (kDrop) valid = valid && key[s] != kSortSentinel;
         uint32_t digit = valid ? ((key[s] >> bit) & mask) : 0u;
-        // lanes holding the same digit: intersect the eight per-bit ballots
+        // lanes holding the same digit: intersect the per-bit ballots of the
+        // pass's digit bits
         uint32_t peers = __ballot_sync(0xffffffffu, valid);
 #pragma unroll
         for (int b = 0; b < 8; ++b) {
+            if (b >= digit_bits) break;
             uint32_t bal = __ballot_sync(0xffffffffu, (digit >> b) & 1u);
             peers &= ((digit >> b) & 1u) ? bal : ~bal;
         }
@@ -516,10 +518,14 @@ static int radix_sort_impl(uint32_t* keys, uint32_t* values, uint32_t* keys_alt,
     const int blocks = ceil_div(max_count, kSortChunk);
     uint32_t *kin = keys, *vin = values, *kout = keys_alt, *vout = values_alt;
     const int* count = count_device;
+    // the key bits split into passes of near-equal width (13 tile bits: 7 + 6),
+    // so no pass pays for a 256-bin digit it does not need
+    const int width = end_bit - begin_bit;
+    int bit = begin_bit;
     for (int p = 0; p < passes; ++p) {
-        int bit = begin_bit + 8 * p;
-        // the last pass only looks at the bits below end_bit
-        uint32_t mask = end_bit - bit >= 8 ? 0xFFu : ((1u << (end_bit - bit)) - 1u);
+        const int digit_bits = width / passes + (p < width % passes ? 1 : 0);
+        const uint32_t mask = (1u << digit_bits) - 1u;
+        const int bins = 1 << digit_bits;
         uint32_t* dt = scratch.digit_total + kBins * p;
         const bool drop = kept_device && p == 0;
         if (drop)
@@ -528,20 +534,24 @@ static int radix_sort_impl(uint32_t* keys, uint32_t* values, uint32_t* keys_alt,
         else
             radix_upsweep<false><<<blocks, kSortThreads, 0, stream>>>(kin, count, max_count, bit, mask,
                                                                       scratch.block_hist, scratch.max_blocks, dt);
-        radix_scan<<<kBins, kSortThreads, 0, stream>>>(count, max_count, scratch.block_hist, scratch.max_blocks, dt);
+        radix_scan<<<bins, kSortThreads, 0, stream>>>(count, max_count, scratch.block_hist, scratch.max_blocks, dt);
         const uint32_t* vsrc = identity_values && p == 0 ? nullptr : vin;
         if (identity_values && p == 0 && drop)
             radix_downsweep<true, true><<<blocks, kSortThreads, 0, stream>>>(
-                kin, vsrc, kout, vout, count, max_count, bit, mask, scratch.block_hist, scratch.max_blocks);
+                kin, vsrc, kout, vout, count, max_count, bit, mask, digit_bits, scratch.block_hist,
+                scratch.max_blocks);
         else if (identity_values && p == 0)
             radix_downsweep<true, false><<<blocks, kSortThreads, 0, stream>>>(
-                kin, vsrc, kout, vout, count, max_count, bit, mask, scratch.block_hist, scratch.max_blocks);
+                kin, vsrc, kout, vout, count, max_count, bit, mask, digit_bits, scratch.block_hist,
+                scratch.max_blocks);
         else if (drop)
             radix_downsweep<false, true><<<blocks, kSortThreads, 0, stream>>>(
-                kin, vsrc, kout, vout, count, max_count, bit, mask, scratch.block_hist, scratch.max_blocks);
+                kin, vsrc, kout, vout, count, max_count, bit, mask, digit_bits, scratch.block_hist,
+                scratch.max_blocks);
         else
             radix_downsweep<false, false><<<blocks, kSortThreads, 0, stream>>>(
-                kin, vsrc, kout, vout, count, max_count, bit, mask, scratch.block_hist, scratch.max_blocks);
+                kin, vsrc, kout, vout, count, max_count, bit, mask, digit_bits, scratch.block_hist,
+                scratch.max_blocks);
         if (drop) {
             // later passes (and the caller) see only the kept keys
             radix_kept<<<1, kBins, 0, stream>>>(dt, kept_device);
@@ -549,6 +559,7 @@ static int radix_sort_impl(uint32_t* keys, uint32_t* values, uint32_t* keys_alt,
         }
         uint32_t* tk = kin; kin = kout; kout = tk;
         uint32_t* tv = vin; vin = vout; vout = tv;
+        bit += digit_bits;
     }
     *result_in_alt = (passes % 2) == 1;
     return launched(3 * passes + (kept_device ? 1 : 0));
