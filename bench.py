@@ -102,6 +102,8 @@ def parse():
                    help="skip the 3.0M-Gaussian 2048x1360 batched-form measurement")
     p.add_argument("--gate-iterations", type=int, default=6000,
                    help="iterations of each held-out PSNR gate run (reduced schedule)")
+    p.add_argument("--no-programmatic-launch", action="store_true",
+                   help="launch the step's kernels without programmatic dependent launch (for comparison)")
     return p.parse_args()
 
 
@@ -562,6 +564,7 @@ def run_gsn(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     gsn.lib()
+    gsn.set_programmatic_launch(not args.no_programmatic_launch)
     target_model, model, train, extent = scene(args.gaussians)
     views = 3 if args.profile_only else args.views
     if views:
@@ -916,6 +919,7 @@ def run_gsn(args):
         "config": {"workload": WORKLOAD,
                    "form": chosen, "gaussians": n, "width": 1600, "height": 1064,
                    "records_per_step": records, "visible_gaussians": vis, "parallelism": f"replicas{world}",
+                   "programmatic_launch": not args.no_programmatic_launch,
                    "l2": "inputs larger than L2 (params + Adam moments 835 MB, a new 5 MB target per step)"},
         "gpu_launches": forms[chosen]["gpu_launches"],
         "forms": forms,

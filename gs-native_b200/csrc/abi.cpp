@@ -102,6 +102,11 @@ int gsn_stream_synchronize(void* stream) {
 
 uint64_t gsn_kernel_launch_count(void) { return gsn::launch_count(); }
 
+int gsn_set_programmatic_launch(int enabled) {
+    gsn::set_programmatic_launch(enabled != 0);
+    return GSN_OK;
+}
+
 int gsn_profile_enable(int enabled) {
     gsn::profile_enable(enabled != 0);
     return GSN_OK;

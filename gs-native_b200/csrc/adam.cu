@@ -321,6 +321,7 @@ __device__ __forceinline__ void adam_pairs_bf16(uint32_t* __restrict__ P, uint32
 
 template <int D, bool kBf16>
 __global__ void __launch_bounds__(256, 2) gaussian_update_kernel(GaussianUpdateArgs a) {
+    pdl_begin();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n) return;
     const int64_t N = a.n;
@@ -468,17 +469,17 @@ int launch_gaussian_update(const GaussianUpdateArgs& a, int sh_degree, cudaStrea
     const int d = sh_degree < 0 ? 0 : (sh_degree > 3 ? 3 : sh_degree);
     if (a.bf16_sh) {
         switch (d) {
-            case 0: gaussian_update_kernel<0, true><<<grid, 256, 0, stream>>>(a); break;
-            case 1: gaussian_update_kernel<1, true><<<grid, 256, 0, stream>>>(a); break;
-            case 2: gaussian_update_kernel<2, true><<<grid, 256, 0, stream>>>(a); break;
-            default: gaussian_update_kernel<3, true><<<grid, 256, 0, stream>>>(a); break;
+            case 0: launch_step(gaussian_update_kernel<0, true>, grid, 256, 0, stream, a); break;
+            case 1: launch_step(gaussian_update_kernel<1, true>, grid, 256, 0, stream, a); break;
+            case 2: launch_step(gaussian_update_kernel<2, true>, grid, 256, 0, stream, a); break;
+            default: launch_step(gaussian_update_kernel<3, true>, grid, 256, 0, stream, a); break;
         }
     } else {
         switch (d) {
-            case 0: gaussian_update_kernel<0, false><<<grid, 256, 0, stream>>>(a); break;
-            case 1: gaussian_update_kernel<1, false><<<grid, 256, 0, stream>>>(a); break;
-            case 2: gaussian_update_kernel<2, false><<<grid, 256, 0, stream>>>(a); break;
-            default: gaussian_update_kernel<3, false><<<grid, 256, 0, stream>>>(a); break;
+            case 0: launch_step(gaussian_update_kernel<0, false>, grid, 256, 0, stream, a); break;
+            case 1: launch_step(gaussian_update_kernel<1, false>, grid, 256, 0, stream, a); break;
+            case 2: launch_step(gaussian_update_kernel<2, false>, grid, 256, 0, stream, a); break;
+            default: launch_step(gaussian_update_kernel<3, false>, grid, 256, 0, stream, a); break;
         }
     }
     return launched(1);

@@ -11,6 +11,7 @@ namespace gsn {
 namespace {
 
 __global__ void __launch_bounds__(32) advance_frame_kernel(StepSchedule s, StepFrame* __restrict__ f) {
+    pdl_begin();
     __shared__ int step, view;
     if (threadIdx.x == 0) {
         // a record overflow of the previous step is folded in before the
@@ -52,7 +53,7 @@ int launch_advance_frame(const StepSchedule& s, StepFrame* frame, cudaStream_t s
     if (!frame || !s.cameras || !s.targets || !s.views || !s.position_lr || !s.c1 || !s.c2 || !s.seeds || !s.cursor ||
         !s.status || s.steps <= 0 || s.view_count <= 0)
         return GSN_ERR_INVALID_ARGUMENT;
-    advance_frame_kernel<<<1, 32, 0, stream>>>(s, frame);
+    launch_step(advance_frame_kernel, 1, 32, 0, stream, s, frame);
     return launched(1);
 }
 

@@ -63,6 +63,7 @@ __global__ void __launch_bounds__(kThreads, 3) loss_gradient_kernel(const float*
                                                                    const StepFrame* __restrict__ frame,
                                                                    float* __restrict__ grad, int width, int height,
                                                                    double* __restrict__ sums) {
+    pdl_begin();
     extern __shared__ float smem[];
     const uint8_t* __restrict__ target = frame ? frame->target : target_arg;
     __shared__ double red[kThreads / 32];
@@ -282,6 +283,7 @@ __global__ void __launch_bounds__(kThreads, 3) loss_gradient_fast_kernel(const f
                                                                         const StepFrame* __restrict__ frame,
                                                                         float* __restrict__ grad, int width,
                                                                         int height, double* __restrict__ sums) {
+    pdl_begin();
     extern __shared__ float smem[];
     const uint8_t* __restrict__ target = frame ? frame->target : target_arg;
     __shared__ double red[kThreads / 32];
@@ -516,6 +518,7 @@ __global__ void __launch_bounds__(kThreads, 3) loss_gradient_fast_kernel(const f
 }
 
 __global__ void finalize_loss_kernel(const double* sums, int width, int height, double* out) {
+    pdl_begin();
     double count = 3.0 * static_cast<double>(width) * height;
     double l1 = sums[0] / count, ssim = sums[1] / count, mse = sums[2] / count;
     out[0] = 0.8 * l1 + 0.2 * (1.0 - ssim);
@@ -546,15 +549,16 @@ int launch_loss_gradient(const float* image, const uint8_t* target, const StepFr
     }
     dim3 grid(ceil_div(width, kT), ceil_div(height, kT), 3);
     if (fast)
-        loss_gradient_fast_kernel<<<grid, kThreads, kSmemBytes, stream>>>(image, target, frame, grad, width, height,
-                                                                         sums);
+        launch_step(loss_gradient_fast_kernel, grid, kThreads, kSmemBytes, stream, image, target, frame, grad, width,
+                    height, sums);
     else
-        loss_gradient_kernel<<<grid, kThreads, kSmemBytes, stream>>>(image, target, frame, grad, width, height, sums);
+        launch_step(loss_gradient_kernel, grid, kThreads, kSmemBytes, stream, image, target, frame, grad, width, height,
+                    sums);
     return launched(1);
 }
 
 int launch_finalize_loss(const double* sums, int width, int height, double* out, cudaStream_t stream) {
-    finalize_loss_kernel<<<1, 1, 0, stream>>>(sums, width, height, out);
+    launch_step(finalize_loss_kernel, 1, 1, 0, stream, sums, width, height, out);
     return launched(1);
 }
 

@@ -37,6 +37,13 @@ const char* kNames[kStageCount] = {"project",       "depth_sort",     "record_sc
 
 void note_launch(int kernels) { g_launches.fetch_add(static_cast<uint64_t>(kernels), std::memory_order_relaxed); }
 
+namespace {
+std::atomic<bool> g_programmatic_launch{true};
+}  // namespace
+
+void set_programmatic_launch(bool on) { g_programmatic_launch.store(on, std::memory_order_relaxed); }
+bool programmatic_launch() { return g_programmatic_launch.load(std::memory_order_relaxed); }
+
 uint64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
 void profile_enable(bool on) {

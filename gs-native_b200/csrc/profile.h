@@ -25,6 +25,9 @@ enum Stage {
 
 void note_launch(int kernels = 1);
 uint64_t launch_count();
+// Programmatic dependent launch of the training step's kernels (on by default).
+void set_programmatic_launch(bool on);
+bool programmatic_launch();
 void profile_enable(bool on);
 bool profile_enabled();
 void stage_mark(cudaStream_t stream, int stage);

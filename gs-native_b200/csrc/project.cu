@@ -136,6 +136,7 @@ __global__ void __launch_bounds__(256) emit_records_culled(const uint32_t* __res
                                                            int tile_count_x, uint32_t* __restrict__ tile_keys,
                                                            uint32_t* __restrict__ record_ids, int64_t capacity,
                                                            int* overflow) {
+    pdl_begin();
     const int64_t gidx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     const int64_t p = gidx >> 2;
     const int sub = static_cast<int>(gidx & 3);
@@ -203,6 +204,7 @@ template <int D, bool kBf16, int TW = kTile, int TH = kTile>
 __global__ void __launch_bounds__(256) project_kernel(const float* __restrict__ params,
                                                       gsn_camera cam_arg, const gsn_camera* __restrict__ cam_dev,
                                                       int n, ProjectOutputs out) {
+    pdl_begin();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const gsn_camera cam = cam_dev ? *cam_dev : cam_arg;
@@ -331,10 +333,10 @@ void launch_project_layout(const float* params, int n, const gsn_camera& cam, co
                            const ProjectOutputs& out, cudaStream_t stream) {
     dim3 grid(ceil_div(n, 256));
     switch (d) {
-        case 0: project_kernel<0, kBf16><<<grid, 256, 0, stream>>>(params, cam, cam_dev, n, out); break;
-        case 1: project_kernel<1, kBf16><<<grid, 256, 0, stream>>>(params, cam, cam_dev, n, out); break;
-        case 2: project_kernel<2, kBf16><<<grid, 256, 0, stream>>>(params, cam, cam_dev, n, out); break;
-        default: project_kernel<3, kBf16><<<grid, 256, 0, stream>>>(params, cam, cam_dev, n, out); break;
+        case 0: launch_step(project_kernel<0, kBf16>, grid, 256, 0, stream, params, cam, cam_dev, n, out); break;
+        case 1: launch_step(project_kernel<1, kBf16>, grid, 256, 0, stream, params, cam, cam_dev, n, out); break;
+        case 2: launch_step(project_kernel<2, kBf16>, grid, 256, 0, stream, params, cam, cam_dev, n, out); break;
+        default: launch_step(project_kernel<3, kBf16>, grid, 256, 0, stream, params, cam, cam_dev, n, out); break;
     }
 }
 
@@ -345,10 +347,14 @@ static void launch_project_tiles(const float* params, int n, const gsn_camera& c
                           cudaStream_t stream) {
     dim3 grid(ceil_div(n, 256));
     switch (d) {
-        case 0: project_kernel<0, false, TW, TH><<<grid, 256, 0, stream>>>(params, cam, nullptr, n, out); break;
-        case 1: project_kernel<1, false, TW, TH><<<grid, 256, 0, stream>>>(params, cam, nullptr, n, out); break;
-        case 2: project_kernel<2, false, TW, TH><<<grid, 256, 0, stream>>>(params, cam, nullptr, n, out); break;
-        default: project_kernel<3, false, TW, TH><<<grid, 256, 0, stream>>>(params, cam, nullptr, n, out); break;
+        case 0: launch_step(project_kernel<0, false, TW, TH>, grid, 256, 0, stream, params, cam, nullptr, n, out);
+            break;
+        case 1: launch_step(project_kernel<1, false, TW, TH>, grid, 256, 0, stream, params, cam, nullptr, n, out);
+            break;
+        case 2: launch_step(project_kernel<2, false, TW, TH>, grid, 256, 0, stream, params, cam, nullptr, n, out);
+            break;
+        default: launch_step(project_kernel<3, false, TW, TH>, grid, 256, 0, stream, params, cam, nullptr, n, out);
+            break;
     }
 }
 
@@ -368,9 +374,8 @@ int launch_emit_records_culled(const uint32_t* sorted_ids, const int* record_sta
                                uint32_t* tile_keys, uint32_t* record_ids, int64_t capacity, int* overflow,
                                cudaStream_t stream) {
     if (n <= 0) return GSN_OK;
-    emit_records_culled<<<ceil_div(4ll * n, 256), 256, 0, stream>>>(sorted_ids, record_start, rects, means,
-                                                                    conic_opacity, n, tile_count_x, tile_keys,
-                                                                    record_ids, capacity, overflow);
+    launch_step(emit_records_culled, ceil_div(4ll * n, 256), 256, 0, stream, sorted_ids, record_start, rects, means,
+                conic_opacity, n, tile_count_x, tile_keys, record_ids, capacity, overflow);
     return launched(1);
 }
 

@@ -64,6 +64,7 @@ __device__ __forceinline__ void red_add_v4(float* address, float4 v) {
 
 template <bool kFast>
 __global__ void __launch_bounds__(kRasterThreads, 12) raster_backward_kernel(RasterBackwardArgs a) {
+    pdl_begin();
     __shared__ uint32_t s_id[kRasterBatch];
     __shared__ float2 s_mean[kRasterBatch];
     __shared__ float4 s_conic[kRasterBatch];
@@ -333,8 +334,8 @@ int launch_raster_backward(const RasterBackwardArgs& a, cudaStream_t stream) {
     int64_t tiles = static_cast<int64_t>(a.cam.tile_count_x) * a.cam.tile_count_y;
     if (tiles <= 0) return GSN_OK;
     if (!a.contributors) return GSN_ERR_INVALID_ARGUMENT;
-    if (a.fast) raster_backward_kernel<true><<<static_cast<unsigned>(tiles), kRasterThreads, 0, stream>>>(a);
-    else raster_backward_kernel<false><<<static_cast<unsigned>(tiles), kRasterThreads, 0, stream>>>(a);
+    if (a.fast) launch_step(raster_backward_kernel<true>, static_cast<unsigned>(tiles), kRasterThreads, 0, stream, a);
+    else launch_step(raster_backward_kernel<false>, static_cast<unsigned>(tiles), kRasterThreads, 0, stream, a);
     return launched(1);
 }
 

@@ -55,6 +55,7 @@ __device__ __forceinline__ Staged fetch(const RasterForwardArgs& a, int64_t r, i
 
 template <bool kFast, bool kCount>
 __global__ void __launch_bounds__(kRasterThreads) raster_forward_kernel(RasterForwardArgs a) {
+    pdl_begin();
     __shared__ float2 s_mean[kRasterBatch];
     __shared__ float4 s_conic[kRasterBatch];  // exact form: conic + opacity; fast form: fast_record terms
     __shared__ float3 s_color[kRasterBatch];
@@ -223,12 +224,12 @@ int launch_raster_forward(const RasterForwardArgs& a, cudaStream_t stream) {
     if (tiles <= 0) return GSN_OK;
     const unsigned grid = static_cast<unsigned>(tiles);
     if (a.pair_count) {
-        if (a.fast) raster_forward_kernel<true, true><<<grid, kRasterThreads, 0, stream>>>(a);
-        else raster_forward_kernel<false, true><<<grid, kRasterThreads, 0, stream>>>(a);
+        if (a.fast) launch_step(raster_forward_kernel<true, true>, grid, kRasterThreads, 0, stream, a);
+        else launch_step(raster_forward_kernel<false, true>, grid, kRasterThreads, 0, stream, a);
     } else if (a.fast) {
-        raster_forward_kernel<true, false><<<grid, kRasterThreads, 0, stream>>>(a);
+        launch_step(raster_forward_kernel<true, false>, grid, kRasterThreads, 0, stream, a);
     } else {
-        raster_forward_kernel<false, false><<<grid, kRasterThreads, 0, stream>>>(a);
+        launch_step(raster_forward_kernel<false, false>, grid, kRasterThreads, 0, stream, a);
     }
     return launched(1);
 }

@@ -47,6 +47,7 @@ __global__ void __launch_bounds__(kSortThreads) radix_upsweep(const uint32_t* __
                                                               uint32_t* __restrict__ block_hist,
                                                               size_t hist_stride,
                                                               uint32_t* __restrict__ digit_total) {
+    pdl_begin();
     __shared__ uint32_t hist[kSortWarps][kBins];
     const int n = load_count(n_dev, n_host);
     const int64_t start = static_cast<int64_t>(blockIdx.x) * kSortChunk;
@@ -82,6 +83,7 @@ __global__ void __launch_bounds__(kSortThreads) radix_scan(const int* n_dev, int
                                                            uint32_t* __restrict__ block_hist,
                                                            size_t hist_stride,
                                                            const uint32_t* __restrict__ digit_total) {
+    pdl_begin();
     __shared__ uint32_t warp_sums[kSortWarps];
     __shared__ uint32_t carry;
     const int n = load_count(n_dev, n_host);
@@ -153,6 +155,7 @@ __global__ void __launch_bounds__(kSortThreads) radix_downsweep(
     const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ values_in,
     uint32_t* __restrict__ keys_out, uint32_t* __restrict__ values_out, const int* n_dev, int n_host,
     int bit, uint32_t mask, int digit_bits, const uint32_t* __restrict__ block_hist, size_t hist_stride) {
+    pdl_begin();
     __shared__ uint32_t counts[kSortWarps][kBins];
     __shared__ uint32_t global_base[kBins];
     __shared__ uint32_t local_base[kBins];
@@ -253,6 +256,7 @@ __global__ void __launch_bounds__(kSortThreads) radix_downsweep(
 
 // Keys kept by a dropping first pass: the sum of its digit totals.
 __global__ void radix_kept(const uint32_t* __restrict__ digit_total, int* __restrict__ kept) {
+    pdl_begin();
     __shared__ uint32_t part[kSortWarps];
     uint32_t v = digit_total[threadIdx.x];
 #pragma unroll
@@ -328,6 +332,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_onepass(const int* in, cons
                                                              int n, const int* __restrict__ valid_dev, int* out,
                                                              unsigned long long* __restrict__ status,
                                                              int* __restrict__ ticket, int* __restrict__ error) {
+    pdl_begin();
     __shared__ int warp_sums[kScanThreads / 32];
     __shared__ int tile[kScanChunk];
     __shared__ int s_chunk;
@@ -421,6 +426,7 @@ __global__ void __launch_bounds__(256) emit_records(const uint32_t* __restrict__
                                                     uint32_t* __restrict__ tile_keys,
                                                     uint32_t* __restrict__ record_ids, int64_t capacity,
                                                     int* overflow) {
+    pdl_begin();
     const int64_t gidx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     const int64_t p = gidx >> 2;
     const int sub = static_cast<int>(gidx & 3);
@@ -455,6 +461,7 @@ constexpr int kRangeItems = 8;
 
 __global__ void __launch_bounds__(256) tile_ranges(const uint32_t* __restrict__ tiles, const int* n_dev,
                                                    int max_records, int tile_count, int64_t* __restrict__ offsets) {
+    pdl_begin();
     const int n = min(*n_dev, max_records);
     const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
     const int64_t first = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -529,32 +536,33 @@ static int radix_sort_impl(uint32_t* keys, uint32_t* values, uint32_t* keys_alt,
         uint32_t* dt = scratch.digit_total + kBins * p;
         const bool drop = kept_device && p == 0;
         if (drop)
-            radix_upsweep<true><<<blocks, kSortThreads, 0, stream>>>(kin, count, max_count, bit, mask,
-                                                                     scratch.block_hist, scratch.max_blocks, dt);
+            launch_step(radix_upsweep<true>, blocks, kSortThreads, 0, stream, kin, count, max_count, bit, mask,
+                        scratch.block_hist, scratch.max_blocks, dt);
         else
-            radix_upsweep<false><<<blocks, kSortThreads, 0, stream>>>(kin, count, max_count, bit, mask,
-                                                                      scratch.block_hist, scratch.max_blocks, dt);
-        radix_scan<<<bins, kSortThreads, 0, stream>>>(count, max_count, scratch.block_hist, scratch.max_blocks, dt);
+            launch_step(radix_upsweep<false>, blocks, kSortThreads, 0, stream, kin, count, max_count, bit, mask,
+                        scratch.block_hist, scratch.max_blocks, dt);
+        launch_step(radix_scan, bins, kSortThreads, 0, stream, count, max_count, scratch.block_hist,
+                    scratch.max_blocks, dt);
         const uint32_t* vsrc = identity_values && p == 0 ? nullptr : vin;
         if (identity_values && p == 0 && drop)
-            radix_downsweep<true, true><<<blocks, kSortThreads, 0, stream>>>(
+            launch_step(radix_downsweep<true, true>, blocks, kSortThreads, 0, stream,
                 kin, vsrc, kout, vout, count, max_count, bit, mask, digit_bits, scratch.block_hist,
                 scratch.max_blocks);
         else if (identity_values && p == 0)
-            radix_downsweep<true, false><<<blocks, kSortThreads, 0, stream>>>(
+            launch_step(radix_downsweep<true, false>, blocks, kSortThreads, 0, stream,
                 kin, vsrc, kout, vout, count, max_count, bit, mask, digit_bits, scratch.block_hist,
                 scratch.max_blocks);
         else if (drop)
-            radix_downsweep<false, true><<<blocks, kSortThreads, 0, stream>>>(
+            launch_step(radix_downsweep<false, true>, blocks, kSortThreads, 0, stream,
                 kin, vsrc, kout, vout, count, max_count, bit, mask, digit_bits, scratch.block_hist,
                 scratch.max_blocks);
         else
-            radix_downsweep<false, false><<<blocks, kSortThreads, 0, stream>>>(
+            launch_step(radix_downsweep<false, false>, blocks, kSortThreads, 0, stream,
                 kin, vsrc, kout, vout, count, max_count, bit, mask, digit_bits, scratch.block_hist,
                 scratch.max_blocks);
         if (drop) {
             // later passes (and the caller) see only the kept keys
-            radix_kept<<<1, kBins, 0, stream>>>(dt, kept_device);
+            launch_step(radix_kept, 1, kBins, 0, stream, dt, kept_device);
             count = kept_device;
         }
         uint32_t* tk = kin; kin = kout; kout = tk;
@@ -640,7 +648,8 @@ int launch_exclusive_scan(const int* in, const uint32_t* gather, int* out, int n
     int* ticket = static_cast<int*>(scratch);
     auto* status = reinterpret_cast<unsigned long long*>(static_cast<char*>(scratch) + 16);
     if (cudaMemsetAsync(scratch, 0, scan_scratch_bytes(n), stream) != cudaSuccess) return GSN_ERR_CUDA;
-    scan_onepass<<<blocks, kScanThreads, 0, stream>>>(in, gather, n, valid_device, out, status, ticket, ticket + 1);
+    launch_step(scan_onepass, blocks, kScanThreads, 0, stream, in, gather, n, valid_device, out, status, ticket,
+                ticket + 1);
     return launched(1);
 }
 
@@ -648,8 +657,8 @@ int launch_emit_records(const uint32_t* sorted_ids, const int* record_start, con
                         int tile_count_x, uint32_t* tile_keys, uint32_t* record_ids, int64_t capacity,
                         int* overflow, cudaStream_t stream) {
     if (n <= 0) return GSN_OK;
-    emit_records<<<ceil_div(4ll * n, 256), 256, 0, stream>>>(sorted_ids, record_start, rects, n, tile_count_x,
-                                                             tile_keys, record_ids, capacity, overflow);
+    launch_step(emit_records, ceil_div(4ll * n, 256), 256, 0, stream, sorted_ids, record_start, rects, n,
+                tile_count_x, tile_keys, record_ids, capacity, overflow);
     return launched(1);
 }
 
@@ -659,8 +668,8 @@ int launch_tile_ranges(const uint32_t* sorted_tiles, const int* record_count_dev
     int64_t work = runs > tile_count + 1 ? runs : tile_count + 1;
     int blocks = static_cast<int>(ceil_div(work, 256));
     if (blocks > 148 * 32) blocks = 148 * 32;
-    tile_ranges<<<blocks, 256, 0, stream>>>(sorted_tiles, record_count_device, max_records, tile_count,
-                                           offsets);
+    launch_step(tile_ranges, blocks, 256, 0, stream, sorted_tiles, record_count_device, max_records, tile_count,
+                offsets);
     return launched(1);
 }
 

@@ -81,6 +81,7 @@ def lib():
         "gsn_device_alloc": ([ctypes.c_size_t, P(vp)], i32),
         "gsn_device_free": ([vp], i32),
         "gsn_kernel_launch_count": ([], ctypes.c_uint64),
+        "gsn_set_programmatic_launch": ([i32], i32),
         "gsn_profile_enable": ([i32], i32),
         "gsn_profile_collect": ([P(ctypes.c_double), i32], i32),
         "gsn_stage_name": ([i32], ctypes.c_char_p),
@@ -193,6 +194,11 @@ class Renderer:
 
 def launch_count():
     return int(lib().gsn_kernel_launch_count())
+
+
+def set_programmatic_launch(on=True):
+    """Programmatic dependent launch of the training step's kernels (default on)."""
+    _check(lib().gsn_set_programmatic_launch(int(bool(on))), "set_programmatic_launch")
 
 
 def profile_enable(on=True):

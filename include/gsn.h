@@ -50,6 +50,14 @@ int gsn_stream_synchronize(void* stream);
 /* Number of this library's kernel launches since load (process-wide). */
 uint64_t gsn_kernel_launch_count(void);
 
+/* Programmatic dependent launch of the training step's kernels (gs-native
+ * extension, process-wide, on by default): on an eager stream each step kernel
+ * is launched with programmatic stream serialization and waits for its
+ * predecessor on the device, so a grid's CTAs are scheduled while the one
+ * before it drains. Launches captured into a CUDA graph never use it. Results
+ * are the same either way. */
+int gsn_set_programmatic_launch(int enabled);
+
 /* Stage profiler: when enabled, stage boundaries record CUDA events on the
  * stream of the stage; gsn_profile_collect synchronises and writes the device
  * milliseconds per stage since the last collect into ms[0..count) (stage
