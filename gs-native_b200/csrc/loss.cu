@@ -15,6 +15,8 @@
 #include "common.cuh"
 #include "kernels.h"
 
+#include <atomic>
+
 namespace gsn {
 
 namespace {
@@ -534,18 +536,19 @@ int launch_loss_gradient(const float* image, const uint8_t* target, const StepFr
     if (width <= 0 || height <= 0) return GSN_ERR_INVALID_ARGUMENT;
     if (sums && cudaMemsetAsync(sums, 0, 3 * sizeof(double), stream) != cudaSuccess) return GSN_ERR_CUDA;
     // the dynamic shared-memory opt-in is a per-device, per-kernel attribute
-    static bool configured[64][2] = {};
+    // set once per device and form; concurrent host threads may both set it
+    static std::atomic<bool> configured[64][2] = {};
     int device = 0;
     if (cudaGetDevice(&device) != cudaSuccess) return GSN_ERR_CUDA;
     if (device < 0 || device >= 64) return GSN_ERR_CUDA;
-    if (!configured[device][fast ? 1 : 0]) {
+    if (!configured[device][fast ? 1 : 0].load()) {
         const cudaError_t e =
             fast ? cudaFuncSetAttribute(loss_gradient_fast_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         static_cast<int>(kSmemBytes))
                  : cudaFuncSetAttribute(loss_gradient_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         static_cast<int>(kSmemBytes));
         if (e != cudaSuccess) return GSN_ERR_CUDA;
-        configured[device][fast ? 1 : 0] = true;
+        configured[device][fast ? 1 : 0].store(true);
     }
     dim3 grid(ceil_div(width, kT), ceil_div(height, kT), 3);
     if (fast)
