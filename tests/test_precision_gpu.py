@@ -181,17 +181,24 @@ def test_trainer_precision_form_trains_like_plain_form():
         images.append((img * 255).round().clamp(0, 255).to(t.uint8).cpu().numpy())
     points, colors = scenes.initial_points(hidden, 5000, 2)
     train_c, train_i = cams[1:], images[1:]
+    # Two runs per form: runs differ only through the order of the backward's
+    # float atomics, which the density decisions amplify (single runs of this
+    # 1,500-iteration scene spread by a few tenths of a dB, rarely more than 1
+    # dB), so the forms are compared on their means.
     result = {}
     for precision in (0, 1):
-        opts = gsn.TrainingOptions.defaults(densify_from=100, densify_until=600, densify_interval=100,
-                                            opacity_reset_interval=100000, precision=precision)
-        tr = gsn.Trainer()
-        assert tr.initialize(train_c, train_i, points, colors, opts) == 0
-        before, _ = tr.evaluate(cams[:1], images[:1])
-        assert tr.train(1500) == 0
-        after, _ = tr.evaluate(cams[:1], images[:1])
-        result[precision] = (before, after, tr.state()["count"])
-        tr.close()
+        runs = []
+        for _ in range(2):
+            opts = gsn.TrainingOptions.defaults(densify_from=100, densify_until=600, densify_interval=100,
+                                                opacity_reset_interval=100000, precision=precision)
+            tr = gsn.Trainer()
+            assert tr.initialize(train_c, train_i, points, colors, opts) == 0
+            before, _ = tr.evaluate(cams[:1], images[:1])
+            assert tr.train(1500) == 0
+            after, _ = tr.evaluate(cams[:1], images[:1])
+            runs.append((before, after, tr.state()["count"]))
+            tr.close()
+        result[precision] = (runs[0][0], float(np.mean([r[1] for r in runs])), runs)
     assert result[0][1] > result[0][0] + 3.0
     assert result[1][1] > result[1][0] + 3.0
     assert abs(result[1][1] - result[0][1]) < 0.5, result
