@@ -181,14 +181,17 @@ def test_trainer_precision_form_trains_like_plain_form():
         images.append((img * 255).round().clamp(0, 255).to(t.uint8).cpu().numpy())
     points, colors = scenes.initial_points(hidden, 5000, 2)
     train_c, train_i = cams[1:], images[1:]
-    # Two runs per form: runs differ only through the order of the backward's
-    # float atomics, which the density decisions amplify (single runs of this
-    # 1,500-iteration scene spread by a few tenths of a dB, rarely more than 1
-    # dB), so the forms are compared on their means.
+    # Three runs per form, compared on their medians. Runs differ only through
+    # the order of the backward's float atomics, which the density decisions of
+    # this small 1,500-iteration scene amplify: over 8 fresh runs each, plain
+    # ended at 19.0-19.5 dB and the precision form (bf16 SH storage with
+    # stochastic rounding) at 18.5-19.6 dB, with single runs in the test suite
+    # as low as 17.5 dB. The full-scale held-out gate in bench.py measures the
+    # forms' quality; this test checks that training is not systematically off.
     result = {}
     for precision in (0, 1):
         runs = []
-        for _ in range(2):
+        for _ in range(3):
             opts = gsn.TrainingOptions.defaults(densify_from=100, densify_until=600, densify_interval=100,
                                                 opacity_reset_interval=100000, precision=precision)
             tr = gsn.Trainer()
@@ -198,7 +201,7 @@ def test_trainer_precision_form_trains_like_plain_form():
             after, _ = tr.evaluate(cams[:1], images[:1])
             runs.append((before, after, tr.state()["count"]))
             tr.close()
-        result[precision] = (runs[0][0], float(np.mean([r[1] for r in runs])), runs)
+        result[precision] = (runs[0][0], float(np.median([r[1] for r in runs])), runs)
     assert result[0][1] > result[0][0] + 3.0
     assert result[1][1] > result[1][0] + 3.0
     assert abs(result[1][1] - result[0][1]) < 0.5, result
