@@ -241,6 +241,10 @@ __device__ __forceinline__ void chain_rule(const float* __restrict__ p, int64_t 
 // the parameter step differs from the reference's by at most a few ulps of
 // the step.
 // PTX sqrt.approx.f32 (relative error within 2^-23 on normal inputs).
+__device__ __forceinline__ void prefetch_l2(const float* address) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(address));
+}
+
 __device__ __forceinline__ float sqrt_approx(float x) {
     float y;
     asm("sqrt.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
@@ -331,6 +335,16 @@ __global__ void __launch_bounds__(256, 2) gaussian_update_kernel(GaussianUpdateA
     float adu = s2.y, adv = s2.z;
     const bool visible = a.tile_counts[i] > 0;
     const gsn_camera cam = a.frame ? a.frame->cam : a.cam;
+    // the moment rows Adam will read are fetched into L2 while the chain rule
+    // computes: bytes in flight that cost no registers (the kernel runs at 128
+    // registers and is bound by DRAM latency)
+    if (a.m && !(a.sparse && !visible)) {
+#pragma unroll 2
+        for (int r = 0; r < physical_rows<kBf16>(); ++r) {
+            prefetch_l2(a.m + static_cast<int64_t>(r) * N + i);
+            prefetch_l2(a.v + static_cast<int64_t>(r) * N + i);
+        }
+    }
 
     // view-space statistics (solver.cu:468-490) and round accumulation
     // (density_controller.cu:280-295)
