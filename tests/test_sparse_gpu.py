@@ -120,19 +120,26 @@ def test_sparse_adam_skips_invisible_gaussians():
 def test_training_with_spatial_order_and_sparse_adam():
     import test_trainer_gpu as tt
     cams, images, points, colors = tt.ring_scene()
+    # Three runs per form, compared on their medians: runs differ only through
+    # the order of the backward's float atomics, and plain alone spread over
+    # 32.49-32.87 dB across eight runs of this scene.
     out = {}
     for form in ("plain", "fast"):
         fast = form == "fast"
-        opts = gsn.TrainingOptions.defaults(densify_from=100, densify_until=700, densify_interval=100,
-                                            exact_culling=int(fast), sparse_adam=int(fast), spatial_order=int(fast),
-                                            log_density=1)
-        tr = gsn.Trainer()
-        assert tr.initialize(cams, images, points, colors, opts) == 0
-        assert tr.train(900) == 0
-        log = tr.density_log()
-        parents = host(log["parents"], np.int32, log["after"])
-        assert ((parents >= -1) & (parents < log["before"])).all()
-        out[form] = (tr.evaluate_metrics(cams, images)["psnr"], tr.state()["count"])
+        runs = []
+        for _ in range(3):
+            opts = gsn.TrainingOptions.defaults(densify_from=100, densify_until=700, densify_interval=100,
+                                                exact_culling=int(fast), sparse_adam=int(fast),
+                                                spatial_order=int(fast), log_density=1)
+            tr = gsn.Trainer()
+            assert tr.initialize(cams, images, points, colors, opts) == 0
+            assert tr.train(900) == 0
+            log = tr.density_log()
+            parents = host(log["parents"], np.int32, log["after"])
+            assert ((parents >= -1) & (parents < log["before"])).all()
+            runs.append((tr.evaluate_metrics(cams, images)["psnr"], tr.state()["count"]))
+            tr.close()
+        out[form] = (float(np.median([r[0] for r in runs])), float(np.median([r[1] for r in runs])), runs)
     # the sparse update changes the optimisation (no momentum steps off-view);
     # on this 10-view ring it stays within the run-to-run spread of plain
     assert abs(out["fast"][0] - out["plain"][0]) < 0.35, out
