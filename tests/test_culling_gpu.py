@@ -118,6 +118,9 @@ def test_training_with_culling_matches_plain():
     # plain runs of this 10-view scene spread by up to ~0.3 dB from one process
     # to the next, and their Gaussian counts by about 1 %, so only loose bounds
     # are meaningful here
-    p, c = _train(0, 900, 700), _train(1, 900, 700)
-    assert abs(c[0] - p[0]) < 0.35
-    assert abs(c[1] - p[1]) <= 0.03 * p[1]
+    # so each form is run three times and compared on its medians
+    runs = {culled: [_train(culled, 900, 700) for _ in range(3)] for culled in (0, 1)}
+    p = [float(np.median([r[k] for r in runs[0]])) for k in (0, 1)]
+    c = [float(np.median([r[k] for r in runs[1]])) for k in (0, 1)]
+    assert abs(c[0] - p[0]) < 0.35, runs
+    assert abs(c[1] - p[1]) <= 0.03 * p[1], runs

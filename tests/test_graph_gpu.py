@@ -139,5 +139,8 @@ def test_trainer_graph_steady_state_trains_like_eager():
     that run only checks the counts and a loose PSNR bound."""
     out = _graph_vs_eager(100000, 100, 460)
     assert out[0][2] == out[1][2] and abs(out[0][0] - out[1][0]) < 0.03, out
-    out = _graph_vs_eager(100, 400, 460)
-    assert abs(out[0][2] - out[1][2]) <= 0.01 * out[0][2] and abs(out[0][0] - out[1][0]) < 0.3, out
+    # three runs of each, compared on their medians
+    runs = [_graph_vs_eager(100, 400, 460) for _ in range(3)]
+    psnr = [float(np.median([r[g][0] for r in runs])) for g in (0, 1)]
+    count = [float(np.median([r[g][2] for r in runs])) for g in (0, 1)]
+    assert abs(count[0] - count[1]) <= 0.01 * count[0] and abs(psnr[0] - psnr[1]) < 0.3, runs
