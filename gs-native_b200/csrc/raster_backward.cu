@@ -342,6 +342,7 @@ __global__ void __launch_bounds__(kRasterThreads, 12) raster_backward_kernel(Ras
 // slot with plain stores, since this warp alone writes them.
 constexpr int kTilePix = 8;     // pixels per lane
 constexpr int kTileBatch = 64;  // records staged per batch (two per lane)
+constexpr int kTileChunks = kTileBatch / 32;
 
 __global__ void __launch_bounds__(32) raster_backward_tile_kernel(RasterBackwardArgs a) {
     pdl_begin();
@@ -408,9 +409,9 @@ __global__ void __launch_bounds__(32) raster_backward_tile_kernel(RasterBackward
         const int batch = static_cast<int>(min(static_cast<int64_t>(kTileBatch), end - base));
         // stage two records per lane; the take flags of the batch (a record some
         // pixel of the tile took in the forward pass) become two ballots
-        uint32_t took[2];
+        uint32_t took[kTileChunks];
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
+        for (int h = 0; h < kTileChunks; ++h) {
             const int slot = lane + h * 32;
             bool flag = false;
             if (slot < batch) {
@@ -434,7 +435,7 @@ __global__ void __launch_bounds__(32) raster_backward_tile_kernel(RasterBackward
         const int rel = static_cast<int>(base - begin);
         const int wend = min(batch, bound - rel);  // records below the tile's bound
 #pragma unroll 1
-        for (int h = 0; h < 2; ++h) {
+        for (int h = 0; h < kTileChunks; ++h) {
             const int lim = wend - h * 32;
             if (lim <= 0) break;
             uint32_t m = lim < 32 ? took[h] & ((1u << lim) - 1u) : took[h];
