@@ -69,11 +69,11 @@ MODEL_GAUSSIANS = 1_200_000
 # DRAM bytes (read + write) of one gaussian_update launch on this workload, per
 # update form, from the ncu captures summarised in profiles/.
 NCU_TRAFFIC = {
-    "dense": (900_431_104 + 801_656_576,
+    "dense": (939_872_768 + 794_836_736,
               "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/gaussian_update_plain_1.2M.md"),
     "sparse": (604_525_312 + 483_656_704,
                "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/gaussian_update_sparse_1.2M.md"),
-    "sparse_bf16": (385_936_896 + 276_065_792,
+    "sparse_bf16": (380_198_656 + 268_296_960,
                     "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/gaussian_update_bf16_sparse_1.2M.md"),
 }
 
