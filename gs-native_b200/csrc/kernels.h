@@ -78,7 +78,7 @@ int launch_project_tiled(const float* params, int n, const gsn_camera& cam, int 
 // device memory, so no host sync is needed.
 struct RadixSortScratch {
     uint32_t* block_hist;   // [256 * max_blocks]
-    uint32_t* digit_total;  // [256 * passes]
+    uint32_t* digit_total;  // [passes][16 partial copies][256]
     size_t max_blocks;
 };
 size_t radix_sort_scratch_bytes(int max_count);

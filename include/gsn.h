@@ -94,7 +94,7 @@ int gsn_sort_pairs(uint32_t* keys, uint32_t* values, uint32_t* keys_alt, uint32_
  * take the device-wide synchronisation that cudaMalloc/cudaFree imply. The caller
  * still passes all four key/value arrays; the sort's histogram scratch lives in a
  * static device array inside the library, sized for at most
- * GSN_SORT_NOALLOC_MAX_COUNT pairs (5.6 MB, reserved on every GPU that loads the
+ * GSN_SORT_NOALLOC_MAX_COUNT pairs (5.7 MB, reserved on every GPU that loads the
  * library until the process exits). Larger counts return GSN_ERR_CAPACITY and
  * launch nothing. The function calls no cudaMalloc/cudaFree.
  *
