@@ -1,4 +1,4 @@
-"""Exact tile culling (sort.cu cull_row_span): the culled renderer emits a
+"""Exact tile culling (project.cu cull_row_span): the culled renderer emits a
 subset of the reference's records; the image, the per-pixel work and the
 gradients are unchanged; every dropped record is one whose alpha stays below
 1/255 at every pixel of its tile (checked in FP64 from the device's own
