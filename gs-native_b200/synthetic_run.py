@@ -138,6 +138,7 @@ def main():
     p.add_argument("--sparse", action="store_true", help="visibility-masked Adam on the Morton-ordered model")
     p.add_argument("--fast", action="store_true", help="fast blend arithmetic (Horner power, hardware exp2)")
     p.add_argument("--fp32-ssim", action="store_true", help="with --precision: the fp32 SSIM kernel, not tcgen05")
+    p.add_argument("--density-seed", type=int, default=0, help="seed of the density controller's random draws")
     args = p.parse_args()
     import torch
 
@@ -148,7 +149,8 @@ def main():
     opts = gsn.TrainingOptions.defaults(max_gaussians=args.cap, precision=int(args.precision),
                                         graph=int(args.graph), exact_culling=int(args.culled),
                                         sparse_adam=int(args.sparse), spatial_order=int(args.sparse),
-                                        fast_blend=int(args.fast), fp32_ssim=int(args.fp32_ssim))
+                                        fast_blend=int(args.fast), fp32_ssim=int(args.fp32_ssim),
+                                        density_seed=args.density_seed)
     trainer = gsn.Trainer()
     assert trainer.initialize(train, train_images, points, colors, opts) == 0
     torch.cuda.synchronize()
@@ -175,6 +177,7 @@ def main():
         "iters_per_s": round(args.iterations / (device_ms / 1000.0), 2), "gaussians": st["count"],
         "psnr_test_db": round(psnr, 4), "loss_test": round(loss, 6), "psnr_train_subset_db": round(psnr_train, 4),
         "setup_s": round(setup_s, 1), "resolution": [args.width, args.height], "cap": args.cap,
+        "density_seed": args.density_seed,
         "form": ("precision_bf16" + ("_fp32ssim" if args.fp32_ssim else "") if args.precision else "plain_fp32") +
                 ("_culled" if args.culled else "") +
                 ("_sparse" if args.sparse else "") + ("_fast" if args.fast else "") + ("_graph" if args.graph else ""),
