@@ -71,7 +71,7 @@ MODEL_GAUSSIANS = 1_200_000
 NCU_TRAFFIC = {
     "dense": (939_872_768 + 794_836_736,
               "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/gaussian_update_plain_1.2M.md"),
-    "sparse": (604_525_312 + 483_656_704,
+    "sparse": (615_015_680 + 483_678_208,
                "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/gaussian_update_sparse_1.2M.md"),
     "sparse_bf16": (380_198_656 + 268_296_960,
                     "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/gaussian_update_bf16_sparse_1.2M.md"),
