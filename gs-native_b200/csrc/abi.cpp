@@ -343,6 +343,12 @@ int gsn_solver_set_sparse_adam(gsn_solver* s, int enabled) {
     return GSN_OK;
 }
 
+int gsn_solver_set_lazy_moment_decay(gsn_solver* s, int enabled) {
+    if (!s) return GSN_ERR_INVALID_ARGUMENT;
+    s->impl.SetLazyMomentDecay(enabled != 0);
+    return GSN_OK;
+}
+
 int gsn_solver_status(gsn_solver* s, int* status) {
     if (!s || !status) return GSN_ERR_INVALID_ARGUMENT;
     *status = GSN_OK;
@@ -587,6 +593,12 @@ int gsn_trainer_destroy(gsn_trainer* t) {
 int gsn_trainer_set_stream(gsn_trainer* t, void* stream) {
     if (!t) return GSN_ERR_INVALID_ARGUMENT;
     t->impl.SetStream(AsStream(stream));
+    return GSN_OK;
+}
+
+int gsn_trainer_set_lazy_moment_decay(gsn_trainer* t, int enabled) {
+    if (!t) return GSN_ERR_INVALID_ARGUMENT;
+    t->impl.GetSolver().SetLazyMomentDecay(enabled != 0);
     return GSN_OK;
 }
 

@@ -251,10 +251,12 @@ __device__ __forceinline__ float sqrt_approx(float x) {
     return y;
 }
 
-template <int CNT>
+// kLazy: the stored moments are first scaled by d1 = b1^k and d2 = b2^k, the
+// decay of the k steps the Gaussian skipped under the visibility-masked update.
+template <int CNT, bool kLazy = false>
 __device__ __forceinline__ void adam_rows(float* __restrict__ P, float* __restrict__ M, float* __restrict__ V,
                                           int64_t N, int i, int row0, const float* g, const float* lr, float c1,
-                                          float c2) {
+                                          float c2, float d1 = 1.0f, float d2 = 1.0f) {
     float p[CNT], m[CNT], v[CNT];
 #pragma unroll
     for (int r = 0; r < CNT; ++r) {
@@ -262,6 +264,10 @@ __device__ __forceinline__ void adam_rows(float* __restrict__ P, float* __restri
         p[r] = P[idx];
         m[r] = M[idx];
         v[r] = V[idx];
+        if constexpr (kLazy) {
+            m[r] *= d1;
+            v[r] *= d2;
+        }
     }
 #pragma unroll
     for (int r = 0; r < CNT; ++r) {
@@ -284,10 +290,11 @@ __device__ __forceinline__ void adam_rows(float* __restrict__ P, float* __restri
 // Gaussian per 32-bit word, the parameters and both moments), computed in fp32
 // and written back with stochastic rounding; coefficient by coefficient the
 // noise stream is the one a row-by-row pass draws.
-template <int PAIRS>
+template <int PAIRS, bool kLazy = false>
 __device__ __forceinline__ void adam_pairs_bf16(uint32_t* __restrict__ P, uint32_t* __restrict__ M,
                                                 uint32_t* __restrict__ V, int64_t N, int i, int pair0,
-                                                const float* g, const float* lr, float c1, float c2, uint32_t& rng) {
+                                                const float* g, const float* lr, float c1, float c2, uint32_t& rng,
+                                                float d1 = 1.0f, float d2 = 1.0f) {
     // all of the group's words first (three per pair), so they are in flight
     // together; then pair by pair: widen, step, round, narrow, store
     uint32_t pw[PAIRS], mw[PAIRS], vw[PAIRS];
@@ -305,8 +312,12 @@ __device__ __forceinline__ void adam_pairs_bf16(uint32_t* __restrict__ P, uint32
         for (int h = 0; h < 2; ++h) {
             const int r = 2 * q + h;
             float p = h ? bf16_hi(pw[q]) : bf16_lo(pw[q]);
-            const float m = h ? bf16_hi(mw[q]) : bf16_lo(mw[q]);
-            const float v = h ? bf16_hi(vw[q]) : bf16_lo(vw[q]);
+            float m = h ? bf16_hi(mw[q]) : bf16_lo(mw[q]);
+            float v = h ? bf16_hi(vw[q]) : bf16_lo(vw[q]);
+            if constexpr (kLazy) {
+                m *= d1;
+                v *= d2;
+            }
             const float first = 0.9f * m + 0.1f * g[r];
             const float second = 0.999f * v + 0.001f * g[r] * g[r];
             p -= __fdividef(lr[r] * (first * c1), sqrt_approx(second * c2) + 1e-15f);
@@ -323,7 +334,11 @@ __device__ __forceinline__ void adam_pairs_bf16(uint32_t* __restrict__ P, uint32
     }
 }
 
-template <int D, bool kBf16>
+// log2 of Adam's decay rates, for the lazy decay b^k = 2^(k log2 b)
+constexpr float kLog2Beta1 = -0.15200309344504995f;    // log2(0.9)
+constexpr float kLog2Beta2 = -0.0014434168696687032f;  // log2(0.999)
+
+template <int D, bool kBf16, bool kLazy>
 __global__ void __launch_bounds__(256, 2) gaussian_update_kernel(GaussianUpdateArgs a) {
     pdl_begin();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -418,7 +433,19 @@ __global__ void __launch_bounds__(256, 2) gaussian_update_kernel(GaussianUpdateA
     const float c1 = a.frame ? a.frame->c1 : a.c1;
     const float c2 = a.frame ? a.frame->c2 : a.c2;
     const float lr_geo[10] = {lr0, lr0, lr0, a.lr[1], a.lr[1], a.lr[1], a.lr[2], a.lr[2], a.lr[2], a.lr[3]};
-    adam_rows<10>(P, M, V, N, i, 0, ch.g, lr_geo, c1, c2);
+    // lazy moment decay: the moments decay as a dense step with a zero gradient
+    // would have decayed them over the steps this Gaussian skipped (its
+    // parameters do not take those steps' momentum moves); step 0 in last_step
+    // means unknown (after a remap), which decays nothing
+    float d1 = 1.0f, d2 = 1.0f;
+    if constexpr (kLazy) {
+        const uint32_t last = a.last_step[i];
+        const uint32_t skipped = last != 0u && a.step > last + 1u ? a.step - last - 1u : 0u;
+        d1 = exp2f(static_cast<float>(skipped) * kLog2Beta1);
+        d2 = exp2f(static_cast<float>(skipped) * kLog2Beta2);
+        a.last_step[i] = a.step;
+    }
+    adam_rows<10, kLazy>(P, M, V, N, i, 0, ch.g, lr_geo, c1, c2, d1, d2);
     if constexpr (kBf16) {
         // one group per colour channel: its 16 coefficients are 8 pair words
         // per array, the bytes in flight of the fp32 form's 8-row groups
@@ -432,9 +459,10 @@ __global__ void __launch_bounds__(256, 2) gaussian_update_kernel(GaussianUpdateA
             float g16[kShStride];
 #pragma unroll
             for (int k = 0; k < kShStride; ++k) g16[k] = k < K ? ch.grgb[c] * ch.basis[k] : 0.0f;
-            adam_pairs_bf16<kShStride / 2>(reinterpret_cast<uint32_t*>(P), reinterpret_cast<uint32_t*>(M),
-                                           reinterpret_cast<uint32_t*>(V), N, i,
-                                           kGeometryRows + c * (kShStride / 2), g16, lr_sh, c1, c2, rng);
+            adam_pairs_bf16<kShStride / 2, kLazy>(reinterpret_cast<uint32_t*>(P), reinterpret_cast<uint32_t*>(M),
+                                                  reinterpret_cast<uint32_t*>(V), N, i,
+                                                  kGeometryRows + c * (kShStride / 2), g16, lr_sh, c1, c2, rng, d1,
+                                                  d2);
         }
     } else {
         float lr_sh[8];
@@ -448,7 +476,8 @@ __global__ void __launch_bounds__(256, 2) gaussian_update_kernel(GaussianUpdateA
 #pragma unroll
                 for (int k = 0; k < 8; ++k) g8[k] = half * 8 + k < K ? ch.grgb[c] * ch.basis[half * 8 + k] : 0.0f;
                 lr_sh[0] = half == 0 ? a.lr[4] : a.lr[5];
-                adam_rows<8>(P, M, V, N, i, GSN_SH_INDEX + c * kShStride + half * 8, g8, lr_sh, c1, c2);
+                adam_rows<8, kLazy>(P, M, V, N, i, GSN_SH_INDEX + c * kShStride + half * 8, g8, lr_sh, c1, c2, d1,
+                                    d2);
             }
         }
     }
@@ -475,28 +504,36 @@ __global__ void remap_moments_kernel(const int* __restrict__ parents, const floa
     }
 }
 
+template <bool kLazy>
+int launch_update(const GaussianUpdateArgs& a, int d, dim3 grid, cudaStream_t stream) {
+    if (a.bf16_sh) {
+        switch (d) {
+            case 0: launch_step(gaussian_update_kernel<0, true, kLazy>, grid, 256, 0, stream, a); break;
+            case 1: launch_step(gaussian_update_kernel<1, true, kLazy>, grid, 256, 0, stream, a); break;
+            case 2: launch_step(gaussian_update_kernel<2, true, kLazy>, grid, 256, 0, stream, a); break;
+            default: launch_step(gaussian_update_kernel<3, true, kLazy>, grid, 256, 0, stream, a); break;
+        }
+    } else {
+        switch (d) {
+            case 0: launch_step(gaussian_update_kernel<0, false, kLazy>, grid, 256, 0, stream, a); break;
+            case 1: launch_step(gaussian_update_kernel<1, false, kLazy>, grid, 256, 0, stream, a); break;
+            case 2: launch_step(gaussian_update_kernel<2, false, kLazy>, grid, 256, 0, stream, a); break;
+            default: launch_step(gaussian_update_kernel<3, false, kLazy>, grid, 256, 0, stream, a); break;
+        }
+    }
+    return launched(1);
+}
+
 }  // namespace
 
 int launch_gaussian_update(const GaussianUpdateArgs& a, int sh_degree, cudaStream_t stream) {
     if (a.n <= 0) return GSN_OK;
     dim3 grid(ceil_div(a.n, 256));
     const int d = sh_degree < 0 ? 0 : (sh_degree > 3 ? 3 : sh_degree);
-    if (a.bf16_sh) {
-        switch (d) {
-            case 0: launch_step(gaussian_update_kernel<0, true>, grid, 256, 0, stream, a); break;
-            case 1: launch_step(gaussian_update_kernel<1, true>, grid, 256, 0, stream, a); break;
-            case 2: launch_step(gaussian_update_kernel<2, true>, grid, 256, 0, stream, a); break;
-            default: launch_step(gaussian_update_kernel<3, true>, grid, 256, 0, stream, a); break;
-        }
-    } else {
-        switch (d) {
-            case 0: launch_step(gaussian_update_kernel<0, false>, grid, 256, 0, stream, a); break;
-            case 1: launch_step(gaussian_update_kernel<1, false>, grid, 256, 0, stream, a); break;
-            case 2: launch_step(gaussian_update_kernel<2, false>, grid, 256, 0, stream, a); break;
-            default: launch_step(gaussian_update_kernel<3, false>, grid, 256, 0, stream, a); break;
-        }
-    }
-    return launched(1);
+    if (a.last_step && !a.sparse) return GSN_ERR_INVALID_ARGUMENT;  // lazy decay belongs to the sparse update
+    if (a.last_step)
+        return launch_update<true>(a, d, grid, stream);
+    return launch_update<false>(a, d, grid, stream);
 }
 
 int launch_remap_moments(const int* parents, const float* prev_m, const float* prev_v, float* m, float* v,

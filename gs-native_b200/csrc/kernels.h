@@ -221,6 +221,11 @@ struct GaussianUpdateArgs {
     bool bf16_sh;             // precision-form layout of params, m and v (10 fp32 + 48 bf16 rows)
     uint32_t seed;            // stochastic-rounding seed of the step (precision form)
     bool sparse;              // visibility-masked Adam: Gaussians with tile_counts == 0 keep p, m, v
+    // optional with sparse: lazy moment decay. last_step[i] is the step that last
+    // updated Gaussian i (0: unknown); a visible Gaussian's moments first decay by
+    // b1^k, b2^k for the k steps it skipped, and last_step[i] becomes step
+    uint32_t* last_step;
+    uint32_t step;
     // optional statistics of the learned density policy (all set or all null),
     // updated for Gaussians visible in the frame: round maximum of the screen
     // radius, round sums of depth and depth^2, and the norms of this step's

@@ -312,6 +312,10 @@ class Solver:
         fn = declare("gsn_solver_set_sparse_adam", [ctypes.c_void_p, ctypes.c_int])
         _check(fn(self.handle, int(bool(enabled))), "set_sparse_adam")
 
+    def set_lazy_moment_decay(self, enabled=True):
+        fn = declare("gsn_solver_set_lazy_moment_decay", [ctypes.c_void_p, ctypes.c_int])
+        _check(fn(self.handle, int(bool(enabled))), "set_lazy_moment_decay")
+
     def set_tensor_core_loss(self, enabled=True):
         _check(lib().gsn_solver_set_tensor_core_loss(self.handle, int(bool(enabled))), "set_tensor_core_loss")
 
@@ -550,6 +554,10 @@ class Trainer:
 
     def train(self, iterations):
         return lib().gsn_trainer_train(self.handle, int(iterations))
+
+    def set_lazy_moment_decay(self, enabled=True):
+        fn = declare("gsn_trainer_set_lazy_moment_decay", [ctypes.c_void_p, ctypes.c_int])
+        _check(fn(self.handle, int(bool(enabled))), "set_lazy_moment_decay")
 
     def render(self, camera, image_ptr):
         return lib().gsn_trainer_render(self.handle, ctypes.byref(camera), ctypes.c_void_p(image_ptr))

@@ -49,6 +49,7 @@ bool Solver::ResetOpacityHistory() {
 
 bool Solver::RemapGaussians(const int* parent_ids, int gaussian_count) {
     if (gaussian_count < 0) return false;
+    last_step_count_ = 0;  // step records restart as unknown after any remap
     if (gaussian_count == 0) {
         m_.Reset();
         v_.Reset();
@@ -183,6 +184,18 @@ bool Solver::UpdateGaussians(const CameraParams& camera, const Renderer& rendere
     a.bf16_sh = bf16_sh_;
     a.sparse = sparse_adam_;
     a.seed = static_cast<uint32_t>(iteration);
+    if (adam && lazy_moments_) {
+        if (!sparse_adam_ || frame_) return false;  // sparse eager updates only
+        if (last_step_count_ != count) {
+            if (!last_step_.Reserve(static_cast<size_t>(count)) ||
+                cudaMemsetAsync(last_step_.get(), 0, static_cast<size_t>(count) * sizeof(uint32_t), stream_) !=
+                    cudaSuccess)
+                return false;
+            last_step_count_ = count;
+        }
+        a.last_step = last_step_.get();
+        a.step = static_cast<uint32_t>(iteration);
+    }
     gsn::stage_mark(stream_, gsn::kStageGaussianUpdate);
     if (gsn::launch_gaussian_update(a, std::clamp(sh_degree, 0, 3), stream_) != GSN_OK) return false;
     gsn::stage_mark(stream_, gsn::kStageOther);

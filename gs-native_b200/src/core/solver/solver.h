@@ -106,6 +106,13 @@ public:
     // the reference updates all of them every iteration (solver.cu:912-915).
     void SetSparseAdam(bool enabled) { sparse_adam_ = enabled; }
     bool GetSparseAdam() const { return sparse_adam_; }
+    // Lazy moment decay for the sparse update: a Gaussian that skipped k steps has
+    // its moments decayed by 0.9^k and 0.999^k before its next update, as k dense
+    // steps with a zero gradient would have decayed them (its parameters do not
+    // take those steps' momentum moves). Eager steps only: an update through a
+    // captured step frame (CUDA graph) is refused.
+    void SetLazyMomentDecay(bool enabled) { lazy_moments_ = enabled; }
+    bool GetLazyMomentDecay() const { return lazy_moments_; }
     bool GetTensorCoreLoss() const { return tensor_core_loss_; }
     // Device status word of the tensor-core passes: 0, or GSN_ERR_TIMEOUT.
     const int* GetStatusDevice() const { return status_.get(); }
@@ -145,6 +152,9 @@ private:
     bool bf16_sh_ = false;
     bool tensor_core_loss_ = false;
     bool sparse_adam_ = false;
+    bool lazy_moments_ = false;
+    DeviceArray<uint32_t> last_step_;  // [N] step of each Gaussian's last update, 0: unknown
+    int last_step_count_ = 0;          // Gaussians last_step_ is valid for (0 after a remap)
     bool fast_loss_ = false;  // set by Iterate from the renderer's fast blend setting
     DeviceArray<int> status_;
 };

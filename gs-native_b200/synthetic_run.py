@@ -139,7 +139,11 @@ def main():
     p.add_argument("--fast", action="store_true", help="fast blend arithmetic (Horner power, hardware exp2)")
     p.add_argument("--fp32-ssim", action="store_true", help="with --precision: the fp32 SSIM kernel, not tcgen05")
     p.add_argument("--density-seed", type=int, default=0, help="seed of the density controller's random draws")
+    p.add_argument("--lazy-decay", action="store_true",
+                   help="with --sparse, no --graph: decay skipped Gaussians' moments lazily")
     args = p.parse_args()
+    if args.lazy_decay and (args.graph or not args.sparse):
+        p.error("--lazy-decay needs --sparse and eager steps (no --graph)")
     import torch
 
     gsn.lib()
@@ -153,6 +157,8 @@ def main():
                                         density_seed=args.density_seed)
     trainer = gsn.Trainer()
     assert trainer.initialize(train, train_images, points, colors, opts) == 0
+    if args.lazy_decay:
+        trainer.set_lazy_moment_decay(True)
     torch.cuda.synchronize()
     log = []
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -180,7 +186,8 @@ def main():
         "density_seed": args.density_seed,
         "form": ("precision_bf16" + ("_fp32ssim" if args.fp32_ssim else "") if args.precision else "plain_fp32") +
                 ("_culled" if args.culled else "") +
-                ("_sparse" if args.sparse else "") + ("_fast" if args.fast else "") + ("_graph" if args.graph else ""),
+                ("_sparse" if args.sparse else "") + ("_lazy" if args.lazy_decay else "") +
+                ("_fast" if args.fast else "") + ("_graph" if args.graph else ""),
         "log": log,
     }), flush=True)
 

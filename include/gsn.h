@@ -253,6 +253,11 @@ int gsn_solver_loss_device(gsn_solver* s, const double** out);
  * in the frame keep parameters and moments; the reference updates all
  * 58 x N every iteration (solver.cu:912-915). */
 int gsn_solver_set_sparse_adam(gsn_solver* s, int enabled);
+/* Lazy moment decay for the sparse update (gs-native extension, off by default):
+ * a Gaussian that skipped k steps has its moments scaled by 0.9^k and 0.999^k
+ * before its next update, the decay k dense zero-gradient steps would apply.
+ * Needs sparse Adam; eager steps only (a step through a CUDA graph fails). */
+int gsn_solver_set_lazy_moment_decay(gsn_solver* s, int enabled);
 /* Stage entry points of Iterate for parity tests and partial pipelines:
  * dL/dimage into the solver's buffer (device float[pixels * 3] via *out);
  * screen-space gradients ([count][12] floats via *out); mapped parameter
@@ -372,6 +377,9 @@ int gsn_trainer_initialize(gsn_trainer* t, const gsn_camera* cameras, const uint
                            const gsn_training_options* options);
 /* Train (gaussian_splatting.cpp:130-198). */
 int gsn_trainer_train(gsn_trainer* t, int iterations);
+/* The trainer's solver: gsn_solver_set_lazy_moment_decay (needs the sparse_adam
+ * option and graph = 0). */
+int gsn_trainer_set_lazy_moment_decay(gsn_trainer* t, int enabled);
 /* Render into a device fp32 HWC image (gaussian_splatting.cpp:200-232). */
 int gsn_trainer_render(gsn_trainer* t, const gsn_camera* camera, float* image);
 /* Mean PSNR / loss over views with host u8 HWC images (FP64 reductions). */

@@ -117,6 +117,63 @@ def test_sparse_adam_skips_invisible_gaussians():
     assert np.allclose(ms2[:, vis2], md2[:, vis2], rtol=1e-4, atol=1e-7)
 
 
+def test_lazy_moment_decay_matches_dense_moments():
+    """Lazy moment decay (gsn_solver_set_lazy_moment_decay): with every learning
+    rate at zero the parameters never move, so dense, sparse and lazy runs see the
+    same gradients. A Gaussian hidden for two steps then reaches its next visible
+    step with the dense run's moments (decayed by 0.9^2 and 0.999^2), while plain
+    sparse Adam carries its moments over undecayed."""
+    t = torch()
+    params = scenes.random_gaussians(30000, 9, mean_sigma=3.0)
+    cams = scenes.ring_cameras(4, 8.0, 15.0, 320, 240, 280.0, 280.0)
+    tgt = dev(np.random.default_rng(4).integers(0, 256, size=(240, 320, 3), dtype=np.uint8))
+    n = params.shape[1]
+    sequence = (cams[0], cams[2], cams[2], cams[0])
+    res = {}
+    for mode in ("dense", "sparse", "lazy"):
+        p = dev(params)
+        img = empty((240, 320, 3), t.float32)
+        r, s = gsn.Renderer(), gsn.Solver()
+        s.set_learning_rates(0.0, 0.0, 0.0, 0.0, 0.0)
+        s.set_sparse_adam(mode != "dense")
+        s.set_lazy_moment_decay(mode == "lazy")
+        vis = []
+        for cam in sequence:
+            assert r.render(p.data_ptr(), n, cam, [0, 0, 0], img.data_ptr(), 3) == 0
+            assert s.iterate(cam, r, img.data_ptr(), tgt.data_ptr(), p.data_ptr(), n, 0.0, 3) == 0
+            sync()
+            vis.append(host(r.buffers().tile_counts, np.int32, n) > 0)
+        m, v, _ = s.moments()
+        res[mode] = (host(m, np.float32, 58 * n).reshape(58, n), host(v, np.float32, 58 * n).reshape(58, n), vis,
+                     p.cpu().numpy())
+    md, vd, vis, pd = res["dense"]
+    assert np.array_equal(pd, params)  # zero learning rates: nothing moves
+    hidden = vis[0] & ~vis[1] & ~vis[2] & vis[3]
+    assert hidden.sum() > 100
+    ml, vl = res["lazy"][:2]
+    ms, vs = res["sparse"][:2]
+    assert np.allclose(ml[:, hidden], md[:, hidden], rtol=1e-4, atol=1e-7)
+    assert np.allclose(vl[:, hidden], vd[:, hidden], rtol=1e-4, atol=1e-12)
+    assert not np.allclose(ms[:, hidden], md[:, hidden], rtol=1e-4, atol=1e-7)
+    # Gaussians visible at every step take the same updates in all three runs
+    always = vis[0] & vis[1] & vis[2] & vis[3]
+    assert always.sum() > 100
+    assert np.allclose(ml[:, always], md[:, always], rtol=1e-4, atol=1e-7)
+
+
+def test_lazy_moment_decay_needs_the_sparse_update():
+    t = torch()
+    params = scenes.random_gaussians(2000, 9, mean_sigma=3.0)
+    cam = scenes.ring_cameras(4, 8.0, 15.0, 160, 120, 140.0, 140.0)[0]
+    tgt = dev(np.zeros((120, 160, 3), dtype=np.uint8))
+    p = dev(params)
+    img = empty((120, 160, 3), t.float32)
+    r, s = gsn.Renderer(), gsn.Solver()
+    s.set_lazy_moment_decay(True)  # without set_sparse_adam the step is refused
+    assert r.render(p.data_ptr(), params.shape[1], cam, [0, 0, 0], img.data_ptr(), 3) == 0
+    assert s.iterate(cam, r, img.data_ptr(), tgt.data_ptr(), p.data_ptr(), params.shape[1], 1e-3, 3) != 0
+
+
 def test_training_with_spatial_order_and_sparse_adam():
     import test_trainer_gpu as tt
     cams, images, points, colors = tt.ring_scene()
