@@ -424,7 +424,8 @@ __global__ void __launch_bounds__(256, 2) gaussian_update_kernel(GaussianUpdateA
                 a.grads_out[(GSN_SH_INDEX + c * kShStride + k) * N + i] = k < K ? ch.grgb[c] * ch.basis[k] : 0.0f;
     }
     // visibility-masked (sparse) Adam: a Gaussian outside the view keeps its
-    // parameters and moments (no momentum step, no moment decay)
+    // parameters and moments (no momentum step, no moment decay; with lazy decay
+    // the skipped steps' decay is applied at its next visible step, below)
     if (!a.m || (a.sparse && !visible)) return;
     float* __restrict__ P = a.params;
     float* __restrict__ M = a.m;

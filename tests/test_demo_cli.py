@@ -1,7 +1,8 @@
 """Command-line handling of the demo programs (gsn_train, gsn_render) on the
 host: the flags each one takes (the reference demos' flags plus the training
 forms' switches), and that a bad command line or an unreadable scene ends with
-status 1 and a message before any device work."""
+status 1 and a message before any device work; likewise the option checks of the
+synthetic full-run driver (synthetic_run.py)."""
 import os
 import subprocess
 
@@ -64,3 +65,13 @@ def test_render_reports_an_unreadable_scene(tmp_path):
                "--output", str(tmp_path / "out"))
     assert out.returncode == 1
     assert "failed" in out.stderr
+
+
+@pytest.mark.parametrize("args", [["--lazy-decay"], ["--lazy-decay", "--sparse", "--graph"]])
+def test_synthetic_run_rejects_lazy_decay_outside_eager_sparse_steps(args):
+    # lazy moment decay needs the sparse update and eager steps; the driver says
+    # so before it touches the device
+    import sys
+    script = os.path.join(ROOT, "gs-native_b200", "synthetic_run.py")
+    out = subprocess.run([sys.executable, script, *args], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 2 and "--lazy-decay needs --sparse" in out.stderr
